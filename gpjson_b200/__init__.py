@@ -1,0 +1,389 @@
+"""gpjson_b200 — B200-native structural index and JSONPath queries over NDJSON.
+
+Python mirror of GPJSON's polyglot library object (what
+``Polyglot.eval('gpjson', 'jsonpath')`` returns, GPJSONLibrary.java:48-54):
+
+    gpjson = GPJSON()
+    result = gpjson.query("dataset.json", "$.user.lang")
+    result[0][line][0]  # -> str (UTF-8 slice of the line) or None
+
+``query(file, paths, options)`` follows QueryFunction.call
+(functions/QueryFunction.java:48-265): a path or a list of 1..255 paths, an
+optional options mapping, and a Result indexed [query][line][slot] whose
+items are the matched values as strings or None (result/Result.java,
+ResultArray.java, ResultItem.java).  Everything runs on the GPU through the
+native library; there is no CPU path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import json
+import mmap
+import os
+from collections.abc import Sequence
+from ctypes import POINTER, byref, c_char_p, c_int, c_int64, c_size_t, c_uint8, c_void_p
+
+import numpy as np
+
+from . import _lib
+
+__all__ = [
+    "GPJSON",
+    "GPJSONException",
+    "JSONPathException",
+    "UnsupportedJSONPathException",
+    "CompiledQuery",
+    "File",
+    "Result",
+    "ResultArray",
+    "ResultItem",
+    "compile_path",
+    "prepare_queries",
+]
+
+MAX_QUERIES = _lib.GPJ_MAX_QUERIES
+MAX_LEVELS = _lib.GPJ_MAX_LEVELS
+
+
+class GPJSONException(Exception):
+    """GPJSONException.java: any failure of a query call.  ``code`` is the
+    native status (GPJ_E*)."""
+
+    def __init__(self, message: str, code: int = _lib.GPJ_EINVAL):
+        super().__init__(message)
+        self.code = code
+
+
+class JSONPathException(GPJSONException):
+    """jsonpath/JSONPathException.java: the path does not parse."""
+
+
+class UnsupportedJSONPathException(JSONPathException):
+    """jsonpath/UnsupportedJSONPathException.java: valid JSONPath outside
+    the supported subset ([*], .., [a,b], other filters)."""
+
+
+class CompiledQuery:
+    """JSONPathResult.java: bytecode, max depth and number of result stores."""
+
+    __slots__ = ("path", "bytecode", "max_depth", "num_results")
+
+    def __init__(self, path: str, bytecode: bytes, max_depth: int, num_results: int):
+        self.path = path
+        self.bytecode = bytecode
+        self.max_depth = max_depth
+        self.num_results = num_results
+
+    def __repr__(self) -> str:
+        return f"CompiledQuery({self.path!r}, depth={self.max_depth}, results={self.num_results})"
+
+
+def compile_path(path: str) -> CompiledQuery:
+    """JSONPathParser(path).compile() via the native compiler."""
+    lib = _lib.load()
+    cap = 4096 + 16 * len(path.encode("utf-8"))
+    while True:
+        out = (c_uint8 * cap)()
+        n, depth, res = c_size_t(), c_int(), c_int()
+        err = ctypes.create_string_buffer(512)
+        rc = lib.gpj_compile(path.encode("utf-8"), out, cap, byref(n), byref(depth), byref(res), err, 512)
+        if rc == _lib.GPJ_ELIMIT and n.value > cap:
+            cap = n.value
+            continue
+        break
+    msg = err.value.decode("utf-8", "replace")
+    if rc == _lib.GPJ_EUNSUPPORTED:
+        raise UnsupportedJSONPathException(msg, rc)
+    if rc == _lib.GPJ_EPARSE:
+        raise JSONPathException(msg, rc)
+    if rc != _lib.GPJ_OK:
+        raise GPJSONException(msg or f"gpj_compile failed ({rc})", rc)
+    return CompiledQuery(path, bytes(out[: n.value]), depth.value, res.value)
+
+
+class ResultItem(Sequence):
+    """result/ResultItem.java:32-52: the slots of one line for one query."""
+
+    __slots__ = ("_array", "_line")
+
+    def __init__(self, array: "ResultArray", line: int):
+        self._array = array
+        self._line = line
+
+    def __len__(self) -> int:
+        return self._array.results_per_line
+
+    def offsets(self, slot: int) -> tuple[int, int]:
+        o = self._array.offsets[self._line, slot]
+        return int(o[0]), int(o[1])
+
+    def __getitem__(self, slot):
+        if isinstance(slot, slice):
+            return [self[i] for i in range(*slot.indices(len(self)))]
+        if slot < 0:
+            slot += len(self)
+        if not 0 <= slot < len(self):
+            raise IndexError(slot)
+        start, end = self.offsets(slot)
+        if start == -1:
+            return None
+        if end < start:
+            # The reference builds new byte[end - start] here and fails with
+            # NegativeArraySizeException (ResultItem.java:190).
+            raise GPJSONException(f"result ({start}, {end}) has no end offset")
+        return self._array.file_bytes[start:end].decode("utf-8", "replace")
+
+
+class ResultArray(Sequence):
+    """result/ResultArray.java: one query's results, indexed by line."""
+
+    def __init__(self, offsets: np.ndarray, file_bytes):
+        self.offsets = offsets  # [lines][slots][2]
+        self.file_bytes = file_bytes
+        self.results_per_line = offsets.shape[1]
+
+    def __len__(self) -> int:
+        return self.offsets.shape[0]
+
+    def __getitem__(self, line):
+        if isinstance(line, slice):
+            return [self[i] for i in range(*line.indices(len(self)))]
+        if line < 0:
+            line += len(self)
+        if not 0 <= line < len(self):
+            raise IndexError(line)
+        return ResultItem(self, line)
+
+
+class Result(Sequence):
+    """result/Result.java: [query] -> ResultArray.  ``offsets`` is the raw
+    int64 array [queries][lines][slots][2] (start, end), -1 for a miss."""
+
+    def __init__(self, offsets: np.ndarray, file_bytes, paths: list[str]):
+        self.offsets = offsets
+        self.file_bytes = file_bytes
+        self.paths = paths
+
+    @property
+    def number_of_lines(self) -> int:
+        return self.offsets.shape[1]
+
+    def __len__(self) -> int:
+        return self.offsets.shape[0]
+
+    def __getitem__(self, q):
+        if isinstance(q, slice):
+            return [self[i] for i in range(*q.indices(len(self)))]
+        if q < 0:
+            q += len(self)
+        if not 0 <= q < len(self):
+            raise IndexError(q)
+        return ResultArray(self.offsets[q], self.file_bytes)
+
+
+def prepare_queries(queries, options=None) -> tuple[list[str], list[CompiledQuery]]:
+    """Argument handling and compilation of QueryFunction.call
+    (QueryFunction.java:64-136): a path or a list of 1..255 paths, an
+    optional mapping with `disable_fallback`, every path compiled, the depth
+    within the 16 levels of LeveledBitmapsIndex.  Raises GPJSONException
+    (or its JSONPath subclasses) with the reference's messages."""
+    if isinstance(queries, str):
+        paths = [queries]
+    elif isinstance(queries, (list, tuple)):
+        if len(queries) > MAX_QUERIES:
+            raise GPJSONException("Maximum size of queries is 255", _lib.GPJ_ELIMIT)
+        paths = list(queries)
+        if not all(isinstance(p, str) for p in paths):
+            raise GPJSONException("expected queries to be a string or string array")
+    else:
+        raise GPJSONException("expected queries to be a string or string array")
+    if not paths:
+        raise GPJSONException("expected queries to contain at least one query")
+    if options is not None and not hasattr(options, "get"):
+        raise GPJSONException("Invalid options")
+    disable_fallback = bool((options or {}).get("disable_fallback", False))
+    compiled = []
+    for i, p in enumerate(paths):
+        try:
+            compiled.append(compile_path(p))
+        except UnsupportedJSONPathException as e:
+            how = "fallback disabled" if disable_fallback else "no CPU fallback in this library"
+            raise UnsupportedJSONPathException(f"Unsupported JSON path ({i}, {how}): {e}", e.code) from e
+        except JSONPathException as e:
+            raise JSONPathException(f"Failed to parse JSON path ({i}): {e}", e.code) from e
+    depth = max(q.max_depth for q in compiled)
+    if depth > MAX_LEVELS:
+        raise GPJSONException(f"Invalid number of levels: {depth}", _lib.GPJ_ELIMIT)
+    return paths, compiled
+
+
+class _Native:
+    """A native context (gpj_ctx*)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = c_void_p()
+        rc = self.lib.gpj_create(device, byref(h))
+        if rc != _lib.GPJ_OK:
+            raise GPJSONException(self.lib.gpj_last_error(None).decode("utf-8", "replace"), rc)
+        self.h = h
+
+    def check(self, rc: int) -> None:
+        if rc != _lib.GPJ_OK:
+            msg = self.lib.gpj_last_error(self.h).decode("utf-8", "replace")
+            if rc == _lib.GPJ_EUNSUPPORTED:
+                raise UnsupportedJSONPathException(msg, rc)
+            if rc == _lib.GPJ_EPARSE:
+                raise JSONPathException(msg, rc)
+            raise GPJSONException(msg, rc)
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.gpj_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class File:
+    """An NDJSON input resident in device memory together with its index
+    (the reference keeps fileMemory and the index buffers for one call:
+    QueryFunction.java:148-245)."""
+
+    def __init__(self, native: _Native, handle: c_void_p, host_bytes=None, keepalive=None):
+        self._native = native
+        self._h = handle
+        self.host_bytes = host_bytes
+        self._keepalive = keepalive
+
+    @property
+    def size(self) -> int:
+        return self._native.lib.gpj_file_size(self._h)
+
+    def build_index(self, num_levels: int) -> None:
+        """CombinedIndex.create + LeveledBitmapsIndex(num_levels).create."""
+        self._native.check(self._native.lib.gpj_index_build(self._native.h, self._h, num_levels))
+
+    @property
+    def num_lines(self) -> int:
+        n = c_int64()
+        self._native.check(self._native.lib.gpj_index_num_lines(self._h, byref(n)))
+        return n.value
+
+    def newline_index(self) -> np.ndarray:
+        lines = self.num_lines
+        out = np.empty(lines, dtype=np.int64)
+        self._native.check(
+            self._native.lib.gpj_index_copy_newlines(self._native.h, self._h, out.ctypes.data, lines)
+        )
+        return out
+
+    def string_index(self) -> np.ndarray:
+        words = (self.size + 63) // 64
+        out = np.empty(words, dtype=np.uint64)
+        self._native.check(
+            self._native.lib.gpj_index_copy_string_index(self._native.h, self._h, out.ctypes.data, words)
+        )
+        return out
+
+    def leveled_bitmaps(self, num_levels: int) -> np.ndarray:
+        words = (self.size + 63) // 64
+        out = np.empty(words * num_levels, dtype=np.uint64)
+        self._native.check(
+            self._native.lib.gpj_index_copy_leveled_bitmaps(self._native.h, self._h, out.ctypes.data, out.size)
+        )
+        return out.reshape(num_levels, words)
+
+    def run(self, queries: list[CompiledQuery], slots: int | None = None) -> np.ndarray:
+        """One fused find_value pass; returns int64 [nq][lines][slots][2]."""
+        nq = len(queries)
+        slots = slots or max(q.num_results for q in queries)
+        bufs = [ctypes.create_string_buffer(q.bytecode, len(q.bytecode)) for q in queries]
+        ptrs = (c_void_p * nq)(*[ctypes.addressof(b) for b in bufs])
+        lens = (c_size_t * nq)(*[len(q.bytecode) for q in queries])
+        out = np.empty((nq, self.num_lines, slots, 2), dtype=np.int64)
+        self._native.check(
+            self._native.lib.gpj_query(self._native.h, self._h, nq, ptrs, lens, slots, out.ctypes.data, out.size)
+        )
+        return out
+
+    def release(self) -> None:
+        if self._h:
+            self._native.lib.gpj_file_release(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class GPJSON:
+    """The library object of GPJSONLibrary.java: members ``query`` and
+    ``exportTimings``."""
+
+    def __init__(self, device: int = 0):
+        self._native = _Native(device)
+
+    # -- files ---------------------------------------------------------------
+    def open(self, filename: str | os.PathLike) -> File:
+        h = c_void_p()
+        self._native.check(self._native.lib.gpj_file_open(self._native.h, os.fsencode(filename), byref(h)))
+        return File(self._native, h)
+
+    def load_bytes(self, data: bytes | bytearray | memoryview | np.ndarray) -> File:
+        arr = np.frombuffer(data, dtype=np.uint8) if not isinstance(data, np.ndarray) else data
+        h = c_void_p()
+        self._native.check(
+            self._native.lib.gpj_file_from_host(self._native.h, arr.ctypes.data, arr.size, byref(h))
+        )
+        return File(self._native, h, host_bytes=bytes(arr.tobytes()) if arr.size < (1 << 26) else arr)
+
+    def from_device(self, ptr: int, n: int, keepalive=None) -> File:
+        """Wraps n bytes already in device memory (e.g. a torch uint8 tensor's
+        data_ptr()); `keepalive` is held for the File's lifetime."""
+        h = c_void_p()
+        self._native.check(self._native.lib.gpj_file_from_device(self._native.h, c_void_p(ptr), n, byref(h)))
+        return File(self._native, h, keepalive=keepalive)
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        self._native.check(self._native.lib.gpj_set_stream(self._native.h, c_void_p(stream_handle or 0)))
+
+    # -- the reference members ------------------------------------------------
+    def query(self, filename, queries, options=None) -> Result:
+        """QueryFunction.call: query(file, path | [paths], options?)."""
+        paths, compiled = prepare_queries(queries, options)
+        depth = max(q.max_depth for q in compiled)
+        f = self.open(filename)
+        try:
+            f.build_index(depth)
+            offsets = f.run(compiled)
+        finally:
+            f.release()
+        with open(filename, "rb") as fh:
+            size = os.fstat(fh.fileno()).st_size
+            file_bytes = mmap.mmap(fh.fileno(), 0, access=mmap.ACCESS_READ) if size else b""
+        return Result(offsets, file_bytes, paths)
+
+    def exportTimings(self) -> str:  # noqa: N802  (reference member name)
+        """ExportTimingsFunction: the context's phase timings as JSON."""
+        n = c_size_t()
+        self._native.lib.gpj_get_timings(self._native.h, None, 0, byref(n))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        self._native.check(self._native.lib.gpj_get_timings(self._native.h, buf, n.value + 1, byref(n)))
+        return buf.value.decode()
+
+    def timings(self) -> dict:
+        return json.loads(self.exportTimings())
+
+    def kernel_launches(self) -> int:
+        return self._native.lib.gpj_kernel_launches(self._native.h)
+
+    def close(self) -> None:
+        self._native.close()

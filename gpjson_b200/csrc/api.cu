@@ -1,0 +1,772 @@
+// C ABI of gpjson_b200 (include/gpjson_b200.h): contexts, input files,
+// index builds, queries, results and diagnostics.
+//
+// This is the host runtime that replaces the reference's grCUDA-derived
+// CUDARuntime (gpu/CUDARuntime.java) and the orchestration of
+// functions/QueryFunction.java:48-265 and the stages/ classes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gpjson_b200.h"
+#include "device_common.cuh"
+#include "index_kernel.h"
+#include "jsonpath.h"
+#include "query_kernel.h"
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct Phase {
+    std::string name;
+    double device_ms;  // CUDA-event time on the context's stream
+    double host_ms;    // wall time of the call around it
+};
+
+}  // namespace
+
+struct gpj_ctx {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    std::string err;
+
+    // scratch of the index kernel
+    unsigned long long* d_tile_state = nullptr;
+    int64_t tile_state_words = 0;
+    unsigned int* d_counter = nullptr;
+    unsigned long long* d_status = nullptr;
+    unsigned long long* h_status = nullptr;  // pinned, 2 words
+    uint32_t epoch = 0;
+    int index_occupancy[3] = {0, 0, 0};  // levels <=4, <=8, <=16
+    int query_occupancy = 0;
+
+    // pinned staging for file reads
+    uint8_t* h_stage = nullptr;
+    size_t stage_bytes = 0;
+
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t launches = 0;
+    std::vector<Phase> phases;
+};
+
+struct gpj_file {
+    gpj_ctx* ctx = nullptr;
+    const uint8_t* d_data = nullptr;
+    uint8_t* d_owned = nullptr;
+    int64_t n = 0;
+    int64_t words = 0;
+
+    uint64_t* d_str = nullptr;
+    uint64_t* d_lvl = nullptr;
+    int lvl_cap = 0;
+    int64_t* d_nl = nullptr;
+    int64_t nl_cap = 0;
+    bool indexed = false;
+    int num_levels = 0;
+    int64_t num_lines = 0;
+
+    // uploaded bytecode (cached across calls with identical queries)
+    std::vector<uint8_t> ir_host;
+    uint8_t* d_ir = nullptr;
+    size_t d_ir_cap = 0;
+    // results of gpj_query with a host destination
+    int64_t* d_out = nullptr;
+    size_t d_out_cap = 0;  // elements
+};
+
+struct gpj_result {
+    int64_t nq = 0, lines = 0;
+    int slots = 0;
+    std::vector<int64_t> offsets;
+};
+
+namespace {
+
+int fail(gpj_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+int cuda_fail(gpj_ctx* ctx, cudaError_t e, const char* what) {
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "CUDA error %d (%s: %s) in %s", static_cast<int>(e),
+                  cudaGetErrorName(e), cudaGetErrorString(e), what);
+    return fail(ctx, e == cudaErrorMemoryAllocation ? GPJ_ENOMEM : GPJ_ECUDA, buf);
+}
+
+#define GPJ_CUDA(ctx, call)                                        \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call); \
+    } while (0)
+
+template <typename T>
+int device_alloc(gpj_ctx* ctx, T** p, size_t count, const char* what) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(ctx, e, what);
+    }
+    *p = static_cast<T*>(q);
+    return GPJ_OK;
+}
+
+template <typename T>
+void device_free(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+// Records a phase measured between ev0 (recorded at `host_start`) and now.
+int end_phase(gpj_ctx* ctx, const char* name, double host_start) {
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    GPJ_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+    float ms = 0.f;
+    GPJ_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->phases.push_back(Phase{name, static_cast<double>(ms), now_ms() - host_start});
+    return GPJ_OK;
+}
+
+int ensure_tile_state(gpj_ctx* ctx, int64_t ntiles) {
+    const int64_t words = 3 * ntiles;
+    if (words > ctx->tile_state_words) {
+        device_free(ctx->d_tile_state);
+        ctx->tile_state_words = 0;
+        const int64_t cap = std::max<int64_t>(words, 3 * 4096);
+        int rc = device_alloc(ctx, &ctx->d_tile_state, static_cast<size_t>(cap), "cudaMalloc(tile state)");
+        if (rc) return rc;
+        GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_tile_state, 0, cap * 8, ctx->stream));
+        ctx->tile_state_words = cap;
+        ctx->epoch = 0;
+    }
+    if (++ctx->epoch > 0xFFFFu) {  // tags wrapped: clear and restart
+        GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_tile_state, 0, ctx->tile_state_words * 8, ctx->stream));
+        ctx->epoch = 1;
+    }
+    return GPJ_OK;
+}
+
+int occupancy_slot(int num_levels) { return num_levels <= 4 ? 0 : (num_levels <= 8 ? 1 : 2); }
+
+// One launch of the index kernel; *lines receives the line count.
+int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, uint64_t* d_str,
+              uint64_t* d_lvl, int64_t* d_nl, int64_t nl_cap, int64_t* lines) {
+    if (n == 0) {
+        if (nl_cap > 0) GPJ_CUDA(ctx, cudaMemsetAsync(d_nl, 0, 8, ctx->stream));
+        GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        *lines = 1;
+        return GPJ_OK;
+    }
+    const int64_t ntiles = (n + gpj::kIndexTileBytes - 1) / gpj::kIndexTileBytes;
+    int rc = ensure_tile_state(ctx, ntiles);
+    if (rc) return rc;
+    GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned int), ctx->stream));
+    GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    gpj::IndexParams p;
+    p.file = d_file;
+    p.n = n;
+    p.ntiles = ntiles;
+    p.string_index = d_str;
+    p.leveled = d_lvl;
+    p.level_size = (n + 63) / 64;
+    p.num_levels = num_levels;
+    p.newlines = d_nl;
+    p.newline_cap = nl_cap;
+    p.tile_state = ctx->d_tile_state;
+    p.tile_counter = ctx->d_counter;
+    p.status = ctx->d_status;
+    p.epoch = ctx->epoch;
+    const int occ = ctx->index_occupancy[occupancy_slot(num_levels)];
+    const int64_t grid = std::min<int64_t>(ntiles, static_cast<int64_t>(ctx->sms) * occ);
+    GPJ_CUDA(ctx, gpj::launch_index_kernel(p, static_cast<int>(grid), ctx->stream));
+    ctx->launches++;
+    GPJ_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const unsigned long long errs = ctx->h_status[1];
+    if (errs) {
+        std::string m = "index kernel reported:";
+        if (errs & gpj::kErrLookbackTimeout) m += " look-back wait expired;";
+        if (errs & gpj::kErrCopyTimeout) m += " TMA copy wait expired;";
+        if (errs & gpj::kErrEscapeRun)
+            m += " a backslash run longer than 64 KiB crosses a 16 KiB tile boundary;";
+        return fail(ctx, (errs & gpj::kErrEscapeRun) ? GPJ_ELIMIT : GPJ_EDEVICE, m);
+    }
+    *lines = static_cast<int64_t>(ctx->h_status[0]);
+    return GPJ_OK;
+}
+
+int check_ctx(gpj_ctx* ctx) {
+    if (!ctx) return GPJ_EINVAL;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+    return GPJ_OK;
+}
+
+int make_file(gpj_ctx* ctx, int64_t n, gpj_file** out) {
+    gpj_file* f = new (std::nothrow) gpj_file;
+    if (!f) return fail(ctx, GPJ_ENOMEM, "out of host memory");
+    f->ctx = ctx;
+    f->n = n;
+    f->words = (n + 63) / 64;
+    *out = f;
+    return GPJ_OK;
+}
+
+// Packs validated bytecode as [int32 offsets (16-byte padded)][bytes] and
+// uploads it unless the previous upload was identical.
+int upload_queries(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, const size_t* len,
+                   int slots, int* depth_needed) {
+    std::vector<uint8_t> packed;
+    const size_t header = ((static_cast<size_t>(nq) * 4 + 15) / 16) * 16;
+    packed.resize(header);
+    int deepest = 0;
+    for (int q = 0; q < nq; q++) {
+        if (!bc[q] || len[q] == 0) return fail(ctx, GPJ_EINVAL, "empty bytecode for query " + std::to_string(q));
+        int depth = 0, stores = 0;
+        std::string why;
+        if (!gpj::validate_bytecode(bc[q], len[q], GPJ_MAX_LEVELS, slots, &depth, &stores, &why))
+            return fail(ctx, GPJ_EINVAL, "invalid bytecode for query " + std::to_string(q) + ": " + why);
+        deepest = std::max(deepest, depth);
+        const int32_t off = static_cast<int32_t>(packed.size() - header);
+        std::memcpy(packed.data() + 4 * q, &off, 4);
+        packed.insert(packed.end(), bc[q], bc[q] + len[q]);
+    }
+    *depth_needed = deepest;
+    if (packed == f->ir_host && f->d_ir) return GPJ_OK;
+    if (packed.size() > f->d_ir_cap) {
+        device_free(f->d_ir);
+        f->d_ir_cap = 0;
+        int rc = device_alloc(ctx, &f->d_ir, packed.size() * 2, "cudaMalloc(bytecode)");
+        if (rc) return rc;
+        f->d_ir_cap = packed.size() * 2;
+    }
+    GPJ_CUDA(ctx, cudaMemcpyAsync(f->d_ir, packed.data(), packed.size(), cudaMemcpyHostToDevice, ctx->stream));
+    GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    f->ir_host.swap(packed);
+    return GPJ_OK;
+}
+
+int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out) {
+    const size_t header = ((static_cast<size_t>(nq) * 4 + 15) / 16) * 16;
+    gpj::QueryParams p;
+    p.file = f->d_data;
+    p.n = f->n;
+    p.newlines = f->d_nl;
+    p.num_lines = f->num_lines;
+    p.string_index = f->d_str;
+    p.leveled = f->d_lvl;
+    p.level_size = f->words;
+    p.bytecode = f->d_ir + header;
+    p.offsets = reinterpret_cast<const int32_t*>(f->d_ir);
+    p.num_queries = nq;
+    p.slots = slots;
+    p.out = d_out;
+    const int64_t want = (f->num_lines + 255) / 256;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * ctx->query_occupancy));
+    GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->stream));
+    ctx->launches++;
+    return GPJ_OK;
+}
+
+int query_common(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, const size_t* len,
+                 int slots, int64_t** d_out_io, int64_t out_count, bool to_host, int64_t* host_out) {
+    if (nq < 1 || nq > GPJ_MAX_QUERIES)
+        return fail(ctx, GPJ_ELIMIT, "Maximum size of queries is 255 (got " + std::to_string(nq) + ")");
+    if (slots < 1) return fail(ctx, GPJ_EINVAL, "result_slots must be >= 1");
+    if (!f->indexed) return fail(ctx, GPJ_ESTATE, "file is not indexed (call gpj_index_build)");
+    const int64_t need = static_cast<int64_t>(nq) * f->num_lines * slots * 2;
+    if (out_count < need)
+        return fail(ctx, GPJ_EINVAL, "output holds " + std::to_string(out_count) + " elements, " +
+                                         std::to_string(need) + " needed");
+    int depth = 0;
+    int rc = upload_queries(ctx, f, nq, bc, len, slots, &depth);
+    if (rc) return rc;
+    if (depth > f->num_levels)
+        return fail(ctx, GPJ_ESTATE, "queries need " + std::to_string(depth) + " levels, index has " +
+                                         std::to_string(f->num_levels));
+    int64_t* d_out = *d_out_io;
+    const double t0 = now_ms();
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    rc = launch_query(ctx, f, nq, slots, d_out);
+    if (rc) return rc;
+    if (!to_host) return GPJ_OK;
+    rc = end_phase(ctx, "find_value", t0);
+    if (rc) return rc;
+    const double t1 = now_ms();
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    GPJ_CUDA(ctx, cudaMemcpyAsync(host_out, d_out, need * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    return end_phase(ctx, "copy_results", t1);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gpj_version(void) { return "gpjson_b200 0.1 sm_100a"; }
+
+int gpj_create(int device, gpj_ctx** out) {
+    if (!out) return GPJ_EINVAL;
+    *out = nullptr;
+    gpj_ctx* ctx = new (std::nothrow) gpj_ctx;
+    if (!ctx) return GPJ_ENOMEM;
+    auto bail = [&](cudaError_t e, const char* what) {
+        cuda_fail(ctx, e, what);
+        g_create_error = ctx->err;
+        gpj_destroy(ctx);
+        return e == cudaErrorMemoryAllocation ? GPJ_ENOMEM : GPJ_ECUDA;
+    };
+    ctx->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return bail(e, "cudaSetDevice");
+    cudaDeviceProp prop;
+    e = cudaGetDeviceProperties(&prop, device);
+    if (e != cudaSuccess) return bail(e, "cudaGetDeviceProperties");
+    if (prop.major != 10) {
+        g_create_error = std::string("device ") + prop.name + " is not sm_100 (this library is built for sm_100a only)";
+        gpj_destroy(ctx);
+        return GPJ_ECUDA;
+    }
+    ctx->sms = prop.multiProcessorCount;
+    if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(e, "cudaStreamCreate");
+    ctx->stream = ctx->own_stream;
+    if ((e = cudaMalloc(&ctx->d_counter, 16)) != cudaSuccess) return bail(e, "cudaMalloc(counter)");
+    if ((e = cudaMalloc(&ctx->d_status, 16)) != cudaSuccess) return bail(e, "cudaMalloc(status)");
+    if ((e = cudaMallocHost(&ctx->h_status, 16)) != cudaSuccess) return bail(e, "cudaMallocHost(status)");
+    if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess) return bail(e, "cudaEventCreate");
+    if ((e = cudaEventCreate(&ctx->ev1)) != cudaSuccess) return bail(e, "cudaEventCreate");
+    const int levels[3] = {4, 8, 16};
+    for (int i = 0; i < 3; i++) {
+        ctx->index_occupancy[i] = gpj::index_kernel_max_ctas_per_sm(levels[i]);
+        if (ctx->index_occupancy[i] < 1) return bail(cudaGetLastError(), "index kernel occupancy");
+    }
+    ctx->query_occupancy = gpj::find_value_max_ctas_per_sm();
+    if (ctx->query_occupancy < 1) return bail(cudaGetLastError(), "find_value occupancy");
+    *out = ctx;
+    return GPJ_OK;
+}
+
+void gpj_destroy(gpj_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+    device_free(ctx->d_tile_state);
+    device_free(ctx->d_counter);
+    device_free(ctx->d_status);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+}
+
+const char* gpj_last_error(const gpj_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+int gpj_set_stream(gpj_ctx* ctx, void* stream) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    return GPJ_OK;
+}
+
+int gpj_compile(const char* path, uint8_t* out, size_t cap, size_t* len, int* max_depth,
+                int* num_results, char* err, size_t err_cap) {
+    auto set_err = [&](const std::string& m) {
+        if (err && err_cap > 0) {
+            std::strncpy(err, m.c_str(), err_cap - 1);
+            err[err_cap - 1] = '\0';
+        }
+    };
+    if (!path || !len || !max_depth || !num_results) {
+        set_err("null argument");
+        return GPJ_EINVAL;
+    }
+    try {
+        gpj::CompiledPath r = gpj::compile_path(path);
+        *len = r.bytecode.size();
+        *max_depth = r.max_depth;
+        *num_results = r.num_results;
+        if (r.bytecode.size() > cap || (!out && cap > 0)) {
+            set_err("bytecode needs " + std::to_string(r.bytecode.size()) + " bytes");
+            return GPJ_ELIMIT;
+        }
+        if (out) std::memcpy(out, r.bytecode.data(), r.bytecode.size());
+        set_err("");
+        return GPJ_OK;
+    } catch (const gpj::PathError& e) {
+        set_err(e.what());
+        return e.unsupported ? GPJ_EUNSUPPORTED : GPJ_EPARSE;
+    } catch (const std::exception& e) {
+        set_err(e.what());
+        return GPJ_EPARSE;
+    }
+}
+
+int gpj_file_from_device(gpj_ctx* ctx, const void* d_data, int64_t n, gpj_file** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out || n < 0 || (n > 0 && !d_data)) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (reinterpret_cast<uintptr_t>(d_data) % 16 != 0)
+        return fail(ctx, GPJ_EINVAL, "device input must be 16-byte aligned");
+    rc = make_file(ctx, n, out);
+    if (rc) return rc;
+    (*out)->d_data = static_cast<const uint8_t*>(d_data);
+    return GPJ_OK;
+}
+
+int gpj_file_from_host(gpj_ctx* ctx, const void* data, int64_t n, gpj_file** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out || n < 0 || (n > 0 && !data)) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    gpj_file* f = nullptr;
+    rc = make_file(ctx, n, &f);
+    if (rc) return rc;
+    rc = device_alloc(ctx, &f->d_owned, static_cast<size_t>(n), "cudaMalloc(file)");
+    if (rc) {
+        delete f;
+        return rc;
+    }
+    f->d_data = f->d_owned;
+    const double t0 = now_ms();
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    cudaError_t e = cudaMemcpyAsync(f->d_owned, data, static_cast<size_t>(n), cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+        gpj_file_release(f);
+        return cuda_fail(ctx, e, "cudaMemcpyAsync(file)");
+    }
+    rc = end_phase(ctx, "copy_file", t0);
+    if (rc) {
+        gpj_file_release(f);
+        return rc;
+    }
+    *out = f;
+    return GPJ_OK;
+}
+
+int gpj_file_open(gpj_ctx* ctx, const char* filename, gpj_file** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!filename || !out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    FILE* fp = std::fopen(filename, "rb");
+    if (!fp) return fail(ctx, GPJ_EIO, std::string("Failed to open file ") + filename);
+    std::fseek(fp, 0, SEEK_END);
+    const int64_t n = static_cast<int64_t>(std::ftell(fp));
+    std::fseek(fp, 0, SEEK_SET);
+    if (n < 0) {
+        std::fclose(fp);
+        return fail(ctx, GPJ_EIO, std::string("Failed to get size of file ") + filename);
+    }
+    gpj_file* f = nullptr;
+    rc = make_file(ctx, n, &f);
+    if (rc) {
+        std::fclose(fp);
+        return rc;
+    }
+    rc = device_alloc(ctx, &f->d_owned, static_cast<size_t>(n), "cudaMalloc(file)");
+    if (rc) {
+        std::fclose(fp);
+        delete f;
+        return rc;
+    }
+    f->d_data = f->d_owned;
+    // Two pinned halves: the disk read of one chunk overlaps the copy of the other.
+    const size_t chunk = 32u << 20;
+    if (!ctx->h_stage) {
+        cudaError_t e = cudaMallocHost(&ctx->h_stage, 2 * chunk);
+        if (e != cudaSuccess) {
+            std::fclose(fp);
+            gpj_file_release(f);
+            return cuda_fail(ctx, e, "cudaMallocHost(staging)");
+        }
+        ctx->stage_bytes = 2 * chunk;
+    }
+    const double t0 = now_ms();
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
+    int64_t pos = 0;
+    int half = 0;
+    rc = GPJ_OK;
+    while (pos < n) {
+        const size_t want = static_cast<size_t>(std::min<int64_t>(static_cast<int64_t>(chunk), n - pos));
+        uint8_t* stage = ctx->h_stage + half * chunk;
+        cudaEventSynchronize(done[half]);  // the copy that last used this half is done
+        if (std::fread(stage, 1, want, fp) != want) {
+            rc = fail(ctx, GPJ_EIO, std::string("Size of file has changed while reading ") + filename);
+            break;
+        }
+        cudaError_t e = cudaMemcpyAsync(f->d_owned + pos, stage, want, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) {
+            rc = cuda_fail(ctx, e, "cudaMemcpyAsync(file)");
+            break;
+        }
+        cudaEventRecord(done[half], ctx->stream);
+        pos += static_cast<int64_t>(want);
+        half ^= 1;
+    }
+    std::fclose(fp);
+    if (rc == GPJ_OK) rc = end_phase(ctx, "read_file", t0);
+    else cudaStreamSynchronize(ctx->stream);
+    cudaEventDestroy(done[0]);
+    cudaEventDestroy(done[1]);
+    if (rc) {
+        gpj_file_release(f);
+        return rc;
+    }
+    *out = f;
+    return GPJ_OK;
+}
+
+void gpj_file_release(gpj_file* f) {
+    if (!f) return;
+    if (f->ctx) {
+        cudaSetDevice(f->ctx->device);
+        cudaStreamSynchronize(f->ctx->stream);
+    }
+    device_free(f->d_owned);
+    device_free(f->d_str);
+    device_free(f->d_lvl);
+    device_free(f->d_nl);
+    device_free(f->d_ir);
+    device_free(f->d_out);
+    delete f;
+}
+
+int64_t gpj_file_size(const gpj_file* f) { return f ? f->n : -1; }
+
+int gpj_index_build(gpj_ctx* ctx, gpj_file* f, int num_levels) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!f || f->ctx != ctx) return fail(ctx, GPJ_EINVAL, "file does not belong to this context");
+    if (num_levels < 1 || num_levels > GPJ_MAX_LEVELS)
+        return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(num_levels));
+    if (!f->d_str && (rc = device_alloc(ctx, &f->d_str, static_cast<size_t>(f->words), "cudaMalloc(string index)")))
+        return rc;
+    if (f->lvl_cap < num_levels) {
+        device_free(f->d_lvl);
+        f->lvl_cap = 0;
+        rc = device_alloc(ctx, &f->d_lvl, static_cast<size_t>(f->words) * num_levels, "cudaMalloc(leveled bitmaps)");
+        if (rc) return rc;
+        f->lvl_cap = num_levels;
+    }
+    if (!f->d_nl) {
+        f->nl_cap = std::min<int64_t>(f->n + 1, f->n / 256 + 1024);
+        rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(f->nl_cap), "cudaMalloc(newline index)");
+        if (rc) return rc;
+    }
+    f->indexed = false;
+    const double t0 = now_ms();
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    int64_t lines = 0;
+    rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
+    if (rc) return rc;
+    if (lines > f->nl_cap) {  // more lines than the first guess: size exactly and rebuild
+        device_free(f->d_nl);
+        f->nl_cap = lines;
+        rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(lines), "cudaMalloc(newline index)");
+        if (rc) return rc;
+        rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
+        if (rc) return rc;
+    }
+    rc = end_phase(ctx, "build_index", t0);
+    if (rc) return rc;
+    f->num_lines = lines;
+    f->num_levels = num_levels;
+    f->indexed = true;
+    return GPJ_OK;
+}
+
+int gpj_index_num_lines(const gpj_file* f, int64_t* lines) {
+    if (!f || !lines) return GPJ_EINVAL;
+    if (!f->indexed) return GPJ_ESTATE;
+    *lines = f->num_lines;
+    return GPJ_OK;
+}
+
+int gpj_index_copy_newlines(gpj_ctx* ctx, const gpj_file* f, int64_t* host, int64_t count) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!f || !host) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (!f->indexed) return fail(ctx, GPJ_ESTATE, "file is not indexed");
+    if (count < f->num_lines) return fail(ctx, GPJ_EINVAL, "host buffer too small");
+    GPJ_CUDA(ctx, cudaMemcpyAsync(host, f->d_nl, f->num_lines * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GPJ_OK;
+}
+
+int gpj_index_copy_string_index(gpj_ctx* ctx, const gpj_file* f, uint64_t* host, int64_t count) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!f || (!host && f->words > 0)) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (!f->indexed) return fail(ctx, GPJ_ESTATE, "file is not indexed");
+    if (count < f->words) return fail(ctx, GPJ_EINVAL, "host buffer too small");
+    if (f->words == 0) return GPJ_OK;
+    GPJ_CUDA(ctx, cudaMemcpyAsync(host, f->d_str, f->words * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GPJ_OK;
+}
+
+int gpj_index_copy_leveled_bitmaps(gpj_ctx* ctx, const gpj_file* f, uint64_t* host, int64_t count) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!f || (!host && f->words > 0)) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (!f->indexed) return fail(ctx, GPJ_ESTATE, "file is not indexed");
+    const int64_t total = f->words * f->num_levels;
+    if (count < total) return fail(ctx, GPJ_EINVAL, "host buffer too small");
+    if (total == 0) return GPJ_OK;
+    GPJ_CUDA(ctx, cudaMemcpyAsync(host, f->d_lvl, total * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GPJ_OK;
+}
+
+int gpj_build_index_device(gpj_ctx* ctx, const void* d_file, int64_t n, int num_levels,
+                           uint64_t* d_string_index, uint64_t* d_leveled, int64_t* d_newlines,
+                           int64_t newline_cap, int64_t* num_lines) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (n < 0 || !num_lines || (n > 0 && (!d_file || !d_string_index || !d_leveled)) ||
+        newline_cap < 0 || (newline_cap > 0 && !d_newlines))
+        return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (reinterpret_cast<uintptr_t>(d_file) % 16 != 0)
+        return fail(ctx, GPJ_EINVAL, "device input must be 16-byte aligned");
+    if (num_levels < 1 || num_levels > GPJ_MAX_LEVELS)
+        return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(num_levels));
+    const double t0 = now_ms();
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    rc = run_index(ctx, static_cast<const uint8_t*>(d_file), n, num_levels, d_string_index, d_leveled,
+                   d_newlines, newline_cap, num_lines);
+    if (rc) return rc;
+    rc = end_phase(ctx, "build_index", t0);
+    if (rc) return rc;
+    if (*num_lines > newline_cap)
+        return fail(ctx, GPJ_ELIMIT, "newline index needs " + std::to_string(*num_lines) + " entries");
+    return GPJ_OK;
+}
+
+int gpj_query(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, const size_t* len,
+              int slots, int64_t* host_out, int64_t out_count) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!f || !bc || !len || !host_out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    const int64_t need = static_cast<int64_t>(nq) * f->num_lines * std::max(slots, 1) * 2;
+    if (f->indexed && static_cast<size_t>(need) > f->d_out_cap) {
+        device_free(f->d_out);
+        f->d_out_cap = 0;
+        rc = device_alloc(ctx, &f->d_out, static_cast<size_t>(need), "cudaMalloc(results)");
+        if (rc) return rc;
+        f->d_out_cap = static_cast<size_t>(need);
+    }
+    return query_common(ctx, f, nq, bc, len, slots, &f->d_out, out_count, true, host_out);
+}
+
+int gpj_query_device(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, const size_t* len,
+                     int slots, int64_t* d_out, int64_t out_count) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!f || !bc || !len || !d_out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    return query_common(ctx, f, nq, bc, len, slots, &d_out, out_count, false, nullptr);
+}
+
+int gpj_query_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths, gpj_result** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!f || !paths || !out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (nq > GPJ_MAX_QUERIES) return fail(ctx, GPJ_ELIMIT, "Maximum size of queries is 255");
+    if (nq < 1) return fail(ctx, GPJ_EINVAL, "expected queries to contain at least one query");
+    std::vector<gpj::CompiledPath> compiled(static_cast<size_t>(nq));
+    int depth = 0, slots = 0;
+    for (int i = 0; i < nq; i++) {
+        try {
+            compiled[i] = gpj::compile_path(paths[i] ? paths[i] : "");
+        } catch (const gpj::PathError& e) {
+            if (e.unsupported)
+                return fail(ctx, GPJ_EUNSUPPORTED, "Unsupported JSON path (" + std::to_string(i) + "): " + e.what());
+            return fail(ctx, GPJ_EPARSE, "Failed to parse JSON path (" + std::to_string(i) + "): " + e.what());
+        }
+        depth = std::max(depth, compiled[i].max_depth);
+        slots = std::max(slots, compiled[i].num_results);
+    }
+    if (depth > GPJ_MAX_LEVELS)
+        return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(depth));
+    if (!f->indexed || f->num_levels < depth) {
+        rc = gpj_index_build(ctx, f, depth);
+        if (rc) return rc;
+    }
+    gpj_result* r = new (std::nothrow) gpj_result;
+    if (!r) return fail(ctx, GPJ_ENOMEM, "out of host memory");
+    r->nq = nq;
+    r->lines = f->num_lines;
+    r->slots = slots;
+    try {
+        r->offsets.resize(static_cast<size_t>(nq) * f->num_lines * slots * 2);
+    } catch (const std::bad_alloc&) {
+        delete r;
+        return fail(ctx, GPJ_ENOMEM, "out of host memory for results");
+    }
+    std::vector<const uint8_t*> bcs(static_cast<size_t>(nq));
+    std::vector<size_t> lens(static_cast<size_t>(nq));
+    for (int i = 0; i < nq; i++) {
+        bcs[i] = compiled[i].bytecode.data();
+        lens[i] = compiled[i].bytecode.size();
+    }
+    rc = gpj_query(ctx, f, nq, bcs.data(), lens.data(), slots, r->offsets.data(),
+                   static_cast<int64_t>(r->offsets.size()));
+    if (rc) {
+        delete r;
+        return rc;
+    }
+    *out = r;
+    return GPJ_OK;
+}
+
+int64_t gpj_result_num_queries(const gpj_result* r) { return r ? r->nq : -1; }
+int64_t gpj_result_num_lines(const gpj_result* r) { return r ? r->lines : -1; }
+int gpj_result_slots(const gpj_result* r) { return r ? r->slots : -1; }
+const int64_t* gpj_result_offsets(const gpj_result* r) { return r ? r->offsets.data() : nullptr; }
+void gpj_result_release(gpj_result* r) { delete r; }
+
+int gpj_get_timings(gpj_ctx* ctx, char* json, size_t cap, size_t* len) {
+    if (!ctx) return GPJ_EINVAL;
+    std::string s = "{\"phases\":[";
+    for (size_t i = 0; i < ctx->phases.size(); i++) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf, "%s{\"name\":\"%s\",\"device_ms\":%.6f,\"host_ms\":%.6f}", i ? "," : "",
+                      ctx->phases[i].name.c_str(), ctx->phases[i].device_ms, ctx->phases[i].host_ms);
+        s += buf;
+    }
+    s += "],\"kernel_launches\":" + std::to_string(ctx->launches) + "}";
+    if (len) *len = s.size();
+    if (json && cap > 0) {
+        const size_t k = std::min(cap - 1, s.size());
+        std::memcpy(json, s.data(), k);
+        json[k] = '\0';
+    }
+    return GPJ_OK;
+}
+
+void gpj_reset_timings(gpj_ctx* ctx) {
+    if (ctx) ctx->phases.clear();
+}
+
+int64_t gpj_kernel_launches(const gpj_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+}  // extern "C"

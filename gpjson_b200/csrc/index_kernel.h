@@ -1,0 +1,35 @@
+// Host-side interface of the single-pass index kernel (index_kernel.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace gpj {
+
+constexpr int64_t kIndexTileBytes = 16384;
+// The escape state at a tile start is found by scanning back over the bytes
+// before it; a backslash run longer than this crossing a tile start is
+// reported as an error (kErrEscapeRun) instead of being resolved.
+constexpr int64_t kEscapeScanBytes = 1 << 16;
+
+struct IndexParams {
+    const uint8_t* file;
+    int64_t n;
+    int64_t ntiles;
+    uint64_t* string_index;  // ceil(n/64)
+    uint64_t* leveled;       // num_levels * level_size
+    int64_t level_size;      // ceil(n/64)
+    int num_levels;
+    int64_t* newlines;  // newline_cap entries
+    int64_t newline_cap;
+    unsigned long long* tile_state;  // 3 * ntiles words, tagged with `epoch`
+    unsigned int* tile_counter;      // zeroed before the launch
+    unsigned long long* status;      // [0] line count, [1] error bits (zeroed before)
+    uint32_t epoch;                  // 1..65535
+};
+
+cudaError_t launch_index_kernel(const IndexParams& p, int grid, cudaStream_t stream);
+int index_kernel_max_ctas_per_sm(int num_levels);
+
+}  // namespace gpj

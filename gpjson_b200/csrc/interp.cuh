@@ -1,0 +1,203 @@
+// Per-line JSONPath bytecode interpreter over the leveled bitmaps.
+//
+// Semantics follow the reference interpreter find_value
+// (gpjson/src/main/resources/com/koenv/gpjson/kernels/find_value.cu:21-263),
+// which equals Sequential.findValue (sequential/Sequential.java:130-344).
+// Instead of visiting every byte, the scan jumps from one structural bit of
+// the current level to the next: bytes without such a bit cannot change the
+// interpreter's state while it is searching (find_value.cu skips whole zero
+// words for the same reason, :218-222).
+//
+// Where the reference reads out of bounds or trips a device assert, the
+// behaviour below is fixed (marked [bounded]) and the test oracle implements
+// the same choice.  __host__ __device__ so the test suite can run it on the
+// CPU against the oracle.
+#pragma once
+
+#include <cstdint>
+
+#include "word_ops.cuh"
+
+namespace gpj {
+
+// One more than the deepest level a query may reach (16 key/index steps).
+constexpr int kLevelSlots = 17;
+
+struct LineView {
+    const uint8_t* file;
+    int64_t n;
+    const uint64_t* string_index;
+    const uint64_t* levels;  // [level][level_size]
+    int64_t level_size;
+};
+
+GPJ_HD bool is_ws(uint8_t c) { return c == '\n' || c == '\r' || c == '\t' || c == ' '; }
+
+// First set bit of `bm` at a position in [from, limit), or `limit`.
+GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit) {
+    if (from >= limit) return limit;
+    int64_t w = from >> 6;
+    uint64_t m = bm[w] & (~0ull << (from & 63));
+    for (;;) {
+        if (m) {
+            const int64_t p = (w << 6) + ctz64(m);
+            return p < limit ? p : limit;
+        }
+        ++w;
+        if ((w << 6) >= limit) return limit;
+        m = bm[w];
+    }
+}
+
+// Last set bit of `bm` at a position in (floor, from], or -1.
+GPJ_HD int64_t prev_bit(const uint64_t* bm, int64_t from, int64_t floor) {
+    if (from <= floor) return -1;
+    int64_t w = from >> 6;
+    uint64_t m = bm[w] & (~0ull >> (63 - (from & 63)));
+    for (;;) {
+        if (m) {
+            const int64_t k = (w << 6) + 63 - clz64(m);
+            return k > floor ? k : -1;
+        }
+        if ((w << 6) <= floor + 1) return -1;
+        --w;
+        m = bm[w];
+    }
+}
+
+GPJ_HD uint32_t read_varint(const uint8_t* ir, int& pc) {
+    uint32_t v = 0;
+    int shift = 0;
+    uint32_t b;
+    while ((b = ir[pc++]) & 0x80u) {
+        v |= (b & 0x7Fu) << shift;
+        shift += 7;
+    }
+    return v | (b << shift);
+}
+
+// Runs validated bytecode `ir` on the line [line_start, line_end) and writes
+// (start, end) pairs to res[2*k], res[2*k+1] for the k-th STORE_RESULT.
+// res must hold -1 on entry.
+GPJ_HD void run_line(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
+                     int64_t* res) {
+    int64_t level_ends[kLevelSlots];
+    int64_t current_index[kLevelSlots];
+    level_ends[0] = line_end;
+#pragma unroll
+    for (int k = 1; k < kLevelSlots; k++) level_ends[k] = -1;
+#pragma unroll
+    for (int k = 0; k < kLevelSlots; k++) current_index[k] = -1;
+
+    const uint8_t* file = v.file;
+    const int64_t n = v.n;
+    int pc = 0, cur = 0, result_index = 0;
+    uint8_t type = 0xFF;
+    int64_t want_len = 0, want_index = -1;
+    const uint8_t* want = nullptr;
+    bool execute = true;
+
+    int64_t j = line_start;
+    while (j < level_ends[cur] && j < n) {
+        while (execute) {
+            type = ir[pc++];
+            switch (type) {
+                case 0:  // END
+                    return;
+                case 1:  // STORE_RESULT (find_value.cu:59-82)
+                    while (j < n && is_ws(file[j])) ++j;  // [bounded] stops at end of file
+                    res[2 * result_index] = j;
+                    res[2 * result_index + 1] = level_ends[cur];
+                    ++result_index;
+                    break;
+                case 2:  // MOVE_UP (:83-90)
+                    if (level_ends[cur] < 0) return;  // [bounded] would continue at j=-1
+                    j = level_ends[cur];
+                    level_ends[cur] = -1;
+                    --cur;
+                    break;
+                case 3: {  // MOVE_DOWN (:91-111): end of the value = next structural one level up
+                    ++cur;
+                    if (level_ends[cur] == -1) {
+                        const int64_t lim = level_ends[cur - 1];
+                        const int64_t m = next_bit(v.levels + v.level_size * (cur - 1), j + 1, lim);
+                        if (m < lim) level_ends[cur] = m;
+                    }
+                    break;
+                }
+                case 4:  // MOVE_TO_KEY (:112-130)
+                    want_len = read_varint(ir, pc);
+                    want = ir + pc;
+                    pc += static_cast<int>(want_len);
+                    execute = false;
+                    break;
+                case 5:  // MOVE_TO_INDEX (:131-169)
+                    want_index = read_varint(ir, pc);
+                    if (current_index[cur] == -1) {
+                        for (;;) {  // [bounded] only whitespace may precede '['
+                            if (j >= n) return;
+                            const uint8_t c = file[j];
+                            if (c == '[') break;
+                            if (!is_ws(c)) return;
+                            ++j;
+                        }
+                        current_index[cur] = 0;
+                    }
+                    if (want_index == 0) {
+                        ++j;
+                        execute = true;
+                    } else {
+                        execute = false;
+                    }
+                    break;
+                case 6: {  // EXPRESSION_STRING_EQUALS (:170-210)
+                    want_len = read_varint(ir, pc);
+                    want = ir + pc;
+                    pc += static_cast<int>(want_len);
+                    while (j < n && is_ws(file[j])) ++j;  // [bounded]
+                    if (level_ends[cur] - j != want_len) return;
+                    for (int64_t k = 0; k < want_len; k++)
+                        if (want[k] != file[j + k]) return;
+                    break;
+                }
+                default:
+                    return;
+            }
+        }
+
+        // Searching: j is a candidate position ([bounded] only inside the file).
+        if (j < n) {
+            const uint64_t* lv = v.levels + v.level_size * cur;
+            const bool structural = (lv[j >> 6] >> (j & 63)) & 1u;
+            if (type == 4) {  // key match at a structural ':' (:225-251)
+                if (structural && file[j] == ':') {
+                    const int64_t string_end = prev_bit(v.string_index, j - 1, line_start);
+                    const int64_t string_start = string_end - want_len;
+                    if (string_start >= line_start && file[string_start] == '"') {
+                        bool same = true;
+                        for (int64_t k = 0; k < want_len; k++) {
+                            if (want[k] != file[string_start + k + 1]) {
+                                same = false;
+                                break;
+                            }
+                        }
+                        execute = same;
+                    }
+                }
+            } else if (type == 5) {  // index match at a structural ',' (:252-259)
+                if (structural && file[j] == ',') {
+                    ++current_index[cur];
+                    if (want_index == current_index[cur]) execute = true;
+                }
+            }
+        }
+        ++j;
+        if (!execute) {
+            // Nothing happens until the next structural bit of this level.
+            const int64_t lim = level_ends[cur] < n ? level_ends[cur] : n;
+            if (j < lim) j = next_bit(v.levels + v.level_size * cur, j, lim);
+        }
+    }
+}
+
+}  // namespace gpj

@@ -1,0 +1,28 @@
+// Host-side interface of the find_value kernel (query_kernel.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace gpj {
+
+struct QueryParams {
+    const uint8_t* file;
+    int64_t n;
+    const int64_t* newlines;
+    int64_t num_lines;
+    const uint64_t* string_index;
+    const uint64_t* leveled;
+    int64_t level_size;
+    const uint8_t* bytecode;  // all queries back to back
+    const int32_t* offsets;   // start of query q in `bytecode`
+    int num_queries;
+    int slots;     // result slots per line (max num_results)
+    int64_t* out;  // [num_queries][num_lines][slots][2]
+};
+
+cudaError_t launch_find_value(const QueryParams& p, int grid, cudaStream_t stream);
+int find_value_max_ctas_per_sm();
+
+}  // namespace gpj

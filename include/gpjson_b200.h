@@ -1,0 +1,207 @@
+/*
+ * gpjson_b200.h — C ABI of the B200-native GPJSON structural-index and
+ * JSONPath query path.
+ *
+ * This library replaces the layer under GPJSON's `query(file, jsonpath)`
+ * (gpjson/src/main/java/com/koenv/gpjson/functions/QueryFunction.java:48-265):
+ * the grCUDA-derived runtime that reached libcudart/libcuda/libnvrtc through
+ * Truffle NFI (gpu/CUDARuntime.java:76-94, gpu/CUDARuntimeFunction.java:39-186),
+ * the index stages with their host-side carry scans (stages/CombinedIndex.java,
+ * stages/LeveledBitmapsIndex.java) and the per-query find_value launches.
+ * A Java caller binds these symbols with the Panama FFM API; Python binds them
+ * with ctypes (gpjson_b200/_lib.py).
+ *
+ * Conventions
+ *  - Every function returning int returns GPJ_OK (0) or a negative GPJ_E*
+ *    code and never aborts the process.  The message of the last failure on a
+ *    context is available from gpj_last_error().
+ *  - Offsets are int64; -1 marks a miss (QueryFunction.java:197).
+ *  - Host output buffers are owned by the caller; device buffers are owned by
+ *    the gpj_file they belong to, except where a function takes device
+ *    pointers explicitly.
+ *  - One gpj_ctx must not be used by two threads at the same time.
+ *  - All device work of a context runs on one CUDA stream (gpj_set_stream).
+ */
+#ifndef GPJSON_B200_H
+#define GPJSON_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Exported even when the library is built with -fvisibility=hidden. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define GPJ_OK 0
+#define GPJ_EINVAL (-1)       /* bad argument: null pointer, size, alignment */
+#define GPJ_EPARSE (-2)       /* JSONPathException (jsonpath/JSONPathException.java) */
+#define GPJ_EUNSUPPORTED (-3) /* UnsupportedJSONPathException; GPJSON would fall back to
+                                 Jayway JsonPath on the CPU (QueryFunction.java:122-128),
+                                 which this library does not provide */
+#define GPJ_ECUDA (-4)        /* a CUDA runtime call failed (GPJSONException.java:64-70) */
+#define GPJ_ENOMEM (-5)       /* device or pinned-host allocation failed */
+#define GPJ_EIO (-6)          /* the input file could not be opened or read */
+#define GPJ_ELIMIT (-7)       /* a documented limit was exceeded */
+#define GPJ_EDEVICE (-8)      /* a kernel reported an error word (bounded wait expired) */
+#define GPJ_ESTATE (-9)       /* object not in the state the call needs */
+
+/* Limits kept from the reference. */
+#define GPJ_MAX_QUERIES 255   /* QueryFunction.java:74-77 */
+#define GPJ_MAX_LEVELS 16     /* LeveledBitmapsIndex.java:168,183-185 */
+
+typedef struct gpj_ctx gpj_ctx;
+typedef struct gpj_file gpj_file;
+typedef struct gpj_result gpj_result;
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Creates a context on CUDA device `device` (GPJSONContext.java:48-54 and the
+ * CUDARuntime constructor, CUDARuntime.java:76-94).  Kernels are compiled
+ * ahead of time for sm_100a, so there is no run-time NVRTC step
+ * (CUDARuntime.java:267-289). */
+int gpj_create(int device, gpj_ctx **out);
+void gpj_destroy(gpj_ctx *ctx);
+
+/* Message of the last failure on `ctx` (or of the last failed gpj_create when
+ * ctx is NULL).  Valid until the next call on the same context. */
+const char *gpj_last_error(const gpj_ctx *ctx);
+
+/* Runs all later device work of `ctx` on `stream` (a cudaStream_t; NULL =
+ * the context's own stream).  The reference runs everything synchronously on
+ * the legacy default stream (CUDARuntime.java:388). */
+int gpj_set_stream(gpj_ctx *ctx, void *stream);
+
+/* Library version string, e.g. "gpjson_b200 0.1 sm_100a". */
+const char *gpj_version(void);
+
+/* ---- JSONPath compiler --------------------------------------------------- */
+
+/* Compiles `path` (NUL-terminated UTF-8) to GPJSON bytecode, byte-identical to
+ * JSONPathParser.compile() (jsonpath/JSONPathParser.java:20-29).
+ * On success writes the bytecode (at most `cap` bytes) to `out`, its length to
+ * *len, JSONPathResult.getMaxDepth() to *max_depth and getNumResults() to
+ * *num_results.  On GPJ_EPARSE / GPJ_EUNSUPPORTED a message is written to
+ * `err` (at most err_cap bytes, NUL-terminated) when err is not NULL.
+ * Returns GPJ_ELIMIT when the bytecode does not fit in `cap`. */
+int gpj_compile(const char *path, uint8_t *out, size_t cap, size_t *len, int *max_depth,
+                int *num_results, char *err, size_t err_cap);
+
+/* ---- input files ---------------------------------------------------------- */
+
+/* Reads a whole NDJSON file into device memory (QueryFunction.readFile,
+ * QueryFunction.java:316-335) through pinned staging buffers and async copies. */
+int gpj_file_open(gpj_ctx *ctx, const char *filename, gpj_file **out);
+
+/* Copies `n` bytes of host memory into device memory as an input file. */
+int gpj_file_from_host(gpj_ctx *ctx, const void *data, int64_t n, gpj_file **out);
+
+/* Wraps `n` bytes that are already in device memory (not copied, not freed).
+ * `d_data` must be 16-byte aligned and stay valid until gpj_file_release. */
+int gpj_file_from_device(gpj_ctx *ctx, const void *d_data, int64_t n, gpj_file **out);
+
+/* Frees the file's device buffers (input copy, index, results). */
+void gpj_file_release(gpj_file *file);
+
+int64_t gpj_file_size(const gpj_file *file);
+
+/* ---- structural index ------------------------------------------------------ */
+
+/* Builds the newline index, the string (in-string) bitmap and `num_levels`
+ * leveled structural bitmaps of `file` in one pass over the input
+ * (CombinedIndex.create, CombinedIndex.java:28-56, and
+ * LeveledBitmapsIndex.create, LeveledBitmapsIndex.java:40-54, including their
+ * host-side carry scans :98-115, :129-151 and :68-87, which run on the device
+ * here).  1 <= num_levels <= GPJ_MAX_LEVELS.  Synchronous: on return the
+ * index is complete and the line count is known. */
+int gpj_index_build(gpj_ctx *ctx, gpj_file *file, int num_levels);
+
+/* Number of lines = newline-index entries = '\n' count + 1. */
+int gpj_index_num_lines(const gpj_file *file, int64_t *lines);
+
+/* Copies the index to host memory: newline index (int64[lines]: [0]=0 then
+ * every '\n' offset), string index (uint64[ceil(n/64)]) and leveled bitmaps
+ * (uint64[num_levels][ceil(n/64)], level-major).  `count` is the number of
+ * elements the host buffer holds; it must be at least the index size. */
+int gpj_index_copy_newlines(gpj_ctx *ctx, const gpj_file *file, int64_t *host, int64_t count);
+int gpj_index_copy_string_index(gpj_ctx *ctx, const gpj_file *file, uint64_t *host,
+                                int64_t count);
+int gpj_index_copy_leveled_bitmaps(gpj_ctx *ctx, const gpj_file *file, uint64_t *host,
+                                   int64_t count);
+
+/* Device-side stage entry: builds the same index from caller-owned device
+ * buffers, the way the reference's stage tests drive CombinedIndex and
+ * LeveledBitmapsIndex on raw device pointers (StringIndexTest.java,
+ * NewlineIndexTest.java, LeveledBitmapsIndexTest.java).
+ * d_file: n bytes, 16-byte aligned.  d_string_index: ceil(n/64) words.
+ * d_leveled: num_levels*ceil(n/64) words.  d_newlines: newline_cap entries.
+ * *num_lines receives the line count; when it exceeds newline_cap only the
+ * first newline_cap entries were written and GPJ_ELIMIT is returned. */
+int gpj_build_index_device(gpj_ctx *ctx, const void *d_file, int64_t n, int num_levels,
+                           uint64_t *d_string_index, uint64_t *d_leveled, int64_t *d_newlines,
+                           int64_t newline_cap, int64_t *num_lines);
+
+/* ---- queries ---------------------------------------------------------------- */
+
+/* Evaluates `nq` compiled queries (bytecode from gpj_compile) over every line
+ * of an indexed file in one pass, all queries of a line handled together.
+ * Results are identical to running each query alone (the reference reuses
+ * one result buffer across queries, QueryFunction.java:194-201, so lines a
+ * later query misses keep an earlier query's offsets; this library does not).
+ * `result_slots` must be at least every query's num_results; the output
+ * layout is int64[nq][lines][result_slots][2] = (start, end) byte offsets,
+ * -1 for a miss (find_value.cu result layout, QueryFunction.java:194).
+ * The file must be indexed with at least max(max_depth) levels. */
+int gpj_query(gpj_ctx *ctx, gpj_file *file, int nq, const uint8_t *const *bytecode,
+              const size_t *bytecode_len, int result_slots, int64_t *host_out,
+              int64_t out_count);
+
+/* Same as gpj_query but writes the results to caller-owned device memory
+ * `d_out` (same layout) and does not synchronise the stream. */
+int gpj_query_device(gpj_ctx *ctx, gpj_file *file, int nq, const uint8_t *const *bytecode,
+                     const size_t *bytecode_len, int result_slots, int64_t *d_out,
+                     int64_t out_count);
+
+/* The whole reference call query(file, paths) (QueryFunction.call,
+ * QueryFunction.java:48-265) on an opened file: compiles the paths, builds
+ * the index with max(max_depth) levels (reusing an index that has enough
+ * levels), runs all queries in one pass and copies the offsets to the host.
+ * Path errors return GPJ_EPARSE ("Failed to parse JSON path (i)") or
+ * GPJ_EUNSUPPORTED ("Unsupported JSON path (i)"). */
+int gpj_query_paths(gpj_ctx *ctx, gpj_file *file, int nq, const char *const *paths,
+                    gpj_result **out);
+
+/* Result of gpj_query_paths: the Result/ResultArray/ResultItem layout
+ * (result/Result.java:23-29): [query][line][slot] -> (start, end). */
+int64_t gpj_result_num_queries(const gpj_result *r);
+int64_t gpj_result_num_lines(const gpj_result *r);
+int gpj_result_slots(const gpj_result *r);
+/* Pointer to int64[num_queries][num_lines][slots][2], valid until release. */
+const int64_t *gpj_result_offsets(const gpj_result *r);
+void gpj_result_release(gpj_result *r);
+
+/* ---- diagnostics ---------------------------------------------------------- */
+
+/* Phase timings of the context as JSON (the role of Timings.export,
+ * debug/Timings.java:50-88, with CUDA-event device times).  Writes at most
+ * cap bytes including the NUL; *len receives the full length. */
+int gpj_get_timings(gpj_ctx *ctx, char *json, size_t cap, size_t *len);
+void gpj_reset_timings(gpj_ctx *ctx);
+
+/* Number of kernels this context has launched since creation. */
+int64_t gpj_kernel_launches(const gpj_ctx *ctx);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPJSON_B200_H */

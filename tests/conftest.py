@@ -1,0 +1,58 @@
+"""Shared fixtures.  Tests marked `gpu` need a B200 and run the native
+library; everything else runs on the CPU (oracle, compiler, host logic,
+host-compiled device arithmetic)."""
+
+from __future__ import annotations
+
+import ctypes
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+GOLDEN = ROOT / "tests" / "golden"
+FIXTURES = GOLDEN / "fixtures"
+HOSTSIM_SRC = ROOT / "tests" / "hostsim" / "hostsim.cpp"
+HOSTSIM_LIB = ROOT / "tests" / "hostsim" / "libhostsim.so"
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA sm_100 GPU and the native library")
+
+
+@pytest.fixture(scope="session")
+def hostsim():
+    """The device code's arithmetic compiled for the host (test-only)."""
+    deps = [HOSTSIM_SRC] + list((ROOT / "gpjson_b200" / "csrc").glob("*.cuh"))
+    if not HOSTSIM_LIB.exists() or any(d.stat().st_mtime > HOSTSIM_LIB.stat().st_mtime for d in deps):
+        subprocess.run(
+            ["g++", "-std=c++17", "-O2", "-shared", "-fPIC", "-o", str(HOSTSIM_LIB), str(HOSTSIM_SRC)], check=True
+        )
+    L = ctypes.CDLL(str(HOSTSIM_LIB))
+    P = ctypes.c_void_p
+    L.hs_build_index.restype = ctypes.c_int64
+    L.hs_build_index.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P, P, ctypes.c_int64]
+    L.hs_find_values.restype = None
+    L.hs_find_values.argtypes = [P, ctypes.c_int64, P, ctypes.c_int64, P, P, ctypes.c_int, P, ctypes.c_int, P]
+    L.hs_escaped_mask.restype = ctypes.c_uint64
+    L.hs_escaped_mask.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+    return L
+
+
+@pytest.fixture(scope="session")
+def gpjson():
+    """A native GPJSON context on cuda:0 (GPU tests only)."""
+    import gpjson_b200 as gj
+
+    g = gj.GPJSON(0)
+    yield g
+    g.close()
+
+
+def fixture_bytes(rel: str) -> bytes:
+    return (FIXTURES / rel).read_bytes()

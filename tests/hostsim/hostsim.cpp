@@ -1,0 +1,137 @@
+// Test-only CPU harness: runs the device code's per-word arithmetic
+// (gpjson_b200/csrc/word_ops.cuh) and line interpreter (interp.cuh) on the
+// host, in the same tile/word decomposition the index kernel uses, so the
+// test suite can compare them with the oracle without a GPU.  It is built
+// by tests/conftest.py and never used by the library.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../../gpjson_b200/csrc/interp.cuh"
+#include "../../gpjson_b200/csrc/word_ops.cuh"
+
+using namespace gpj;
+
+namespace {
+constexpr int64_t kTileBytes = 16384;
+constexpr int kWordsPerTile = kTileBytes / 64;
+
+uint32_t load_u32(const uint8_t* f, int64_t n, int64_t pos) {
+    uint32_t v = 0;
+    for (int b = 0; b < 4; b++) {
+        const int64_t p = pos + b;
+        if (p < n) v |= static_cast<uint32_t>(f[p]) << (8 * b);
+    }
+    return v;
+}
+
+int backslash_run_parity_before(const uint8_t* f, int64_t pos, int64_t floor) {
+    int64_t k = pos - 1, run = 0;
+    while (k >= floor && f[k] == '\\') {
+        ++run;
+        --k;
+    }
+    return static_cast<int>(run & 1);
+}
+}  // namespace
+
+extern "C" {
+
+// Mirrors the index kernel: per tile, word summaries with a local string
+// state of 0, an exclusive compose-scan inside the tile, a sequential prefix
+// over tiles (the kernel's look-back), then the final masks per word.
+int64_t hs_build_index(const uint8_t* f, int64_t n, int num_levels, uint64_t* str_out,
+                       uint64_t* lvl_out, int64_t* nl_out, int64_t nl_cap) {
+    const int64_t level_size = (n + 63) / 64;
+    const int64_t ntiles = (n + kTileBytes - 1) / kTileBytes;
+    int s_state = 0;
+    int64_t d_state = -1, nl_state = 0;
+    if (nl_cap > 0) nl_out[0] = 0;
+    std::vector<ClassMasks> masks(kWordsPerTile);
+    std::vector<uint64_t> esc(kWordsPerTile), p0(kWordsPerTile);
+    std::vector<Span> excl(kWordsPerTile);
+    for (int64_t t = 0; t < ntiles; t++) {
+        const int64_t tile_start = t * kTileBytes;
+        const int tile_parity = backslash_run_parity_before(f, tile_start, 0);
+        Span acc = span_identity();
+        for (int w = 0; w < kWordsPerTile; w++) {
+            const int64_t ws = tile_start + 64 * w;
+            uint32_t v[16];
+            for (int k = 0; k < 16; k++) v[k] = ws < n ? load_u32(f, n, ws + 4 * k) : 0;
+            masks[w] = classify64(v);
+            // escape carry: backslash run inside the tile, then before it
+            int64_t k = ws - 1, run = 0;
+            while (k >= tile_start && f[k] == '\\') {
+                ++run;
+                --k;
+            }
+            uint32_t cin = static_cast<uint32_t>(run & 1);
+            if (k < tile_start) cin ^= static_cast<uint32_t>(tile_parity);
+            uint32_t cout;
+            const uint64_t e = escaped_mask(masks[w].backslash, cin, &cout);
+            const uint64_t qr = masks[w].quote & ~e;
+            p0[w] = prefix_xor(qr);
+            Span sp;
+            sp.q = popc64(qr) & 1;
+            sp.dd0 = popc64(masks[w].open & ~p0[w]) - popc64(masks[w].close & ~p0[w]);
+            sp.ddt = popc64(masks[w].open) - popc64(masks[w].close);
+            sp.nl = popc64(masks[w].newline);
+            excl[w] = acc;
+            acc = span_compose(acc, sp);
+        }
+        // tile prefix (state before the tile) is (s_state, d_state, nl_state)
+        for (int w = 0; w < kWordsPerTile; w++) {
+            const int64_t ws = tile_start + 64 * w;
+            if (ws >= n) break;
+            const int64_t word = ws / 64;
+            const int s_w = s_state ^ excl[w].q;
+            const int64_t d_w = d_state + (s_state ? (excl[w].ddt - excl[w].dd0) : excl[w].dd0);
+            uint64_t in_str = p0[w] ^ (s_w ? ~0ull : 0ull);
+            const int64_t valid = n - ws < 64 ? n - ws : 64;
+            if (valid < 64) in_str &= (1ull << valid) - 1;
+            str_out[word] = in_str;
+            uint64_t lv[16];
+            split_levels<16>(masks[w].open & ~in_str, masks[w].close & ~in_str,
+                             masks[w].structural & ~in_str, d_w, lv);
+            for (int l = 0; l < num_levels; l++) lvl_out[l * level_size + word] = lv[l];
+            int64_t idx = 1 + nl_state + excl[w].nl;
+            uint64_t nm = masks[w].newline;
+            while (nm) {
+                const int p = ctz64(nm);
+                if (idx < nl_cap) nl_out[idx] = ws + p;
+                ++idx;
+                nm &= nm - 1;
+            }
+        }
+        // apply the tile aggregate
+        const int s_old = s_state;
+        s_state ^= acc.q;
+        d_state += s_old ? (acc.ddt - acc.dd0) : acc.dd0;
+        nl_state += acc.nl;
+    }
+    return nl_state + 1;
+}
+
+// Runs each query's bytecode on every line with the device interpreter.
+// out: [nq][lines][slots][2], filled with -1 here.
+void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t lines,
+                    const uint64_t* str, const uint64_t* lvl, int nq, const uint8_t* const* irs,
+                    int slots, int64_t* out) {
+    LineView v{f, n, str, lvl, (n + 63) / 64};
+    const int64_t per_query = lines * slots * 2;
+    for (int64_t k = 0; k < per_query * nq; k++) out[k] = -1;
+    for (int q = 0; q < nq; q++) {
+        for (int64_t i = 0; i < lines; i++) {
+            const int64_t start = nl[i];
+            const int64_t end = i + 1 < lines ? nl[i + 1] : n;
+            run_line(v, start, end, irs[q], out + q * per_query + i * slots * 2);
+        }
+    }
+}
+
+// Escape-mask check on one word against a byte loop.
+uint64_t hs_escaped_mask(uint64_t bs, uint32_t cin, uint32_t* cout) {
+    return escaped_mask(bs, cin, cout);
+}
+
+}  // extern "C"

@@ -1,0 +1,110 @@
+"""The C ABI library loads, exports every entry point include/gpjson_b200.h
+declares, binds them all in Python, and behaves without a GPU (compiler
+calls work; context creation fails with a status, never a crash)."""
+
+from __future__ import annotations
+
+import re
+import subprocess
+
+import pytest
+
+import gpjson_b200 as gj
+from gpjson_b200 import _lib
+from tests.conftest import ROOT
+
+HEADER = ROOT / "include" / "gpjson_b200.h"
+
+
+def declared_functions() -> set[str]:
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    return set(re.findall(r"\b(gpj_[a-z_0-9]+)\s*\(", text))
+
+
+def exported_symbols() -> set[str]:
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)], check=True, capture_output=True,
+                         text=True).stdout
+    return {line.split()[-1] for line in out.splitlines() if " T " in line}
+
+
+def test_library_exports_every_declared_symbol():
+    declared = declared_functions()
+    assert len(declared) >= 25
+    exported = exported_symbols()
+    assert declared <= exported, declared - exported
+    # nothing but the declared API leaks out of the library
+    assert {s for s in exported if s.startswith("gpj")} == declared
+
+
+def test_python_binding_covers_header():
+    assert set(_lib.SIGNATURES) == declared_functions()
+    lib = _lib.load()
+    for name in _lib.SIGNATURES:
+        assert getattr(lib, name) is not None
+
+
+def test_version_and_compile_without_gpu():
+    lib = _lib.load()
+    assert b"sm_100a" in lib.gpj_version()
+    c = gj.compile_path("$.user.lang")
+    assert c.bytecode[0] == 4 and c.max_depth == 2
+
+
+def test_null_arguments_are_rejected():
+    lib = _lib.load()
+    assert lib.gpj_create(0, None) == _lib.GPJ_EINVAL
+    assert lib.gpj_index_num_lines(None, None) == _lib.GPJ_EINVAL
+    assert lib.gpj_get_timings(None, None, 0, None) == _lib.GPJ_EINVAL
+    assert lib.gpj_kernel_launches(None) == -1
+    lib.gpj_file_release(None)
+    lib.gpj_result_release(None)
+    lib.gpj_destroy(None)
+
+
+def test_context_creation_reports_status():
+    try:
+        import torch
+
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if has_gpu:
+        pytest.skip("a GPU is present; covered by the gpu tests")
+    with pytest.raises(gj.GPJSONException) as ei:
+        gj.GPJSON(0)
+    assert ei.value.code in (_lib.GPJ_ECUDA, _lib.GPJ_ENOMEM)
+    assert "CUDA error" in str(ei.value) or "sm_100" in str(ei.value)
+
+
+def test_query_argument_handling():
+    with pytest.raises(gj.GPJSONException, match="255"):
+        gj.prepare_queries(["$.a"] * 256)
+    with pytest.raises(gj.GPJSONException, match="at least one"):
+        gj.prepare_queries([])
+    with pytest.raises(gj.GPJSONException, match="string or string array"):
+        gj.prepare_queries(3)
+    with pytest.raises(gj.GPJSONException, match="string or string array"):
+        gj.prepare_queries(["$.a", 3])
+    with pytest.raises(gj.UnsupportedJSONPathException, match=r"Unsupported JSON path \(1, fallback disabled\)"):
+        gj.prepare_queries(["$.a", "$[*]"], {"disable_fallback": True})
+    with pytest.raises(gj.JSONPathException, match=r"Failed to parse JSON path \(0\)"):
+        gj.prepare_queries(["$.a b"])
+    with pytest.raises(gj.GPJSONException, match="levels"):
+        gj.prepare_queries("$" + ".a" * 17)
+    paths, compiled = gj.prepare_queries(("$.a", "$.b[0:2]"))
+    assert paths == ["$.a", "$.b[0:2]"] and [c.num_results for c in compiled] == [1, 2]
+
+
+def test_result_views_follow_reference_layout():
+    import numpy as np
+
+    data = b'{"a":"x"}\n{"a":12}\n{"b":1}'
+    offs = np.array([[[[5, 8]], [[15, 17]], [[-1, -1]]]], dtype=np.int64)
+    r = gj.Result(offs, data, ["$.a"])
+    assert len(r) == 1 and len(r[0]) == 3 and len(r[0][0]) == 1
+    assert [r[0][i][0] for i in range(3)] == ['"x"', "12", None]
+    assert r[-1][-1][-1] is None
+    with pytest.raises(IndexError):
+        r[1]
+    with pytest.raises(IndexError):
+        r[0][3]

@@ -1,0 +1,147 @@
+"""GPU parity of the query path (index + fused find_value) against the
+oracle: the reference's end-to-end known answers (QueryFunctionTest.java),
+fused-versus-alone equality, generated NDJSON of the benchmark shapes and
+random small documents with many path shapes."""
+
+from __future__ import annotations
+
+import random
+
+import numpy as np
+import pytest
+
+import gpjson_b200 as gj
+from gpjson_b200 import datagen
+from oracle import oracle
+from tests.conftest import FIXTURES, fixture_bytes
+from tests.test_gpu_index import adversarial_bytes
+from tests.test_oracle import KNOWN_ANSWERS, NOT_FOUND, SIMPLE
+
+TWEET_PATHS = ["$.user.lang", "$.id", "$.user.followers_count", "$.entities.hashtags[0].text"]
+ADV_PATHS = ["$.a.b.c.d", "$.arr[5]", "$.x[0].y[2].z"]
+
+
+def flat_values(result: gj.Result) -> list:
+    out = []
+    for q in range(len(result)):
+        arr = result[q]
+        for line in range(len(arr)):
+            out.extend(arr[line][k] for k in range(len(arr[line])))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path,expected", KNOWN_ANSWERS, ids=[k[0] for k in KNOWN_ANSWERS])
+def test_known_answers(gpjson, path, expected):
+    result = gpjson.query(str(FIXTURES / SIMPLE), path)
+    assert flat_values(result) == expected
+
+
+@pytest.mark.gpu
+def test_key_not_found_in_current_level(gpjson):
+    result = gpjson.query(str(FIXTURES / NOT_FOUND), "$.a.a")
+    assert all(v is None for v in flat_values(result))
+
+
+@pytest.mark.gpu
+def test_multiple_paths_one_call(gpjson):
+    paths = [k[0] for k in KNOWN_ANSWERS]
+    result = gpjson.query(str(FIXTURES / SIMPLE), paths)
+    assert len(result) == len(paths)
+    slots = max(len(k[1]) for k in KNOWN_ANSWERS)
+    for q, (_, expected) in enumerate(KNOWN_ANSWERS):
+        got = [result[q][0][k] for k in range(slots)]
+        assert got == expected + [None] * (slots - len(expected))
+
+
+def run_gpu(gpjson, data: bytes, paths: list[str]) -> np.ndarray:
+    compiled = [gj.compile_path(p) for p in paths]
+    f = gpjson.load_bytes(data)
+    try:
+        f.build_index(max(c.max_depth for c in compiled))
+        return f.run(compiled)
+    finally:
+        f.release()
+
+
+@pytest.mark.gpu
+def test_fused_equals_alone_and_oracle_tweets(gpjson):
+    data = datagen.tweets(32 << 20).tobytes()
+    fused = run_gpu(gpjson, data, TWEET_PATHS)
+    want = oracle.query(data, TWEET_PATHS, mt=True)
+    assert np.array_equal(fused, want)
+    for q, p in enumerate(TWEET_PATHS):
+        alone = run_gpu(gpjson, data, [p])
+        assert np.array_equal(alone[0], fused[q]), p
+
+
+@pytest.mark.gpu
+def test_adversarial_against_oracle(gpjson):
+    data = adversarial_bytes(48 << 20)
+    got = run_gpu(gpjson, data, ADV_PATHS)
+    want = oracle.query(data, ADV_PATHS, mt=True)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_random_documents_many_paths(gpjson):
+    rng = random.Random(11)
+    base = [
+        fixture_bytes(SIMPLE),
+        b'{"a": {"b": "a"},"b": {"a": "c" }}',
+        b'{"a":[1,[2,3],{"b":4}],"c":{"d":[]}}',
+        b'{"a" :[ {"b":[0,1,{"c":"x"}]} , 7 ], "d": "\\"a\\":1"}',
+        b'  {"k\\"ey": 1, "key": [ ], "x":{"y":[[],[1]]}}  ',
+    ]
+    paths = [
+        "$.user.lang", "$.user.values[2]", "$.user.values[0:3]", "$.a.a", "$.a[1][0]", "$.a[2].b",
+        "$.c.d[0]", "$.c.d[0:2]", "$.user.lang[?(@ == 'nl')]", "$[0]", "$.b.a", "$.a[0].b[2].c",
+        "$.key[0]", "$.x.y[1][0]", "$.x.y[0:2]", "$['k\\\"ey']", "$.d",
+    ]
+    lines = []
+    for _ in range(20000):
+        if rng.random() < 0.9:
+            lines.append(rng.choice(base))
+        else:
+            lines.append(bytes(rng.choice(b'{}[]:,"\\ ab') for _ in range(rng.randint(0, 80))))
+    data = b"\n".join(lines)
+    got = run_gpu(gpjson, data, paths)
+    want = oracle.query(data, paths)
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_empty_and_tiny_files(gpjson, tmp_path):
+    for data in [b"", b"\n", b"{}", b'{"a":1}\n{"a":2}\n', b"\n\n\n"]:
+        got = run_gpu(gpjson, data, ["$.a"])
+        want = oracle.query(data, ["$.a"])
+        assert np.array_equal(got, want), data
+
+
+@pytest.mark.gpu
+def test_index_zero_of_empty_array_quirk(gpjson, tmp_path):
+    # [0] as the last step on [] stores (position of ']', -1) like find_value.cu;
+    # reading that item fails like ResultItem.java (negative length).
+    p = tmp_path / "q.ldjson"
+    p.write_bytes(b'{"a": []}\n{"a": [5]}')
+    result = gpjson.query(str(p), "$.a[0]")
+    start, end = result[0][0].offsets(0)
+    assert end == -1 and p.read_bytes()[start:start + 1] == b"]"
+    with pytest.raises(gj.GPJSONException):
+        result[0][0][0]
+    assert result[0][1][0] == "5"
+
+
+@pytest.mark.gpu
+def test_errors(gpjson):
+    path = str(FIXTURES / SIMPLE)
+    with pytest.raises(gj.UnsupportedJSONPathException):
+        gpjson.query(path, "$.a[*]")
+    with pytest.raises(gj.JSONPathException):
+        gpjson.query(path, "$.a b")
+    with pytest.raises(gj.GPJSONException):
+        gpjson.query(path, ["$.a"] * 256)
+    with pytest.raises(gj.GPJSONException):
+        gpjson.query(path, "$" + ".a" * 17)
+    with pytest.raises(gj.GPJSONException):
+        gpjson.query(str(FIXTURES / "does-not-exist.ldjson"), "$.a")

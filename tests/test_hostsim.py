@@ -1,0 +1,116 @@
+"""The device code's arithmetic (word_ops.cuh, interp.cuh) compiled for the
+host and run in the index kernel's tile/word decomposition, against the
+oracle.  Catches logic errors without a GPU; the same sources are compiled
+for sm_100a into the product library."""
+
+from __future__ import annotations
+
+import ctypes
+import random
+
+import numpy as np
+import pytest
+
+from gpjson_b200 import datagen
+from oracle import oracle
+from tests.conftest import fixture_bytes
+from tests.test_gpu_index import FIXTURE_NAMES, adversarial_bytes
+
+
+def hs_index(hostsim, data: bytes, levels: int):
+    f = np.frombuffer(data, dtype=np.uint8)
+    n = f.size
+    words = (n + 63) // 64
+    nl = np.zeros(n + 1, np.int64)
+    st = np.zeros(max(words, 1), np.uint64)
+    lv = np.zeros(max(words * levels, 1), np.uint64)
+    cnt = hostsim.hs_build_index(f.ctypes.data, n, levels, st.ctypes.data, lv.ctypes.data, nl.ctypes.data, n + 1)
+    return nl[:cnt], st[:words], lv[: words * levels].reshape(levels, words)
+
+
+def check_index(hostsim, data: bytes, levels: int):
+    want = oracle.Index(data, levels)
+    nl, st, lv = hs_index(hostsim, data, levels)
+    assert np.array_equal(nl, want.newlines)
+    assert np.array_equal(st, want.strings)
+    assert np.array_equal(lv, want.levels)
+
+
+def test_escape_mask_random_words(hostsim):
+    rng = random.Random(7)
+    for it in range(20000):
+        bs = rng.getrandbits(64) | (rng.getrandbits(64) if it % 2 else 0)
+        if it % 97 == 0:
+            bs = (1 << 64) - 1
+        cin = rng.getrandbits(1)
+        cout = ctypes.c_uint32()
+        got = hostsim.hs_escaped_mask(bs, cin, ctypes.byref(cout))
+        e, want = cin, 0
+        for i in range(64):
+            if e:
+                want |= 1 << i
+            e = (1 - e) if (bs >> i) & 1 else 0
+        keep = ~bs & ((1 << 64) - 1)  # exact on every byte that is not a backslash
+        assert (got & keep) == (want & keep)
+        assert cout.value == e
+
+
+@pytest.mark.parametrize("rel", FIXTURE_NAMES)
+def test_fixtures(hostsim, rel):
+    check_index(hostsim, fixture_bytes(rel), 16)
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_structured_bytes(hostsim, seed):
+    rng = random.Random(seed)
+    alphabet = b'{}[]:,"\\\n ab' if seed % 2 else b'\\\\\\"\n{}[]:,a '
+    for n in [0, 1, 63, 64, 65, 16383, 16384, 16385, 50000]:
+        data = bytes(rng.choice(alphabet) for _ in range(n))
+        check_index(hostsim, data, rng.choice([1, 3, 16]))
+
+
+def test_tile_straddling_escapes(hostsim):
+    # backslash runs ending exactly at, before and after 16 KiB tile starts
+    for run in range(1, 9):
+        for shift in range(-3, 4):
+            pre = b"a" * (16384 - run + shift)
+            data = pre + b"\\" * run + b'"x"{"k":[1,2]}\n' + b"y" * 100
+            check_index(hostsim, data, 3)
+
+
+def test_generated(hostsim):
+    check_index(hostsim, datagen.tweets(1 << 20).tobytes(), 4)
+    check_index(hostsim, adversarial_bytes(3 << 20), 16)
+
+
+def test_interpreter_matches_oracle(hostsim):
+    rng = random.Random(3)
+    base = [
+        fixture_bytes("query_gpu_function/simple_single_line.ldjson"),
+        b'{"a": {"b": "a"},"b": {"a": "c" }}',
+        b'{"a":[1,[2,3],{"b":4}],"c":{"d":[]}}',
+        b'{"a" :[ {"b":[0,1,{"c":"x"}]} , 7 ], "d": "\\"a\\":1"}',
+        b'  {"k\\"ey": 1, "key": [ ], "x":{"y":[[],[1]]}}  ',
+    ]
+    paths = [
+        "$.user.lang", "$.user.values[2]", "$.user.values[0:3]", "$.a.a", "$.a[1][0]", "$.a[2].b",
+        "$.c.d[0]", "$.c.d[0:2]", "$.user.lang[?(@ == 'nl')]", "$[0]", "$.b.a", "$.a[0].b[2].c",
+        "$.key[0]", "$.x.y[1][0]", "$.x.y[0:2]", "$['k\\\"ey']", "$.d",
+    ]
+    for trial in range(40):
+        lines = [rng.choice(base) for _ in range(rng.randint(1, 20))]
+        lines.append(bytes(rng.choice(b'{}[]:,"\\ ab') for _ in range(rng.randint(0, 80))))
+        rng.shuffle(lines)
+        data = b"\n".join(lines)
+        for path in paths:
+            ir, depth, slots = oracle.compile_path(path)
+            idx = oracle.Index(data, depth)
+            want = oracle.find_value(data, idx.newlines, idx.strings, idx.levels, depth, ir, slots)
+            f = np.frombuffer(data, dtype=np.uint8)
+            irb = np.frombuffer(ir, dtype=np.uint8)
+            got = np.empty_like(want)
+            ptrs = (ctypes.c_void_p * 1)(irb.ctypes.data)
+            hostsim.hs_find_values(f.ctypes.data, f.size, idx.newlines.ctypes.data, len(idx.newlines),
+                                   idx.strings.ctypes.data, idx.levels.ctypes.data, 1, ptrs, slots,
+                                   got.ctypes.data)
+            assert np.array_equal(got, want), (path, data[:120])
