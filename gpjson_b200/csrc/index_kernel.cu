@@ -165,9 +165,14 @@ __device__ Carry look_back(unsigned long long* states, int64_t t, const Span& ag
             const int first = inc_mask ? __ffs(inc_mask) - 1 : 32;
             const unsigned need = first == 32 ? ~0u : ((1u << first) - 1);
             if (none_mask & need) {
-                if (++polls > kMaxPolls) {
+                ++polls;
+                // Give up after the poll budget, or at once when another tile
+                // already gave up (its successors would wait for it too).
+                const bool expired = polls > kMaxPolls ||
+                                     ((polls & 1023u) == 0 && ld_acquire(status + 1) != 0);
+                if (expired) {
                     if (lane == 0) atomicOr(status + 1, kErrLookbackTimeout);
-                    break;  // give up with what we have; the host reports the error
+                    break;  // the host reports the error; outputs are not valid
                 }
                 __nanosleep(64);
                 continue;
