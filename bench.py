@@ -1,0 +1,428 @@
+"""Benchmark: input GB/s of the index + fused-query pass on one NDJSON file.
+
+Workload (default): the 2 GiB tweet-like NDJSON file, one index build
+(4 levels) and the four queries $.user.lang, $.id, $.user.followers_count,
+$.entities.hashtags[0].text evaluated fused in one pass.  A step is one
+index + query pass over the whole file with the input resident in HBM
+(`value`), or through the C ABI with pinned host input and host results
+(`e2e`: H2D of the file, index, query, D2H of the offsets).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (launched by torch.distributed.run) every rank processes its own
+file of the same shape (weak scaling, no data-path collective); times are
+the max over ranks.  `--impl reference` times the reference algorithm's CPU
+implementation (the oracle restatement of Sequential.java, multi-threaded)
+on a bounded sample of the same workload on this host's cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+QUERIES = ["$.user.lang", "$.id", "$.user.followers_count", "$.entities.hashtags[0].text"]
+FILE_BYTES = 1 << 31
+LEVELS = 4
+TILE = 16384
+PROFILE_TRAFFIC = ROOT / "profiles" / "traffic.json"
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--bytes", type=int, default=FILE_BYTES, help="input file size (default 2 GiB)")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-sample", type=int, default=512 << 20, help="bytes of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args(argv)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """Max of a per-rank scalar (times are reported as the slowest rank)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int, device=None) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        if device is not None:
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"],
+                stdout=self.file, stderr=subprocess.DEVNULL,
+            )
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        time.sleep(0.25)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = []
+        for line in Path(self.file.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": reasons,
+            "samples": len(rows),
+        }
+
+
+def measured_peak_gbs() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(key: str):
+    """DRAM bytes per launch of the index kernel from the committed ncu
+    summary (profiles/traffic.json), scaled to this input size."""
+    if not PROFILE_TRAFFIC.exists():
+        return None
+    try:
+        entry = json.loads(PROFILE_TRAFFIC.read_text())[key]
+        return entry
+    except Exception:
+        return None
+
+
+def cpu_baseline(data_np, n_sample: int, threads_all: bool):
+    """The oracle port of the reference's sequential path on a sample."""
+    from oracle import oracle
+
+    sample = data_np[:n_sample]
+    # cut at a line boundary so the sample is whole lines
+    cut = int(n_sample)
+    while cut > 0 and sample[cut - 1] != 10:
+        cut -= 1
+    sample = sample[:cut]
+    t0 = time.perf_counter()
+    idx = oracle.Index(sample, LEVELS, mt=threads_all)
+    oracle.query(sample, QUERIES, mt=threads_all, index=idx)
+    dt = time.perf_counter() - t0
+    return cut / dt / 1e9, cut, dt, (oracle.num_threads() if threads_all else 1)
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    """CPU reference arm: the oracle restatement of Sequential, all threads."""
+    if rank != 0:
+        return
+    import numpy as np
+
+    from gpjson_b200 import datagen
+
+    from oracle import oracle
+
+    n = min(args.cpu_sample, args.bytes)
+    data = datagen.tweets(n, seed=datagen.SEED_BASE + 1, p_empty_hashtags=0.3)
+    cut = n
+    while cut > 0 and data[cut - 1] != 10:
+        cut -= 1
+    sample = data[:cut]
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        idx = oracle.Index(sample, LEVELS, mt=True)
+        oracle.query(sample, QUERIES, mt=True, index=idx)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    ms = 1000 * statistics.mean(times)
+    value = cut / (ms / 1000) / 1e9
+    cores = oracle.num_threads()
+    line = {
+        "impl": "reference",
+        "metric": "input GB/s (index+query)",
+        "value": round(value, 4),
+        "unit": "GB/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": {
+            "workload": f"tweet-like NDJSON sample of {cut} B (the 2 GiB workload's generator), index "
+                        f"({LEVELS} levels) + 4 queries",
+            "queries": QUERIES,
+            "bytes_per_step": cut,
+        },
+        "cpu_baseline": {
+            "value": round(value, 4),
+            "unit": "GB/s",
+            "cores": cores,
+            "kind": "port",
+            "sample": f"{cut} B prefix of the seeded 2 GiB tweet-like file, whole lines",
+        },
+        "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank: int, world: int, local: int) -> None:
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import gpjson_b200 as gj
+    from gpjson_b200 import datagen
+
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+
+    n = args.bytes
+    host = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    host_np = host.numpy()
+    datagen.tweets(n, seed=datagen.SEED_BASE + 1 + rank, p_empty_hashtags=0.3, out=host_np)
+    dev = host.to(device, non_blocking=False)
+    torch.cuda.synchronize()
+
+    g = gj.GPJSON(local)
+    # one explicit stream carries our kernels and the timing events
+    stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(stream)
+    g.set_stream(stream.cuda_stream)
+    lib, ctx = g._native.lib, g._native.h
+    compiled = [gj.compile_path(q) for q in QUERIES]
+    bufs = [ctypes.create_string_buffer(c.bytecode, len(c.bytecode)) for c in compiled]
+    ptrs = (ctypes.c_void_p * len(compiled))(*[ctypes.addressof(b) for b in bufs])
+    lens = (ctypes.c_size_t * len(compiled))(*[len(c.bytecode) for c in compiled])
+    slots = max(c.num_results for c in compiled)
+    f = g.from_device(dev.data_ptr(), n, keepalive=dev)
+
+    # first pass sizes the index and result buffers
+    f.build_index(LEVELS)
+    lines = f.num_lines
+    out = torch.empty((len(QUERIES), lines, slots, 2), dtype=torch.int64, device=device)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        g._native.check(lib.gpj_index_build(ctx, f._h, LEVELS))
+        if ev:
+            ev[1].record(stream)
+        g._native.check(lib.gpj_query_device(ctx, f._h, len(compiled), ptrs, lens, slots, out.data_ptr(),
+                                             out.numel()))
+        if ev:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    launches0 = g.kernel_launches()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(world, device)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for k in range(args.steps):
+        step(evs[k])
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier(world, device)
+    clock_info = clocks.stop()
+    launches = g.kernel_launches() - launches0
+    total_ms = start.elapsed_time(end)
+    index_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    query_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    total_ms = max_over_ranks(total_ms, world, device)
+    ms_per_step = total_ms / args.steps
+    value = world * n / (ms_per_step / 1000) / 1e9
+
+    # correctness spot check of the timed output against one solo pass
+    solo = f.run(compiled)
+    assert np.array_equal(solo, out.cpu().numpy()), "fused device results differ from a solo pass"
+
+    # ---- end to end through the C ABI with host buffers ----------------------
+    res_host = torch.empty((len(QUERIES), lines, slots, 2), dtype=torch.int64, pin_memory=True)
+    e2e_times = []
+    for k in range(1 + args.e2e_steps):
+        barrier(world, device)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h = ctypes.c_void_p()
+        g._native.check(lib.gpj_file_from_host(ctx, host.data_ptr(), n, ctypes.byref(h)))
+        g._native.check(lib.gpj_index_build(ctx, h, LEVELS))
+        g._native.check(lib.gpj_query(ctx, h, len(compiled), ptrs, lens, slots, res_host.data_ptr(),
+                                      res_host.numel()))
+        lib.gpj_file_release(h)
+        dt = time.perf_counter() - t0
+        if k > 0:
+            e2e_times.append(dt)
+    e2e_s = max_over_ranks(statistics.mean(e2e_times), world, device)
+    assert np.array_equal(res_host.numpy(), out.cpu().numpy()), "e2e results differ"
+    e2e_value = world * n / e2e_s / 1e9
+
+    # ---- roofline of the dominant kernel ---------------------------------------
+    peak, peak_kind = measured_peak_gbs()
+    words = (n + 63) // 64
+    index_bytes = n + 8 * words * (1 + LEVELS) + 8 * lines
+    query_bytes = 16 * len(QUERIES) * lines * slots + 8 * lines
+    dominant = "index" if index_ms >= query_ms else "find_value"
+    if dominant == "index":
+        achieved = index_bytes / (index_ms / 1000) / 1e9
+        alg = index_bytes
+    else:
+        achieved = query_bytes / (query_ms / 1000) / 1e9
+        alg = query_bytes
+    traffic = None
+    t = ncu_traffic(dominant)
+    if t and t.get("bytes") and t.get("input_bytes"):
+        traffic = round(t["bytes"] * n / t["input_bytes"])
+
+    result = {
+        "metric": "input GB/s (index+query)",
+        "value": round(value, 2),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": {
+            "workload": f"tweet-like NDJSON, {n} B per GPU ({lines} lines), one index build ({LEVELS} levels) "
+                        "+ 4 queries fused in one pass",
+            "queries": QUERIES,
+            "bytes_per_gpu": n,
+            "lines_per_gpu": lines,
+            "l2": "input larger than L2 (2 GiB vs 126 MB)",
+            "parallelism": f"replicas x{world} (one file per GPU)",
+        },
+        "kernels_ms": {"index": round(index_ms, 4), "find_value": round(query_ms, 4)},
+        "roofline": {
+            "bound": "hbm",
+            "kernel": dominant,
+            "achieved": round(achieved, 1),
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "traffic": traffic,
+            "algorithmic_bytes": alg,
+            "peak_kind": f"{peak_kind} copy bandwidth",
+        },
+        "step_frac_of_hbm": round(value / world / peak, 4),
+        "e2e": {
+            "value": round(e2e_value, 3),
+            "unit": "GB/s",
+            "h2d_bytes_per_step": n,
+            "d2h_bytes_per_step": int(res_host.numel() * 8),
+        },
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cut, dt, cores = cpu_baseline(host_np, min(args.cpu_sample, n), threads_all=False)
+        result["cpu_baseline"] = {
+            "value": round(v, 4),
+            "unit": "GB/s",
+            "cores": cores,
+            "kind": "port",
+            "sample": f"{cut} B prefix (whole lines) of the same file, index + 4 queries, {dt:.1f} s",
+        }
+    f.release()
+    g.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def main(argv=None) -> None:
+    args = parse_args(argv)
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -46,7 +46,9 @@ struct gpj_ctx {
     unsigned long long* d_status = nullptr;
     unsigned long long* h_status = nullptr;  // pinned, 2 words
     uint32_t epoch = 0;
-    int index_occupancy[3] = {0, 0, 0};  // levels <=4, <=8, <=16
+    int index_occupancy[3] = {0, 0, 0};  // exact kernel, levels <=4, <=8, <=16
+    int line_occupancy[3] = {0, 0, 0};   // line-parallel kernel
+    int64_t exact_fallbacks = 0;         // builds that needed the exact kernel
     int query_occupancy = 0;
 
     // pinned staging for file reads
@@ -164,7 +166,33 @@ int ensure_tile_state(gpj_ctx* ctx, int64_t ntiles) {
 
 int occupancy_slot(int num_levels) { return num_levels <= 4 ? 0 : (num_levels <= 8 ? 1 : 2); }
 
-// One launch of the index kernel; *lines receives the line count.
+// One launch of an index kernel; on return h_status holds its status words.
+int launch_index(gpj_ctx* ctx, bool exact, const gpj::IndexParams& base) {
+    const int64_t ntiles = base.ntiles;
+    int rc = ensure_tile_state(ctx, ntiles);
+    if (rc) return rc;
+    GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned int), ctx->stream));
+    GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    gpj::IndexParams p = base;
+    p.tile_state = ctx->d_tile_state;
+    p.tile_counter = ctx->d_counter;
+    p.status = ctx->d_status;
+    p.epoch = ctx->epoch;
+    const int slot = occupancy_slot(p.num_levels);
+    const int occ = exact ? ctx->index_occupancy[slot] : ctx->line_occupancy[slot];
+    const int64_t grid = std::min<int64_t>(ntiles, static_cast<int64_t>(ctx->sms) * occ);
+    GPJ_CUDA(ctx, exact ? gpj::launch_index_kernel(p, static_cast<int>(grid), ctx->stream)
+                        : gpj::launch_line_index_kernel(p, static_cast<int>(grid), ctx->stream));
+    ctx->launches++;
+    GPJ_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GPJ_OK;
+}
+
+// Builds the index with the line-parallel kernel, and again with the exact
+// kernel when the input is not well-formed NDJSON; *lines receives the line
+// count.
 int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, uint64_t* d_str,
               uint64_t* d_lvl, int64_t* d_nl, int64_t nl_cap, int64_t* lines) {
     if (n == 0) {
@@ -173,39 +201,32 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
         *lines = 1;
         return GPJ_OK;
     }
-    const int64_t ntiles = (n + gpj::kIndexTileBytes - 1) / gpj::kIndexTileBytes;
-    int rc = ensure_tile_state(ctx, ntiles);
-    if (rc) return rc;
-    GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned int), ctx->stream));
-    GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
-    gpj::IndexParams p;
+    gpj::IndexParams p{};
     p.file = d_file;
     p.n = n;
-    p.ntiles = ntiles;
+    p.ntiles = (n + gpj::kIndexTileBytes - 1) / gpj::kIndexTileBytes;
     p.string_index = d_str;
     p.leveled = d_lvl;
     p.level_size = (n + 63) / 64;
     p.num_levels = num_levels;
     p.newlines = d_nl;
     p.newline_cap = nl_cap;
-    p.tile_state = ctx->d_tile_state;
-    p.tile_counter = ctx->d_counter;
-    p.status = ctx->d_status;
-    p.epoch = ctx->epoch;
-    const int occ = ctx->index_occupancy[occupancy_slot(num_levels)];
-    const int64_t grid = std::min<int64_t>(ntiles, static_cast<int64_t>(ctx->sms) * occ);
-    GPJ_CUDA(ctx, gpj::launch_index_kernel(p, static_cast<int>(grid), ctx->stream));
-    ctx->launches++;
-    GPJ_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(unsigned long long),
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-    GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    const unsigned long long errs = ctx->h_status[1];
+    int rc = launch_index(ctx, false, p);
+    if (rc) return rc;
+    unsigned long long errs = ctx->h_status[1];
+    if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) {
+        ctx->exact_fallbacks++;
+        rc = launch_index(ctx, true, p);
+        if (rc) return rc;
+        errs = ctx->h_status[1];
+    }
     if (errs) {
         std::string m = "index kernel reported:";
         if (errs & gpj::kErrLookbackTimeout) m += " look-back wait expired;";
         if (errs & gpj::kErrCopyTimeout) m += " TMA copy wait expired;";
         if (errs & gpj::kErrEscapeRun)
             m += " a backslash run longer than 64 KiB crosses a 16 KiB tile boundary;";
+        if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) m += " unexpected line check failure;";
         return fail(ctx, (errs & gpj::kErrEscapeRun) ? GPJ_ELIMIT : GPJ_EDEVICE, m);
     }
     *lines = static_cast<int64_t>(ctx->h_status[0]);
@@ -356,6 +377,8 @@ int gpj_create(int device, gpj_ctx** out) {
     for (int i = 0; i < 3; i++) {
         ctx->index_occupancy[i] = gpj::index_kernel_max_ctas_per_sm(levels[i]);
         if (ctx->index_occupancy[i] < 1) return bail(cudaGetLastError(), "index kernel occupancy");
+        ctx->line_occupancy[i] = gpj::line_index_max_ctas_per_sm(levels[i]);
+        if (ctx->line_occupancy[i] < 1) return bail(cudaGetLastError(), "line index kernel occupancy");
     }
     ctx->query_occupancy = gpj::find_value_max_ctas_per_sm();
     if (ctx->query_occupancy < 1) return bail(cudaGetLastError(), "find_value occupancy");
@@ -753,7 +776,8 @@ int gpj_get_timings(gpj_ctx* ctx, char* json, size_t cap, size_t* len) {
                       ctx->phases[i].name.c_str(), ctx->phases[i].device_ms, ctx->phases[i].host_ms);
         s += buf;
     }
-    s += "],\"kernel_launches\":" + std::to_string(ctx->launches) + "}";
+    s += "],\"kernel_launches\":" + std::to_string(ctx->launches) +
+         ",\"exact_index_fallbacks\":" + std::to_string(ctx->exact_fallbacks) + "}";
     if (len) *len = s.size();
     if (json && cap > 0) {
         const size_t k = std::min(cap - 1, s.size());

@@ -12,6 +12,8 @@ enum DeviceError : unsigned long long {
     kErrLookbackTimeout = 1ull << 0,  // a predecessor tile never published
     kErrCopyTimeout = 1ull << 1,      // a TMA copy never completed
     kErrEscapeRun = 1ull << 2,        // backslash run longer than the scan bound
+    kErrIrregular = 1ull << 3,        // a line does not end outside strings at level -1
+    kErrLongLine = 1ull << 4,         // a line runs further past its tile than the bound
 };
 
 // Poll budgets of the bounded waits (each poll also sleeps briefly).

@@ -1,11 +1,13 @@
-// Single-pass structural index for NDJSON on sm_100a.
+// Exact single-pass structural index on sm_100a (any input).
 //
 // Replaces the reference's seven index launches and three host round trips
 // (stages/CombinedIndex.java:28-151, stages/LeveledBitmapsIndex.java:40-103,
 // kernels create_combined_escape_carry_newline_count_index.cu,
 // create_combined_escape_newline_index.cu, create_quote_index.cu,
 // create_string_index.cu, create_leveled_bitmaps_carry_index.cu,
-// create_leveled_bitmaps.cu) with one persistent kernel:
+// create_leveled_bitmaps.cu) with one persistent kernel.  It is the fallback
+// of the line-parallel kernel (index_lines.cu) for inputs that are not
+// well-formed NDJSON:
 //
 //  * The input is cut into 16 KiB tiles claimed in order from an atomic
 //    counter.  Each CTA (256 threads, one 64-byte word per thread) double
@@ -251,10 +253,6 @@ __global__ void __launch_bounds__(kThreads) index_kernel(IndexParams p) {
     uint32_t phase[2] = {0, 0};
     int b = 0;
     while (t < p.ntiles) {
-        // Prefetch the next tile into the other buffer (its last reader
-        // finished before the barrier that ended the previous iteration).
-        if (tid == 0) sh.next_tile = claim_and_load(p, sh, b ^ 1);
-
         if (!mbar_wait_bounded(&sh.bar[b], phase[b])) {
             if (tid == 0) atomicOr(p.status + 1, kErrCopyTimeout);
         }
@@ -369,6 +367,11 @@ __global__ void __launch_bounds__(kThreads) index_kernel(IndexParams p) {
             }
         }
         __syncthreads();
+        // Claim the next tile only now and start its copy into the other
+        // buffer (last read in the previous iteration): a claimed tile is
+        // processed right away, so successors never wait on a tile whose
+        // owner is still busy with an earlier one.
+        if (tid == 0) sh.next_tile = claim_and_load(p, sh, b ^ 1);
 
         // ---- final masks and stores ------------------------------------------
         if (valid > 0) {

@@ -29,7 +29,15 @@ struct IndexParams {
     uint32_t epoch;                  // 1..65535
 };
 
+// Exact kernel: carries string state, level and newline count across tiles
+// by decoupled look-back; correct for any input.
 cudaError_t launch_index_kernel(const IndexParams& p, int grid, cudaStream_t stream);
 int index_kernel_max_ctas_per_sm(int num_levels);
+
+// Line-parallel kernel for NDJSON: every line starts outside strings at
+// level -1; flags kErrIrregular / kErrLongLine when that does not hold and
+// the exact kernel must be used.  tile_state needs 2 * ntiles words.
+cudaError_t launch_line_index_kernel(const IndexParams& p, int grid, cudaStream_t stream);
+int line_index_max_ctas_per_sm(int num_levels);
 
 }  // namespace gpj

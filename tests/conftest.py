@@ -37,6 +37,8 @@ def hostsim():
     P = ctypes.c_void_p
     L.hs_build_index.restype = ctypes.c_int64
     L.hs_build_index.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P, P, ctypes.c_int64]
+    L.hs_build_index_lines.restype = ctypes.c_int64
+    L.hs_build_index_lines.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P, P, ctypes.c_int64]
     L.hs_find_values.restype = None
     L.hs_find_values.argtypes = [P, ctypes.c_int64, P, ctypes.c_int64, P, P, ctypes.c_int, P, ctypes.c_int, P]
     L.hs_escaped_mask.restype = ctypes.c_uint64

@@ -4,6 +4,7 @@
 // test suite can compare them with the oracle without a GPU.  It is built
 // by tests/conftest.py and never used by the library.
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -110,6 +111,76 @@ int64_t hs_build_index(const uint8_t* f, int64_t n, int num_levels, uint64_t* st
         nl_state += acc.nl;
     }
     return nl_state + 1;
+}
+
+// Mirrors the line-parallel kernel (index_lines.cu): per tile, the lines
+// starting in it are indexed from the NDJSON line-start state (outside
+// strings, level -1), continuing past the tile end to the first newline;
+// words are written by the tile whose range holds their first byte.
+// Returns the line count, or -1 when a line does not end in the line-start
+// state (the kernel then defers to the exact kernel).
+int64_t hs_build_index_lines(const uint8_t* f, int64_t n, int num_levels, uint64_t* str_out,
+                             uint64_t* lvl_out, int64_t* nl_out, int64_t nl_cap) {
+    const int64_t level_size = (n + 63) / 64;
+    const int64_t ntiles = (n + kTileBytes - 1) / kTileBytes;
+    int64_t nl_before = 0;
+    bool irregular = false;
+    if (nl_cap > 0) nl_out[0] = 0;
+    for (int64_t t = 0; t < ntiles; t++) {
+        const int64_t ts = t * kTileBytes, te = std::min(n, ts + kTileBytes);
+        int64_t a = -1;
+        for (int64_t i = ts; i < te; i++)
+            if (f[i] == '\n') {
+                if (a < 0) a = i;
+                if (1 + nl_before < nl_cap) nl_out[1 + nl_before] = i;
+                ++nl_before;
+            }
+        if (t == 0) a = 0;
+        if (a < 0) continue;
+        int64_t b = te;
+        while (b < n && f[b] != '\n') ++b;
+        // b == te when the tile ends at a newline or at the end of the file
+        int s = 0;
+        int64_t d = -1;
+        uint32_t esc = 0;
+        for (int64_t ws = (a / 64) * 64; ws < b || (ws < n && ws < ((b + 63) / 64) * 64); ws += 64) {
+            if (ws >= n) break;
+            uint32_t v[16];
+            for (int k = 0; k < 16; k++) v[k] = load_u32(f, n, ws + 4 * k);
+            ClassMasks m = classify64(v);
+            uint64_t keep = ~0ull;
+            if (a > ws) keep &= ~((1ull << (a - ws)) - 1);
+            if (n - ws < 64) keep &= (1ull << (n - ws)) - 1;
+            m.backslash &= keep, m.quote &= keep, m.newline &= keep, m.open &= keep, m.close &= keep,
+                m.structural &= keep;
+            uint32_t cout;
+            const uint64_t e = escaped_mask(m.backslash, esc, &cout);
+            esc = cout;
+            const uint64_t qr = m.quote & ~e;
+            const uint64_t in_str = (prefix_xor(qr) ^ (s ? ~0ull : 0ull)) & keep;
+            const uint64_t open = m.open & ~in_str, close = m.close & ~in_str;
+            // '\n' in (a, b]: must be outside strings at level -1
+            uint64_t check = m.newline;
+            if (a >= ws && a < ws + 64) check &= ~(1ull << (a - ws));
+            if (b < ws + 64 && b >= ws) check &= (b == ws + 63) ? ~0ull : ((2ull << (b - ws)) - 1);
+            else if (b < ws) check = 0;
+            for (uint64_t c = check; c; c &= c - 1) {
+                const int bit = ctz64(c);
+                const uint64_t below = (1ull << bit) - 1;
+                if ((in_str >> bit) & 1) irregular = true;
+                if (d + popc64(open & below) - popc64(close & below) != -1) irregular = true;
+            }
+            if (ws >= a && ws < b) {
+                str_out[ws / 64] = in_str;
+                uint64_t lv[16];
+                split_levels<16>(open, close, m.structural & ~in_str, d, lv);
+                for (int l = 0; l < num_levels; l++) lvl_out[l * level_size + ws / 64] = lv[l];
+            }
+            d += popc64(open) - popc64(close);
+            s = (popc64(qr) & 1) ? !s : s;
+        }
+    }
+    return irregular ? -1 : nl_before + 1;
 }
 
 // Runs each query's bytecode on every line with the device interpreter.

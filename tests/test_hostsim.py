@@ -28,12 +28,33 @@ def hs_index(hostsim, data: bytes, levels: int):
     return nl[:cnt], st[:words], lv[: words * levels].reshape(levels, words)
 
 
-def check_index(hostsim, data: bytes, levels: int):
+def hs_index_lines(hostsim, data: bytes, levels: int):
+    f = np.frombuffer(data, dtype=np.uint8)
+    n = f.size
+    words = (n + 63) // 64
+    nl = np.zeros(n + 1, np.int64)
+    st = np.full(max(words, 1), 0xDEAD, np.uint64)
+    lv = np.full(max(words * levels, 1), 0xDEAD, np.uint64)
+    cnt = hostsim.hs_build_index_lines(f.ctypes.data, n, levels, st.ctypes.data, lv.ctypes.data, nl.ctypes.data,
+                                       n + 1)
+    if cnt < 0:
+        return None
+    return nl[:cnt], st[:words], lv[: words * levels].reshape(levels, words)
+
+
+def check_index(hostsim, data: bytes, levels: int, expect_regular=None):
     want = oracle.Index(data, levels)
     nl, st, lv = hs_index(hostsim, data, levels)
     assert np.array_equal(nl, want.newlines)
     assert np.array_equal(st, want.strings)
     assert np.array_equal(lv, want.levels)
+    lines = hs_index_lines(hostsim, data, levels)
+    if expect_regular is not None:
+        assert (lines is not None) == expect_regular
+    if lines is not None:  # the line-parallel result, when accepted, is exact
+        assert np.array_equal(lines[0], want.newlines)
+        assert np.array_equal(lines[1], want.strings)
+        assert np.array_equal(lines[2], want.levels)
 
 
 def test_escape_mask_random_words(hostsim):
@@ -79,8 +100,18 @@ def test_tile_straddling_escapes(hostsim):
 
 
 def test_generated(hostsim):
-    check_index(hostsim, datagen.tweets(1 << 20).tobytes(), 4)
-    check_index(hostsim, adversarial_bytes(3 << 20), 16)
+    check_index(hostsim, datagen.tweets(1 << 20).tobytes(), 4, expect_regular=True)
+    check_index(hostsim, adversarial_bytes(3 << 20), 16, expect_regular=True)
+
+
+def test_line_parallel_rejects_irregular(hostsim):
+    good = datagen.tweets(200000).tobytes()
+    cut = good.index(b"\n", 100000)
+    for bad in [b'{"a": "x\ny"}', b'{"a": [1, 2}', b'{"a": 1}}', b'"open']:
+        data = good[:cut] + b"\n" + bad + good[cut:]
+        check_index(hostsim, data, 4, expect_regular=False)
+    # brackets and quotes balanced inside a line are fine, whatever the bytes
+    check_index(hostsim, good[:cut] + b'\n{"s":"\\\\\\"\\\\","t":[{}]}' + good[cut:], 4, expect_regular=True)
 
 
 def test_interpreter_matches_oracle(hostsim):
