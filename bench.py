@@ -274,21 +274,19 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     out = torch.empty((len(QUERIES), lines, slots, 2), dtype=torch.int64, device=device)
 
     def step(ev=None):
+        """One pass: index (4 levels) + the 4 queries fused, input in HBM."""
         if ev:
             ev[0].record(stream)
-        g._native.check(lib.gpj_index_build(ctx, f._h, LEVELS))
+        g._native.check(lib.gpj_index_query_device(ctx, f._h, LEVELS, len(compiled), ptrs, lens, slots,
+                                                   out.data_ptr(), lines))
         if ev:
             ev[1].record(stream)
-        g._native.check(lib.gpj_query_device(ctx, f._h, len(compiled), ptrs, lens, slots, out.data_ptr(),
-                                             out.numel()))
-        if ev:
-            ev[2].record(stream)
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
 
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
     launches0 = g.kernel_launches()
     clocks = ClockSampler(local)
     clocks.start()
@@ -305,8 +303,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     clock_info = clocks.stop()
     launches = g.kernel_launches() - launches0
     total_ms = start.elapsed_time(end)
-    index_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
-    query_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    pass_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
     total_ms = max_over_ranks(total_ms, world, device)
     ms_per_step = total_ms / args.steps
     value = world * n / (ms_per_step / 1000) / 1e9
@@ -335,20 +332,15 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     assert np.array_equal(res_host.numpy(), out.cpu().numpy()), "e2e results differ"
     e2e_value = world * n / e2e_s / 1e9
 
-    # ---- roofline of the dominant kernel ---------------------------------------
+    # ---- roofline of the dominant (only) kernel --------------------------------
+    # The fused pass reads the input once and writes the index (string
+    # bitmap, LEVELS level bitmaps, newline offsets) and the query offsets.
     peak, peak_kind = measured_peak_gbs()
     words = (n + 63) // 64
-    index_bytes = n + 8 * words * (1 + LEVELS) + 8 * lines
-    query_bytes = 16 * len(QUERIES) * lines * slots + 8 * lines
-    dominant = "index" if index_ms >= query_ms else "find_value"
-    if dominant == "index":
-        achieved = index_bytes / (index_ms / 1000) / 1e9
-        alg = index_bytes
-    else:
-        achieved = query_bytes / (query_ms / 1000) / 1e9
-        alg = query_bytes
+    alg = n + 8 * words * (1 + LEVELS) + 8 * lines + 16 * len(QUERIES) * lines * slots
+    achieved = alg / (pass_ms / 1000) / 1e9
     traffic = None
-    t = ncu_traffic(dominant)
+    t = ncu_traffic("line_index_kernel")
     if t and t.get("bytes") and t.get("input_bytes"):
         traffic = round(t["bytes"] * n / t["input_bytes"])
 
@@ -374,10 +366,10 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
             "l2": "input larger than L2 (2 GiB vs 126 MB)",
             "parallelism": f"replicas x{world} (one file per GPU)",
         },
-        "kernels_ms": {"index": round(index_ms, 4), "find_value": round(query_ms, 4)},
+        "kernels_ms": {"index_and_query": round(pass_ms, 4)},
         "roofline": {
             "bound": "hbm",
-            "kernel": dominant,
+            "kernel": "line_index_kernel (index + 4 queries, one launch)",
             "achieved": round(achieved, 1),
             "peak": peak,
             "unit": "GB/s",

@@ -312,6 +312,34 @@ class File:
         )
         return out
 
+    def query_paths(self, paths: list[str]) -> np.ndarray:
+        """gpj_query_paths: compile, index and evaluate in one pass; returns
+        int64 [nq][lines][slots][2]."""
+        arr = (c_char_p * len(paths))(*[p.encode("utf-8") for p in paths])
+        r = c_void_p()
+        self._native.check(self._native.lib.gpj_query_paths(self._native.h, self._h, len(paths), arr, byref(r)))
+        lib = self._native.lib
+        try:
+            nq, lines, slots = lib.gpj_result_num_queries(r), lib.gpj_result_num_lines(r), lib.gpj_result_slots(r)
+            count = nq * lines * slots * 2
+            ptr = lib.gpj_result_offsets(r)
+            buf = (ctypes.c_int64 * count).from_address(ptr) if count else []
+            return np.array(buf, dtype=np.int64, copy=True).reshape(nq, lines, slots, 2)
+        finally:
+            lib.gpj_result_release(r)
+
+    def index_and_query_device(self, queries: list[CompiledQuery], num_levels: int, d_out: int, out_lines: int,
+                               slots: int | None = None) -> None:
+        """gpj_index_query_device: index + queries in one pass into device
+        memory at address d_out (int64 [nq][out_lines][slots][2])."""
+        nq = len(queries)
+        slots = slots or max(q.num_results for q in queries)
+        bufs = [ctypes.create_string_buffer(q.bytecode, len(q.bytecode)) for q in queries]
+        ptrs = (c_void_p * nq)(*[ctypes.addressof(b) for b in bufs])
+        lens = (c_size_t * nq)(*[len(q.bytecode) for q in queries])
+        self._native.check(self._native.lib.gpj_index_query_device(
+            self._native.h, self._h, num_levels, nq, ptrs, lens, slots, c_void_p(d_out), out_lines))
+
     def release(self) -> None:
         if self._h:
             self._native.lib.gpj_file_release(self._h)
@@ -358,12 +386,10 @@ class GPJSON:
     # -- the reference members ------------------------------------------------
     def query(self, filename, queries, options=None) -> Result:
         """QueryFunction.call: query(file, path | [paths], options?)."""
-        paths, compiled = prepare_queries(queries, options)
-        depth = max(q.max_depth for q in compiled)
+        paths, _ = prepare_queries(queries, options)
         f = self.open(filename)
         try:
-            f.build_index(depth)
-            offsets = f.run(compiled)
+            offsets = f.query_paths(paths)
         finally:
             f.release()
         with open(filename, "rb") as fh:

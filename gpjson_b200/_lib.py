@@ -57,6 +57,10 @@ SIGNATURES: dict[str, tuple] = {
         c_int,
         [c_void_p, c_void_p, c_int, POINTER(c_void_p), POINTER(c_size_t), c_int, c_void_p, c_int64],
     ),
+    "gpj_index_query_device": (
+        c_int,
+        [c_void_p, c_void_p, c_int, c_int, POINTER(c_void_p), POINTER(c_size_t), c_int, c_void_p, c_int64],
+    ),
     "gpj_query_paths": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_char_p), POINTER(c_void_p)]),
     "gpj_result_num_queries": (c_int64, [c_void_p]),
     "gpj_result_num_lines": (c_int64, [c_void_p]),

@@ -190,11 +190,24 @@ int launch_index(gpj_ctx* ctx, bool exact, const gpj::IndexParams& base) {
     return GPJ_OK;
 }
 
-// Builds the index with the line-parallel kernel, and again with the exact
-// kernel when the input is not well-formed NDJSON; *lines receives the line
-// count.
+// Queries evaluated by the index pass (packed bytecode already on device).
+struct FusedQueries {
+    int nq = 0;
+    int slots = 0;
+    const uint8_t* bytecode = nullptr;
+    const int32_t* offsets = nullptr;
+    int64_t* out = nullptr;
+    int64_t out_lines = 0;  // query stride of `out`
+};
+
+// Builds the index with the line-parallel kernel (evaluating `fq` in the
+// same pass when given), and again with the exact kernel when the input is
+// not well-formed NDJSON.  *lines receives the line count; *queries_done
+// tells whether every line's query results were written.
 int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, uint64_t* d_str,
-              uint64_t* d_lvl, int64_t* d_nl, int64_t nl_cap, int64_t* lines) {
+              uint64_t* d_lvl, int64_t* d_nl, int64_t nl_cap, int64_t* lines, const FusedQueries* fq = nullptr,
+              bool* queries_done = nullptr) {
+    if (queries_done) *queries_done = false;
     if (n == 0) {
         if (nl_cap > 0) GPJ_CUDA(ctx, cudaMemsetAsync(d_nl, 0, 8, ctx->stream));
         GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -211,16 +224,28 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
     p.num_levels = num_levels;
     p.newlines = d_nl;
     p.newline_cap = nl_cap;
-    int rc = launch_index(ctx, false, p);
+    p.materialize = 1;
+    gpj::IndexParams fused = p;
+    if (fq && fq->nq > 0) {
+        fused.num_queries = fq->nq;
+        fused.bytecode = fq->bytecode;
+        fused.offsets = fq->offsets;
+        fused.slots = fq->slots;
+        fused.out = fq->out;
+        fused.out_lines = fq->out_lines;
+    }
+    int rc = launch_index(ctx, false, fused);
     if (rc) return rc;
     unsigned long long errs = ctx->h_status[1];
+    bool exact = false;
     if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) {
         ctx->exact_fallbacks++;
+        exact = true;
         rc = launch_index(ctx, true, p);
         if (rc) return rc;
         errs = ctx->h_status[1];
     }
-    if (errs) {
+    if (errs & ~(gpj::kErrDeferred | gpj::kErrOutOverflow)) {
         std::string m = "index kernel reported:";
         if (errs & gpj::kErrLookbackTimeout) m += " look-back wait expired;";
         if (errs & gpj::kErrCopyTimeout) m += " TMA copy wait expired;";
@@ -230,6 +255,8 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
         return fail(ctx, (errs & gpj::kErrEscapeRun) ? GPJ_ELIMIT : GPJ_EDEVICE, m);
     }
     *lines = static_cast<int64_t>(ctx->h_status[0]);
+    if (queries_done && fq && fq->nq > 0)
+        *queries_done = !exact && !(errs & (gpj::kErrDeferred | gpj::kErrOutOverflow)) && *lines <= fq->out_lines;
     return GPJ_OK;
 }
 
@@ -284,7 +311,7 @@ int upload_queries(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, 
     return GPJ_OK;
 }
 
-int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out) {
+int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, int64_t out_lines) {
     const size_t header = ((static_cast<size_t>(nq) * 4 + 15) / 16) * 16;
     gpj::QueryParams p;
     p.file = f->d_data;
@@ -299,6 +326,7 @@ int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out) {
     p.num_queries = nq;
     p.slots = slots;
     p.out = d_out;
+    p.out_lines = out_lines;
     const int64_t want = (f->num_lines + 255) / 256;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * ctx->query_occupancy));
     GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->stream));
@@ -306,26 +334,122 @@ int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out) {
     return GPJ_OK;
 }
 
-int query_common(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, const size_t* len,
-                 int slots, int64_t** d_out_io, int64_t out_count, bool to_host, int64_t* host_out) {
+int check_query_args(gpj_ctx* ctx, int nq, int slots) {
     if (nq < 1 || nq > GPJ_MAX_QUERIES)
         return fail(ctx, GPJ_ELIMIT, "Maximum size of queries is 255 (got " + std::to_string(nq) + ")");
     if (slots < 1) return fail(ctx, GPJ_EINVAL, "result_slots must be >= 1");
+    return GPJ_OK;
+}
+
+int ensure_index_buffers(gpj_ctx* ctx, gpj_file* f, int num_levels) {
+    int rc;
+    if (num_levels < 1 || num_levels > GPJ_MAX_LEVELS)
+        return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(num_levels));
+    if (!f->d_str && (rc = device_alloc(ctx, &f->d_str, static_cast<size_t>(f->words), "cudaMalloc(string index)")))
+        return rc;
+    if (f->lvl_cap < num_levels) {
+        device_free(f->d_lvl);
+        f->lvl_cap = 0;
+        rc = device_alloc(ctx, &f->d_lvl, static_cast<size_t>(f->words) * num_levels, "cudaMalloc(leveled bitmaps)");
+        if (rc) return rc;
+        f->lvl_cap = num_levels;
+    }
+    if (!f->d_nl) {
+        f->nl_cap = std::min<int64_t>(f->n + 1, f->n / 256 + 1024);
+        rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(f->nl_cap), "cudaMalloc(newline index)");
+        if (rc) return rc;
+    }
+    return GPJ_OK;
+}
+
+// The index pass of a file (and the queries in `fq`, when given, in the same
+// pass).  Grows the newline index and repeats the pass when the file has
+// more lines than the first estimate.
+int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq, bool* queries_done) {
+    int rc = ensure_index_buffers(ctx, f, num_levels);
+    if (rc) return rc;
+    f->indexed = false;
+    const double t0 = now_ms();
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    int64_t lines = 0;
+    rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, fq,
+                   queries_done);
+    if (rc) return rc;
+    if (lines > f->nl_cap) {  // more lines than the first guess: size exactly and rebuild
+        device_free(f->d_nl);
+        f->nl_cap = lines;
+        rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(lines), "cudaMalloc(newline index)");
+        if (rc) return rc;
+        rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, fq,
+                       queries_done);
+        if (rc) return rc;
+    }
+    rc = end_phase(ctx, fq && fq->nq ? "index_and_query" : "build_index", t0);
+    if (rc) return rc;
+    f->num_lines = lines;
+    f->num_levels = num_levels;
+    f->indexed = true;
+    return GPJ_OK;
+}
+
+// Index + queries in one pass when possible, into d_out with query stride
+// out_lines (>= the line count, else GPJ_ELIMIT with *lines_needed set).
+int index_and_query(gpj_ctx* ctx, gpj_file* f, int num_levels, int nq, const uint8_t* const* bc,
+                    const size_t* len, int slots, int64_t* d_out, int64_t out_lines, int64_t* lines_needed) {
+    int rc = check_query_args(ctx, nq, slots);
+    if (rc) return rc;
+    int depth = 0;
+    rc = upload_queries(ctx, f, nq, bc, len, slots, &depth);
+    if (rc) return rc;
+    if (depth > num_levels)
+        return fail(ctx, GPJ_ELIMIT, "queries need " + std::to_string(depth) + " levels, the index is built with " +
+                                         std::to_string(num_levels));
+    FusedQueries fq;
+    fq.nq = nq;
+    fq.slots = slots;
+    const size_t header = ((static_cast<size_t>(nq) * 4 + 15) / 16) * 16;
+    fq.offsets = reinterpret_cast<const int32_t*>(f->d_ir);
+    fq.bytecode = f->d_ir + header;
+    fq.out = d_out;
+    fq.out_lines = out_lines;
+    bool done = false;
+    rc = index_pass(ctx, f, num_levels, &fq, &done);
+    if (rc) return rc;
+    if (lines_needed) *lines_needed = f->num_lines;
+    if (f->num_lines > out_lines)
+        return fail(ctx, GPJ_ELIMIT, "result buffer holds " + std::to_string(out_lines) + " lines, the file has " +
+                                         std::to_string(f->num_lines));
+    if (!done) {
+        // lines the fused pass could not evaluate (or an input that needed the
+        // exact kernel): evaluate every line from the materialised index
+        const double t1 = now_ms();
+        GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+        rc = launch_query(ctx, f, nq, slots, d_out, out_lines);
+        if (rc) return rc;
+        rc = end_phase(ctx, "find_value", t1);
+        if (rc) return rc;
+    }
+    return GPJ_OK;
+}
+
+int query_common(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, const size_t* len,
+                 int slots, int64_t* d_out, int64_t out_count, bool to_host, int64_t* host_out) {
+    int rc = check_query_args(ctx, nq, slots);
+    if (rc) return rc;
     if (!f->indexed) return fail(ctx, GPJ_ESTATE, "file is not indexed (call gpj_index_build)");
     const int64_t need = static_cast<int64_t>(nq) * f->num_lines * slots * 2;
     if (out_count < need)
         return fail(ctx, GPJ_EINVAL, "output holds " + std::to_string(out_count) + " elements, " +
                                          std::to_string(need) + " needed");
     int depth = 0;
-    int rc = upload_queries(ctx, f, nq, bc, len, slots, &depth);
+    rc = upload_queries(ctx, f, nq, bc, len, slots, &depth);
     if (rc) return rc;
     if (depth > f->num_levels)
         return fail(ctx, GPJ_ESTATE, "queries need " + std::to_string(depth) + " levels, index has " +
                                          std::to_string(f->num_levels));
-    int64_t* d_out = *d_out_io;
     const double t0 = now_ms();
     GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    rc = launch_query(ctx, f, nq, slots, d_out);
+    rc = launch_query(ctx, f, nq, slots, d_out, f->num_lines);
     if (rc) return rc;
     if (!to_host) return GPJ_OK;
     rc = end_phase(ctx, "find_value", t0);
@@ -334,6 +458,16 @@ int query_common(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, co
     GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     GPJ_CUDA(ctx, cudaMemcpyAsync(host_out, d_out, need * 8, cudaMemcpyDeviceToHost, ctx->stream));
     return end_phase(ctx, "copy_results", t1);
+}
+
+int ensure_out(gpj_ctx* ctx, gpj_file* f, size_t elems) {
+    if (elems <= f->d_out_cap) return GPJ_OK;
+    device_free(f->d_out);
+    f->d_out_cap = 0;
+    int rc = device_alloc(ctx, &f->d_out, elems, "cudaMalloc(results)");
+    if (rc) return rc;
+    f->d_out_cap = elems;
+    return GPJ_OK;
 }
 
 }  // namespace
@@ -580,42 +714,7 @@ int gpj_index_build(gpj_ctx* ctx, gpj_file* f, int num_levels) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (!f || f->ctx != ctx) return fail(ctx, GPJ_EINVAL, "file does not belong to this context");
-    if (num_levels < 1 || num_levels > GPJ_MAX_LEVELS)
-        return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(num_levels));
-    if (!f->d_str && (rc = device_alloc(ctx, &f->d_str, static_cast<size_t>(f->words), "cudaMalloc(string index)")))
-        return rc;
-    if (f->lvl_cap < num_levels) {
-        device_free(f->d_lvl);
-        f->lvl_cap = 0;
-        rc = device_alloc(ctx, &f->d_lvl, static_cast<size_t>(f->words) * num_levels, "cudaMalloc(leveled bitmaps)");
-        if (rc) return rc;
-        f->lvl_cap = num_levels;
-    }
-    if (!f->d_nl) {
-        f->nl_cap = std::min<int64_t>(f->n + 1, f->n / 256 + 1024);
-        rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(f->nl_cap), "cudaMalloc(newline index)");
-        if (rc) return rc;
-    }
-    f->indexed = false;
-    const double t0 = now_ms();
-    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    int64_t lines = 0;
-    rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
-    if (rc) return rc;
-    if (lines > f->nl_cap) {  // more lines than the first guess: size exactly and rebuild
-        device_free(f->d_nl);
-        f->nl_cap = lines;
-        rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(lines), "cudaMalloc(newline index)");
-        if (rc) return rc;
-        rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
-        if (rc) return rc;
-    }
-    rc = end_phase(ctx, "build_index", t0);
-    if (rc) return rc;
-    f->num_lines = lines;
-    f->num_levels = num_levels;
-    f->indexed = true;
-    return GPJ_OK;
+    return index_pass(ctx, f, num_levels, nullptr, nullptr);
 }
 
 int gpj_index_num_lines(const gpj_file* f, int64_t* lines) {
@@ -690,15 +789,11 @@ int gpj_query(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, const
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (!f || !bc || !len || !host_out) return fail(ctx, GPJ_EINVAL, "bad arguments");
-    const int64_t need = static_cast<int64_t>(nq) * f->num_lines * std::max(slots, 1) * 2;
-    if (f->indexed && static_cast<size_t>(need) > f->d_out_cap) {
-        device_free(f->d_out);
-        f->d_out_cap = 0;
-        rc = device_alloc(ctx, &f->d_out, static_cast<size_t>(need), "cudaMalloc(results)");
+    if (f->indexed) {
+        rc = ensure_out(ctx, f, static_cast<size_t>(std::max(nq, 1)) * f->num_lines * std::max(slots, 1) * 2);
         if (rc) return rc;
-        f->d_out_cap = static_cast<size_t>(need);
     }
-    return query_common(ctx, f, nq, bc, len, slots, &f->d_out, out_count, true, host_out);
+    return query_common(ctx, f, nq, bc, len, slots, f->d_out, out_count, true, host_out);
 }
 
 int gpj_query_device(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, const size_t* len,
@@ -706,7 +801,15 @@ int gpj_query_device(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (!f || !bc || !len || !d_out) return fail(ctx, GPJ_EINVAL, "bad arguments");
-    return query_common(ctx, f, nq, bc, len, slots, &d_out, out_count, false, nullptr);
+    return query_common(ctx, f, nq, bc, len, slots, d_out, out_count, false, nullptr);
+}
+
+int gpj_index_query_device(gpj_ctx* ctx, gpj_file* f, int num_levels, int nq, const uint8_t* const* bc,
+                           const size_t* len, int slots, int64_t* d_out, int64_t out_lines) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!f || f->ctx != ctx || !bc || !len || !d_out || out_lines < 1) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    return index_and_query(ctx, f, num_levels, nq, bc, len, slots, d_out, out_lines, nullptr);
 }
 
 int gpj_query_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths, gpj_result** out) {
@@ -730,29 +833,50 @@ int gpj_query_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths,
     }
     if (depth > GPJ_MAX_LEVELS)
         return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(depth));
-    if (!f->indexed || f->num_levels < depth) {
-        rc = gpj_index_build(ctx, f, depth);
-        if (rc) return rc;
-    }
-    gpj_result* r = new (std::nothrow) gpj_result;
-    if (!r) return fail(ctx, GPJ_ENOMEM, "out of host memory");
-    r->nq = nq;
-    r->lines = f->num_lines;
-    r->slots = slots;
-    try {
-        r->offsets.resize(static_cast<size_t>(nq) * f->num_lines * slots * 2);
-    } catch (const std::bad_alloc&) {
-        delete r;
-        return fail(ctx, GPJ_ENOMEM, "out of host memory for results");
-    }
     std::vector<const uint8_t*> bcs(static_cast<size_t>(nq));
     std::vector<size_t> lens(static_cast<size_t>(nq));
     for (int i = 0; i < nq; i++) {
         bcs[i] = compiled[i].bytecode.data();
         lens[i] = compiled[i].bytecode.size();
     }
-    rc = gpj_query(ctx, f, nq, bcs.data(), lens.data(), slots, r->offsets.data(),
-                   static_cast<int64_t>(r->offsets.size()));
+    // One pass for index and queries, with results strided by a line
+    // capacity (the known line count, else the newline-index estimate).
+    int64_t cap = f->indexed ? f->num_lines : std::min<int64_t>(f->n + 1, f->n / 256 + 1024);
+    for (int attempt = 0; attempt < 2; attempt++) {
+        rc = ensure_out(ctx, f, static_cast<size_t>(nq) * cap * slots * 2);
+        if (rc) return rc;
+        int64_t needed = 0;
+        rc = index_and_query(ctx, f, depth, nq, bcs.data(), lens.data(), slots, f->d_out, cap, &needed);
+        if (rc == GPJ_ELIMIT && needed > cap) {
+            cap = needed;
+            continue;
+        }
+        break;
+    }
+    if (rc) return rc;
+    gpj_result* r = new (std::nothrow) gpj_result;
+    if (!r) return fail(ctx, GPJ_ENOMEM, "out of host memory");
+    r->nq = nq;
+    r->lines = f->num_lines;
+    r->slots = slots;
+    const size_t per_query = static_cast<size_t>(f->num_lines) * slots * 2;
+    try {
+        r->offsets.resize(static_cast<size_t>(nq) * per_query);
+    } catch (const std::bad_alloc&) {
+        delete r;
+        return fail(ctx, GPJ_ENOMEM, "out of host memory for results");
+    }
+    const double t1 = now_ms();
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    for (int q = 0; q < nq; q++) {
+        cudaError_t e = cudaMemcpyAsync(r->offsets.data() + q * per_query, f->d_out + static_cast<size_t>(q) * cap * slots * 2,
+                                        per_query * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e != cudaSuccess) {
+            delete r;
+            return cuda_fail(ctx, e, "cudaMemcpyAsync(results)");
+        }
+    }
+    rc = end_phase(ctx, "copy_results", t1);
     if (rc) {
         delete r;
         return rc;

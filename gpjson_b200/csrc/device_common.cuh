@@ -14,6 +14,8 @@ enum DeviceError : unsigned long long {
     kErrEscapeRun = 1ull << 2,        // backslash run longer than the scan bound
     kErrIrregular = 1ull << 3,        // a line does not end outside strings at level -1
     kErrLongLine = 1ull << 4,         // a line runs further past its tile than the bound
+    kErrDeferred = 1ull << 5,         // some lines were not evaluated by the fused queries
+    kErrOutOverflow = 1ull << 6,      // a line index beyond the result buffer's capacity
 };
 
 // Poll budgets of the bounded waits (each poll also sleeps briefly).

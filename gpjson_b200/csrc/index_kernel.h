@@ -27,6 +27,15 @@ struct IndexParams {
     unsigned int* tile_counter;      // zeroed before the launch
     unsigned long long* status;      // [0] line count, [1] error bits (zeroed before)
     uint32_t epoch;                  // 1..65535
+    int materialize;                 // write string_index / leveled / newlines
+
+    // Queries evaluated in the same pass (line-parallel kernel only; 0 = none).
+    int num_queries;
+    const uint8_t* bytecode;  // all queries back to back
+    const int32_t* offsets;   // start of query q in `bytecode`
+    int slots;
+    int64_t* out;       // [num_queries][out_lines][slots][2]
+    int64_t out_lines;  // line capacity of `out` (its query stride)
 };
 
 // Exact kernel: carries string state, level and newline count across tiles

@@ -1,4 +1,5 @@
-// Line-parallel structural index for NDJSON on sm_100a (the fast path).
+// Line-parallel structural index for NDJSON on sm_100a, with the JSONPath
+// queries evaluated in the same pass (the fast path).
 //
 // In newline-delimited JSON every line is a complete value, so at each
 // '\n' the reference's scan state (Sequential.java:36-128: inside-string
@@ -6,9 +7,8 @@
 // kernel uses that: the CTA that claims a 16 KiB tile builds the index of
 // every line that starts in it, starting each line from that state, and runs
 // on past the tile end to finish its last line.  No string or level carry
-// crosses tiles, so there is no dependency chain between CTAs except the
-// newline count, which is resolved by a wide decoupled look-back after the
-// tile's work is done.
+// crosses tiles, so CTAs depend on each other only through the newline
+// count, which a wide decoupled look-back resolves after the tile's work.
 //
 // The assumption is checked, not trusted: before every '\n' the computed
 // state must be (outside, -1).  If any line breaks it (a raw newline inside
@@ -20,10 +20,18 @@
 // first '\n' of the tile (byte 0 for tile 0) to the first '\n' at or after
 // the tile end, and writes every bitmap word whose first byte lies in R_t,
 // computing all 64 bits of it with its own running state.
+//
+// Fused queries: the final string and level masks of the tile and of the
+// first 16 KiB past it stay in shared memory next to the bytes, so the CTA
+// runs the find_value interpreter (interp.cuh) on its own lines there, one
+// (line, query) pair per thread, and writes the offsets.  Lines that do not
+// fit (or whose evaluation would read past the bytes held) are flagged as
+// deferred and the host evaluates them with the find_value kernel.
 #include <cstdint>
 
 #include "device_common.cuh"
 #include "index_kernel.h"
+#include "interp.cuh"
 #include "tile_common.cuh"
 #include "word_ops.cuh"
 
@@ -32,10 +40,14 @@ namespace gpj {
 namespace {
 
 constexpr int64_t kTile = kRoundBytes;  // 16 KiB
+constexpr int kTileWords = kTile / 64;  // 256
+constexpr int kSmemWords = 2 * kTileWords;  // tile + first extension chunk
 constexpr int64_t kNone = INT64_MAX;
 // Longest run past the tile end a CTA follows to finish its last line; a
 // longer line sends the whole input to the exact kernel.
 constexpr int64_t kMaxExtension = 8ll << 20;
+// Lines of one tile whose starts are kept for the fused queries.
+constexpr int kMaxTileLines = 1024;
 constexpr unsigned long long kPayload48 = (1ull << 48) - 1;
 
 __device__ __forceinline__ unsigned long long tag48(uint32_t epoch, unsigned long long v) {
@@ -114,8 +126,13 @@ __device__ int64_t lookback_newlines(unsigned long long* agg, unsigned long long
     return acc;
 }
 
-struct __align__(128) LShared {
-    uint8_t buf[2][kTile];  // [0] the tile, [1] extension chunks
+// Shared memory of one CTA (dynamic; LV level rows of masks).
+template <int LV>
+struct LShared {
+    uint8_t buf[2][kTile];              // tile, then the first extension chunk (contiguous)
+    uint64_t str[kSmemWords];           // final in-string masks of those words
+    uint64_t lv[LV][kSmemWords];        // final level masks
+    int32_t nlpos[kMaxTileLines];       // offsets of the tile's first newlines
     uint64_t bar[2];
     Span span_scratch[kTileWarps];
     int isum[kTileWarps];
@@ -123,6 +140,7 @@ struct __align__(128) LShared {
     int64_t tile;
     int64_t ext_end;  // b_t
     int64_t nl_before;
+    int64_t smem_hi;  // bytes [tile_start, smem_hi) have final masks in shared memory
     int carry_s, carry_esc;
     int64_t carry_d;
 };
@@ -141,13 +159,13 @@ __device__ __forceinline__ void load_round(const uint8_t* file, int64_t start, i
     for (int64_t i = bulk; i < bytes; i++) dst[i] = file[start + i];
 }
 
-// Final masks of one word given its state, the level split, the stores of
-// an owned word, and the check of the '\n' bits in `check`.
+// Final masks of one word: checks the '\n' bits in `check`, stores the word
+// to shared memory at `slot` (>= 0) and to the global index when `owned`.
 template <int LV>
-__device__ __forceinline__ void finish_word(const IndexParams& p, const ClassMasks& m, uint64_t p0, int s_w,
-                                            int64_t d_w, int64_t word, bool owned, uint64_t valid,
-                                            uint64_t check) {
-    uint64_t in_str = (p0 ^ (s_w ? ~0ull : 0ull)) & valid;
+__device__ __forceinline__ void finish_word(const IndexParams& p, LShared<LV>& sh, const ClassMasks& m, uint64_t p0,
+                                            int s_w, int64_t d_w, int64_t word, bool owned, int slot,
+                                            uint64_t valid, uint64_t check) {
+    const uint64_t in_str = (p0 ^ (s_w ? ~0ull : 0ull)) & valid;
     const uint64_t open = m.open & ~in_str, close = m.close & ~in_str;
     if (check) {
         // every checked '\n' must be outside strings at level -1
@@ -161,18 +179,26 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, const ClassMas
             c &= c - 1;
         }
     }
-    if (!owned) return;
-    p.string_index[word] = in_str;
+    if (!owned && slot < 0) return;
     uint64_t lv[LV];
     split_levels<LV>(open, close, m.structural & ~in_str, d_w, lv);
+    if (slot >= 0) {
+        sh.str[slot] = in_str;
 #pragma unroll
-    for (int l = 0; l < LV; l++)
-        if (l < p.num_levels) p.leveled[p.level_size * l + word] = lv[l];
+        for (int l = 0; l < LV; l++) sh.lv[l][slot] = lv[l];
+    }
+    if (owned && p.materialize) {
+        p.string_index[word] = in_str;
+#pragma unroll
+        for (int l = 0; l < LV; l++)
+            if (l < p.num_levels) p.leveled[p.level_size * l + word] = lv[l];
+    }
 }
 
 template <int LV>
 __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p) {
-    __shared__ LShared sh;
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    LShared<LV>& sh = *reinterpret_cast<LShared<LV>*>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5;
     unsigned long long* nl_agg = p.tile_state;
     unsigned long long* nl_inc = p.tile_state + p.ntiles;
@@ -182,7 +208,6 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
         fence_mbar_init();
     }
     uint32_t phase0 = 0, phase1 = 0;
-    const int64_t words_total = (p.n + 63) >> 6;
 
     for (;;) {
         __syncthreads();  // buffers and shared slots are free
@@ -214,6 +239,14 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
         int64_t first_nl = kNone;
         const int my_nl_excl = block_sum_min(popc64(my_newlines), first_local, sh.isum, sh.imin, &tile_nl, &first_nl);
         if (tid == 0) st_release(nl_agg + t, tag48(p.epoch, static_cast<unsigned long long>(tile_nl)));
+        if (p.num_queries > 0) {
+            uint64_t nm = my_newlines;
+            int k = my_nl_excl;
+            while (nm && k < kMaxTileLines) {
+                sh.nlpos[k++] = 64 * tid + ctz64(nm);
+                nm &= nm - 1;
+            }
+        }
 
         const int64_t a_t = t == 0 ? 0 : (first_nl == kNone ? kNone : tile_start + first_nl);
         if (a_t != kNone) {
@@ -234,13 +267,16 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
             const int64_t d_w = -1 + static_cast<int64_t>(ex.dd0);
             const uint64_t check = m.newline & ~(a_t >= ws && a_t < ws + 64 ? (1ull << (a_t - ws)) : 0ull);
             if (ws < p.n)
-                finish_word<LV>(p, m, p0, s_w, d_w, ws >> 6, ws >= a_t, valid, check);
+                finish_word<LV>(p, sh, m, p0, s_w, d_w, ws >> 6, ws >= a_t, tid, valid, check);
             if (tid == kTileThreads - 1) {
                 sh.carry_s = total.q;
                 sh.carry_d = -1 + static_cast<int64_t>(total.dd0);
                 sh.carry_esc = static_cast<int>(cout);
             }
-            if (tid == 0) sh.ext_end = kNone;
+            if (tid == 0) {
+                sh.ext_end = tile_end;
+                sh.smem_hi = tile_end;
+            }
             __syncthreads();
 
             // ---- extension: finish the last line past the tile end ------------
@@ -279,7 +315,7 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
                     }
                     if (lane == 0) {
                         if (found == kNone && limit < p.n) {
-                            // a very long line: leave it to the exact kernel
+                            // a very long line: leave the input to the exact kernel
                             atomicOr(p.status + 1, kErrLongLine);
                             found = tile_end;
                         }
@@ -294,10 +330,11 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
                     if (tid == 0 && (sh.carry_s != 0 || sh.carry_d != -1)) atomicOr(p.status + 1, kErrIrregular);
                 }
                 for (int64_t cs = tile_end; cs < own_end && cs < p.n; cs += kTile) {
-                    if (tid == 0) {
-                        const int64_t bytes = p.n - cs < kTile ? p.n - cs : kTile;
-                        load_round(p.file, cs, bytes, sh.buf[1], &sh.bar[1]);
-                    }
+                    const bool first_chunk = cs == tile_end;
+                    const int64_t chunk_end = own_end < p.n ? own_end : p.n;
+                    const int64_t bytes = chunk_end - cs < kTile ? chunk_end - cs : kTile;
+                    const int nwords = static_cast<int>((bytes + 63) >> 6);
+                    if (tid == 0) load_round(p.file, cs, bytes, sh.buf[1], &sh.bar[1]);
                     if (!mbar_wait_bounded(&sh.bar[1], phase1) && tid == 0)
                         atomicOr(p.status + 1, kErrCopyTimeout);
                     phase1 ^= 1;
@@ -305,9 +342,12 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
                     const int64_t d_in = sh.carry_d;
                     const int esc_in = sh.carry_esc;
                     const int64_t cw = cs + 64 * tid;
-                    const uint64_t cvalid = bits_between(0, p.n - cw);
-                    ClassMasks e = load_classify(sh.buf[1], tid);
-                    restrict_masks(e, cvalid);
+                    const uint64_t cvalid = tid < nwords ? bits_between(0, cs + bytes - cw) : 0ull;
+                    ClassMasks e{0, 0, 0, 0, 0, 0};
+                    if (tid < nwords) {
+                        e = load_classify(sh.buf[1], tid);
+                        restrict_masks(e, cvalid);
+                    }
                     const uint32_t ecin = escape_carry_in(sh.buf[1], tid, e.backslash, 0, esc_in);
                     uint32_t ecout;
                     const uint64_t eesc = escaped_mask(e.backslash, ecin, &ecout);
@@ -320,14 +360,18 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
                     const int es_w = s_in ^ eex.q;
                     const int64_t ed_w = d_in + (s_in ? (eex.ddt - eex.dd0) : eex.dd0);
                     const uint64_t echeck = (b_t >= cw && b_t < cw + 64) ? (e.newline & (1ull << (b_t - cw))) : 0ull;
-                    if (cw < own_end && cw < p.n)
-                        finish_word<LV>(p, e, ep0, es_w, ed_w, cw >> 6, true, cvalid, echeck);
+                    if (tid < nwords)
+                        finish_word<LV>(p, sh, e, ep0, es_w, ed_w, cw >> 6, true,
+                                        first_chunk ? kTileWords + tid : -1, cvalid, echeck);
                     __syncthreads();  // everyone read the carry and the buffer
-                    if (tid == kTileThreads - 1) {
+                    if (tid == nwords - 1) {
                         sh.carry_s = s_in ^ etotal.q;
                         sh.carry_d = d_in + (s_in ? (etotal.ddt - etotal.dd0) : etotal.dd0);
                         sh.carry_esc = static_cast<int>(ecout);
                     }
+                    // the bytes stay readable for the fused queries only when the
+                    // whole extension fit in this one chunk
+                    if (tid == 0 && first_chunk && own_end <= tile_end + kTile) sh.smem_hi = cs + bytes;
                     __syncthreads();
                 }
             }
@@ -339,13 +383,14 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
             if (tid == 0) {
                 sh.nl_before = before;
                 if (t == p.ntiles - 1) p.status[0] = static_cast<unsigned long long>(before + tile_nl + 1);
-                if (t == 0 && p.newline_cap > 0) p.newlines[0] = 0;
+                if (t == 0 && p.newline_cap > 0 && p.materialize) p.newlines[0] = 0;
             }
         }
         __syncthreads();
-        {
+        const int64_t nl_before = sh.nl_before;
+        if (p.materialize) {
             uint64_t nm = my_newlines;
-            int64_t idx = 1 + sh.nl_before + my_nl_excl;
+            int64_t idx = 1 + nl_before + my_nl_excl;
             while (nm) {
                 const int bit = ctz64(nm);
                 if (idx < p.newline_cap) p.newlines[idx] = ws + bit;
@@ -353,31 +398,86 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
                 nm &= nm - 1;
             }
         }
+
+        // ---- fused queries over this tile's lines -------------------------------
+        if (p.num_queries > 0 && a_t != kNone) {
+            const int lines = tile_nl + (t == 0 ? 1 : 0);
+            if (tile_nl > kMaxTileLines) {
+                if (tid == 0) atomicOr(p.status + 1, kErrDeferred);
+            } else {
+                const int64_t b_t = sh.ext_end;
+                const int64_t hi = sh.smem_hi;
+                LineView view{sh.buf[0] - tile_start, p.n, sh.str - (tile_start >> 6),
+                              &sh.lv[0][0] - (tile_start >> 6), kSmemWords, hi};
+                const int items = lines * p.num_queries;
+                const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
+                for (int it = tid; it < items; it += kTileThreads) {
+                    const int li = it / p.num_queries, q = it - li * p.num_queries;
+                    int64_t start, end, line;
+                    if (t == 0) {
+                        start = li == 0 ? 0 : tile_start + sh.nlpos[li - 1];
+                        line = li;
+                    } else {
+                        start = tile_start + sh.nlpos[li];
+                        line = 1 + nl_before + li;
+                    }
+                    const int nxt = t == 0 ? li : li + 1;  // index in nlpos of the next line's start
+                    end = nxt < tile_nl ? tile_start + sh.nlpos[nxt] : b_t;
+                    if (line >= p.out_lines) {
+                        atomicOr(p.status + 1, kErrOutOverflow);
+                        continue;
+                    }
+                    int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + line) * per_line;
+                    for (int64_t k = 0; k < per_line; k++) res[k] = -1;
+                    if (end > hi ||
+                        run_line(view, start, end, p.bytecode + p.offsets[q], res) == kLineDeferred)
+                        atomicOr(p.status + 1, kErrDeferred);
+                }
+            }
+        }
     }
+}
+
+template <int LV>
+cudaError_t prepare() {
+    static bool done = false;
+    if (done) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(line_index_kernel<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(sizeof(LShared<LV>)));
+    if (e == cudaSuccess) done = true;
+    return e;
+}
+
+template <int LV>
+int occupancy() {
+    if (prepare<LV>() != cudaSuccess) return -1;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, line_index_kernel<LV>, kTileThreads,
+                                                      sizeof(LShared<LV>)) != cudaSuccess)
+        return -1;
+    return blocks;
+}
+
+template <int LV>
+cudaError_t launch(const IndexParams& p, int grid, cudaStream_t stream) {
+    cudaError_t e = prepare<LV>();
+    if (e != cudaSuccess) return e;
+    line_index_kernel<LV><<<grid, kTileThreads, sizeof(LShared<LV>), stream>>>(p);
+    return cudaGetLastError();
 }
 
 }  // namespace
 
 int line_index_max_ctas_per_sm(int lv) {
-    int blocks = 0;
-    cudaError_t e;
-    if (lv <= 4)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, line_index_kernel<4>, kTileThreads, 0);
-    else if (lv <= 8)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, line_index_kernel<8>, kTileThreads, 0);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, line_index_kernel<16>, kTileThreads, 0);
-    return e == cudaSuccess ? blocks : -1;
+    if (lv <= 4) return occupancy<4>();
+    if (lv <= 8) return occupancy<8>();
+    return occupancy<16>();
 }
 
 cudaError_t launch_line_index_kernel(const IndexParams& p, int grid, cudaStream_t stream) {
-    if (p.num_levels <= 4)
-        line_index_kernel<4><<<grid, kTileThreads, 0, stream>>>(p);
-    else if (p.num_levels <= 8)
-        line_index_kernel<8><<<grid, kTileThreads, 0, stream>>>(p);
-    else
-        line_index_kernel<16><<<grid, kTileThreads, 0, stream>>>(p);
-    return cudaGetLastError();
+    if (p.num_levels <= 4) return launch<4>(p, grid, stream);
+    if (p.num_levels <= 8) return launch<8>(p, grid, stream);
+    return launch<16>(p, grid, stream);
 }
 
 }  // namespace gpj

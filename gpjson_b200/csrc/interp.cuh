@@ -29,7 +29,14 @@ struct LineView {
     const uint64_t* string_index;
     const uint64_t* levels;  // [level][level_size]
     int64_t level_size;
+    // Bytes at positions >= hi are not readable through this view (hi = n
+    // for the whole file in device memory; a shared-memory view ends at the
+    // last byte it holds).  A whitespace skip that reaches hi < n cannot be
+    // finished here and the line is reported as deferred.
+    int64_t hi;
 };
+
+enum LineStatus : int { kLineDone = 0, kLineDeferred = 1 };
 
 GPJ_HD bool is_ws(uint8_t c) { return c == '\n' || c == '\r' || c == '\t' || c == ' '; }
 
@@ -78,9 +85,10 @@ GPJ_HD uint32_t read_varint(const uint8_t* ir, int& pc) {
 
 // Runs validated bytecode `ir` on the line [line_start, line_end) and writes
 // (start, end) pairs to res[2*k], res[2*k+1] for the k-th STORE_RESULT.
-// res must hold -1 on entry.
-GPJ_HD void run_line(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
-                     int64_t* res) {
+// res must hold -1 on entry.  Returns kLineDeferred when the view ends
+// before the line's evaluation does.
+GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
+                    int64_t* res) {
     int64_t level_ends[kLevelSlots];
     int64_t current_index[kLevelSlots];
     level_ends[0] = line_end;
@@ -91,6 +99,8 @@ GPJ_HD void run_line(const LineView& v, int64_t line_start, int64_t line_end, co
 
     const uint8_t* file = v.file;
     const int64_t n = v.n;
+    const int64_t hi = v.hi;
+    const int skip_end = hi < n ? kLineDeferred : kLineDone;
     int pc = 0, cur = 0, result_index = 0;
     uint8_t type = 0xFF;
     int64_t want_len = 0, want_index = -1;
@@ -103,15 +113,16 @@ GPJ_HD void run_line(const LineView& v, int64_t line_start, int64_t line_end, co
             type = ir[pc++];
             switch (type) {
                 case 0:  // END
-                    return;
+                    return kLineDone;
                 case 1:  // STORE_RESULT (find_value.cu:59-82)
-                    while (j < n && is_ws(file[j])) ++j;  // [bounded] stops at end of file
+                    while (j < hi && is_ws(file[j])) ++j;  // [bounded] stops at end of file
+                    if (j >= hi && skip_end) return kLineDeferred;
                     res[2 * result_index] = j;
                     res[2 * result_index + 1] = level_ends[cur];
                     ++result_index;
                     break;
                 case 2:  // MOVE_UP (:83-90)
-                    if (level_ends[cur] < 0) return;  // [bounded] would continue at j=-1
+                    if (level_ends[cur] < 0) return kLineDone;  // [bounded] would continue at j=-1
                     j = level_ends[cur];
                     level_ends[cur] = -1;
                     --cur;
@@ -135,10 +146,10 @@ GPJ_HD void run_line(const LineView& v, int64_t line_start, int64_t line_end, co
                     want_index = read_varint(ir, pc);
                     if (current_index[cur] == -1) {
                         for (;;) {  // [bounded] only whitespace may precede '['
-                            if (j >= n) return;
+                            if (j >= hi) return skip_end;
                             const uint8_t c = file[j];
                             if (c == '[') break;
-                            if (!is_ws(c)) return;
+                            if (!is_ws(c)) return kLineDone;
                             ++j;
                         }
                         current_index[cur] = 0;
@@ -154,19 +165,20 @@ GPJ_HD void run_line(const LineView& v, int64_t line_start, int64_t line_end, co
                     want_len = read_varint(ir, pc);
                     want = ir + pc;
                     pc += static_cast<int>(want_len);
-                    while (j < n && is_ws(file[j])) ++j;  // [bounded]
-                    if (level_ends[cur] - j != want_len) return;
+                    while (j < hi && is_ws(file[j])) ++j;  // [bounded]
+                    if (j >= hi && skip_end) return kLineDeferred;
+                    if (level_ends[cur] - j != want_len) return kLineDone;
                     for (int64_t k = 0; k < want_len; k++)
-                        if (want[k] != file[j + k]) return;
+                        if (want[k] != file[j + k]) return kLineDone;
                     break;
                 }
                 default:
-                    return;
+                    return kLineDone;
             }
         }
 
         // Searching: j is a candidate position ([bounded] only inside the file).
-        if (j < n) {
+        if (j < hi) {
             const uint64_t* lv = v.levels + v.level_size * cur;
             const bool structural = (lv[j >> 6] >> (j & 63)) & 1u;
             if (type == 4) {  // key match at a structural ':' (:225-251)
@@ -198,6 +210,7 @@ GPJ_HD void run_line(const LineView& v, int64_t line_start, int64_t line_end, co
             if (j < lim) j = next_bit(v.levels + v.level_size * cur, j, lim);
         }
     }
+    return kLineDone;
 }
 
 }  // namespace gpj

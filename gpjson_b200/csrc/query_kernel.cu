@@ -19,7 +19,7 @@ namespace {
 
 __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size};
+    LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size, p.n};
     const int64_t lines = p.num_lines;
     const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < lines;
@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
         const int64_t start = p.newlines[i];
         const int64_t end = i + 1 < lines ? p.newlines[i + 1] : p.n;
         for (int q = 0; q < p.num_queries; q++) {
-            int64_t* res = p.out + (static_cast<int64_t>(q) * lines + i) * per_line;
+            int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + i) * per_line;
             for (int64_t k = 0; k < per_line; k++) res[k] = -1;
             run_line(view, start, end, p.bytecode + p.offsets[q], res);
         }

@@ -19,7 +19,8 @@ struct QueryParams {
     const int32_t* offsets;   // start of query q in `bytecode`
     int num_queries;
     int slots;     // result slots per line (max num_results)
-    int64_t* out;  // [num_queries][num_lines][slots][2]
+    int64_t* out;       // [num_queries][out_lines][slots][2]
+    int64_t out_lines;  // query stride of `out` (>= num_lines)
 };
 
 cudaError_t launch_find_value(const QueryParams& p, int grid, cudaStream_t stream);

@@ -51,6 +51,14 @@ GPJ_HD int clz64(uint64_t x) {  // x != 0
 #endif
 }
 
+GPJ_HD uint32_t mulhi32(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+    return __umulhi(a, b);
+#else
+    return static_cast<uint32_t>((static_cast<uint64_t>(a) * b) >> 32);
+#endif
+}
+
 // 0x80 in every byte of x equal to the byte replicated in `pattern`
 // (pattern bytes < 0x80), 0 elsewhere.  Exact for all 256 byte values:
 // the low seven bits are compared with a carry-free add, bit 7 must be 0.
@@ -101,13 +109,24 @@ GPJ_HD void classify32(const uint32_t v[8], uint32_t& bs, uint32_t& qt, uint32_t
         const uint32_t fo = eq_bytes(y, 0x7B7B7B7Bu);
         const uint32_t fc = eq_bytes(y, 0x7D7D7D7Du);
         const uint32_t fs = fo | fc | eq_bytes(x, 0x3A3A3A3Au) | eq_bytes(x, 0x2C2C2C2Cu);
-        const int sh = 7 - w;
-        bs |= fb >> sh;
-        qt |= fq >> sh;
-        nl |= fn >> sh;
-        op |= fo >> sh;
-        cl |= fc >> sh;
-        st |= fs >> sh;
+        // flags of different w occupy different bits, so adding equals OR;
+        // the high half of f * 2^(25+w) is f >> (7-w) (one multiply-add)
+        if (w < 7) {
+            const uint32_t mul = 1u << (25 + w);
+            bs += mulhi32(fb, mul);
+            qt += mulhi32(fq, mul);
+            nl += mulhi32(fn, mul);
+            op += mulhi32(fo, mul);
+            cl += mulhi32(fc, mul);
+            st += mulhi32(fs, mul);
+        } else {
+            bs += fb;
+            qt += fq;
+            nl += fn;
+            op += fo;
+            cl += fc;
+            st += fs;
+        }
     }
 }
 

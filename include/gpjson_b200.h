@@ -167,6 +167,20 @@ int gpj_query_device(gpj_ctx *ctx, gpj_file *file, int nq, const uint8_t *const 
                      const size_t *bytecode_len, int result_slots, int64_t *d_out,
                      int64_t out_count);
 
+/* Builds the index of `file` with `num_levels` levels and evaluates the `nq`
+ * compiled queries in the same pass over the input: each line is indexed
+ * and queried while its bytes and bitmaps are in shared memory (the
+ * reference runs CombinedIndex, LeveledBitmapsIndex and one find_value
+ * launch per query, QueryFunction.java:165-241).  The index is kept as by
+ * gpj_index_build.  d_out: caller-owned device memory holding
+ * int64[nq][out_lines][slots][2]; out_lines must be at least the file's line
+ * count (GPJ_ELIMIT otherwise; the index is built and gpj_index_num_lines
+ * reports the count).  Lines stay -1 where a query misses; results equal
+ * running each query alone.  Synchronous. */
+int gpj_index_query_device(gpj_ctx *ctx, gpj_file *file, int num_levels, int nq,
+                           const uint8_t *const *bytecode, const size_t *bytecode_len,
+                           int result_slots, int64_t *d_out, int64_t out_lines);
+
 /* The whole reference call query(file, paths) (QueryFunction.call,
  * QueryFunction.java:48-265) on an opened file: compiles the paths, builds
  * the index with max(max_depth) levels (reusing an index that has enough

@@ -55,13 +55,18 @@ def test_multiple_paths_one_call(gpjson):
 
 
 def run_gpu(gpjson, data: bytes, paths: list[str]) -> np.ndarray:
+    """Both device paths: the fused index+query pass (gpj_query_paths) and
+    the separate index build + find_value kernel (gpj_query); they must agree."""
     compiled = [gj.compile_path(p) for p in paths]
     f = gpjson.load_bytes(data)
     try:
+        fused = f.query_paths(paths)
         f.build_index(max(c.max_depth for c in compiled))
-        return f.run(compiled)
+        separate = f.run(compiled)
     finally:
         f.release()
+    assert np.array_equal(fused, separate), "fused and separate query paths differ"
+    return fused
 
 
 @pytest.mark.gpu
@@ -130,6 +135,38 @@ def test_index_zero_of_empty_array_quirk(gpjson, tmp_path):
     with pytest.raises(gj.GPJSONException):
         result[0][0][0]
     assert result[0][1][0] == "5"
+
+
+@pytest.mark.gpu
+def test_fused_device_entry(gpjson):
+    import torch
+
+    data = datagen.tweets(12 << 20).tobytes()
+    compiled = [gj.compile_path(p) for p in TWEET_PATHS]
+    f = gpjson.load_bytes(data)
+    try:
+        f.build_index(4)
+        lines = f.num_lines
+        out = torch.full((len(compiled), lines, 1, 2), 7, dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+        for _ in range(2):
+            f.index_and_query_device(compiled, 4, out.data_ptr(), lines)
+            assert np.array_equal(out.cpu().numpy(), oracle.query(data, TWEET_PATHS))
+        small = torch.empty((len(compiled), lines - 1, 1, 2), dtype=torch.int64, device="cuda")
+        with pytest.raises(gj.GPJSONException):
+            f.index_and_query_device(compiled, 4, small.data_ptr(), lines - 1)
+    finally:
+        f.release()
+
+
+@pytest.mark.gpu
+def test_irregular_input_falls_back_exactly(gpjson):
+    good = datagen.tweets(300000).tobytes()
+    cut = good.index(b"\n", 150000)
+    data = good[:cut] + b'\n{"user": {"lang": "x\ny"}}' + good[cut:]
+    got = run_gpu(gpjson, data, TWEET_PATHS)
+    assert np.array_equal(got, oracle.query(data, TWEET_PATHS))
+    assert gpjson.timings()["exact_index_fallbacks"] >= 1
 
 
 @pytest.mark.gpu
