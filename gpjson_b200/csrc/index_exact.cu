@@ -289,9 +289,9 @@ __global__ void __launch_bounds__(kThreads) index_kernel(IndexParams p) {
         }
         ClassMasks m;
         {
-            uint32_t b0, q0, n0, o0, c0, s0, b1, q1, n1, o1, c1, s1;
-            classify32(v, b0, q0, n0, o0, c0, s0);
-            classify32(v + 8, b1, q1, n1, o1, c1, s1);
+            uint32_t b0, q0, n0, o0, c0, s0, k0, b1, q1, n1, o1, c1, s1, k1;
+            classify32(v, b0, q0, n0, o0, c0, s0, k0);
+            classify32(v + 8, b1, q1, n1, o1, c1, s1, k1);
             if (rot) {  // first classified half is the upper 32 bytes
                 m.backslash = (static_cast<uint64_t>(b0) << 32) | b1;
                 m.quote = (static_cast<uint64_t>(q0) << 32) | q1;

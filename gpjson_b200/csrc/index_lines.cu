@@ -131,6 +131,7 @@ template <int LV>
 struct LShared {
     uint8_t buf[2][kTile];              // tile, then the first extension chunk (contiguous)
     uint64_t str[kSmemWords];           // final in-string masks of those words
+    uint64_t colon[kSmemWords];         // ':' outside strings
     uint64_t lv[LV][kSmemWords];        // final level masks
     int32_t nlpos[kMaxTileLines];       // offsets of the tile's first newlines
     uint64_t bar[2];
@@ -184,6 +185,7 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, LShared<LV>& s
     split_levels<LV>(open, close, m.structural & ~in_str, d_w, lv);
     if (slot >= 0) {
         sh.str[slot] = in_str;
+        sh.colon[slot] = m.colon & ~in_str;
 #pragma unroll
         for (int l = 0; l < LV; l++) sh.lv[l][slot] = lv[l];
     }
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
                     const int esc_in = sh.carry_esc;
                     const int64_t cw = cs + 64 * tid;
                     const uint64_t cvalid = tid < nwords ? bits_between(0, cs + bytes - cw) : 0ull;
-                    ClassMasks e{0, 0, 0, 0, 0, 0};
+                    ClassMasks e{0, 0, 0, 0, 0, 0, 0};
                     if (tid < nwords) {
                         e = load_classify(sh.buf[1], tid);
                         restrict_masks(e, cvalid);
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p)
                 const int64_t b_t = sh.ext_end;
                 const int64_t hi = sh.smem_hi;
                 LineView view{sh.buf[0] - tile_start, p.n, sh.str - (tile_start >> 6),
-                              &sh.lv[0][0] - (tile_start >> 6), kSmemWords, hi};
+                              &sh.lv[0][0] - (tile_start >> 6), kSmemWords, hi, sh.colon - (tile_start >> 6)};
                 const int items = lines * p.num_queries;
                 const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
                 for (int it = tid; it < items; it += kTileThreads) {

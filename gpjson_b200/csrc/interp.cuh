@@ -34,6 +34,10 @@ struct LineView {
     // last byte it holds).  A whitespace skip that reaches hi < n cannot be
     // finished here and the line is reported as deferred.
     int64_t hi;
+    // Optional ':' outside strings, indexed like string_index.  When given,
+    // a key search jumps only between structural colons and an index search
+    // only between the other structural characters.
+    const uint64_t* colon;
 };
 
 enum LineStatus : int { kLineDone = 0, kLineDeferred = 1 };
@@ -53,6 +57,24 @@ GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit) {
         ++w;
         if ((w << 6) >= limit) return limit;
         m = bm[w];
+    }
+}
+
+// First position in [from, limit) set in bm and (in `filt`, or not in it
+// when `invert`), or `limit`.
+GPJ_HD int64_t next_bit_filtered(const uint64_t* bm, const uint64_t* filt, bool invert, int64_t from,
+                                 int64_t limit) {
+    if (from >= limit) return limit;
+    int64_t w = from >> 6;
+    uint64_t m = bm[w] & (invert ? ~filt[w] : filt[w]) & (~0ull << (from & 63));
+    for (;;) {
+        if (m) {
+            const int64_t p = (w << 6) + ctz64(m);
+            return p < limit ? p : limit;
+        }
+        ++w;
+        if ((w << 6) >= limit) return limit;
+        m = bm[w] & (invert ? ~filt[w] : filt[w]);
     }
 }
 
@@ -207,7 +229,12 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
         if (!execute) {
             // Nothing happens until the next structural bit of this level.
             const int64_t lim = level_ends[cur] < n ? level_ends[cur] : n;
-            if (j < lim) j = next_bit(v.levels + v.level_size * cur, j, lim);
+            if (j < lim) {
+                if (v.colon)
+                    j = next_bit_filtered(v.levels + v.level_size * cur, v.colon, type != 4, j, lim);
+                else
+                    j = next_bit(v.levels + v.level_size * cur, j, lim);
+            }
         }
     }
     return kLineDone;

@@ -19,7 +19,7 @@ namespace {
 
 __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size, p.n};
+    LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size, p.n, nullptr};
     const int64_t lines = p.num_lines;
     const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
     for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < lines;

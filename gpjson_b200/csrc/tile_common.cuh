@@ -34,9 +34,9 @@ __device__ __forceinline__ ClassMasks load_classify(const uint8_t* buf, int w) {
     v[4] = q1.x, v[5] = q1.y, v[6] = q1.z, v[7] = q1.w;
     v[8] = q2.x, v[9] = q2.y, v[10] = q2.z, v[11] = q2.w;
     v[12] = q3.x, v[13] = q3.y, v[14] = q3.z, v[15] = q3.w;
-    uint32_t b0, qa, n0, o0, c0, s0, b1, qb, n1, o1, c1, s1;
-    classify32(v, b0, qa, n0, o0, c0, s0);
-    classify32(v + 8, b1, qb, n1, o1, c1, s1);
+    uint32_t b0, qa, n0, o0, c0, s0, k0, b1, qb, n1, o1, c1, s1, k1;
+    classify32(v, b0, qa, n0, o0, c0, s0, k0);
+    classify32(v + 8, b1, qb, n1, o1, c1, s1, k1);
     auto join = [rot](uint32_t first, uint32_t second) {
         return rot ? ((static_cast<uint64_t>(first) << 32) | second)
                    : ((static_cast<uint64_t>(second) << 32) | first);
@@ -48,6 +48,7 @@ __device__ __forceinline__ ClassMasks load_classify(const uint8_t* buf, int w) {
     m.open = join(o0, o1);
     m.close = join(c0, c1);
     m.structural = join(s0, s1);
+    m.colon = join(k0, k1);
     return m;
 }
 
@@ -58,6 +59,7 @@ __device__ __forceinline__ void restrict_masks(ClassMasks& m, uint64_t keep) {
     m.open &= keep;
     m.close &= keep;
     m.structural &= keep;
+    m.colon &= keep;
 }
 
 // Escape state of the first byte of word w (parity of the backslash run that

@@ -86,6 +86,7 @@ struct ClassMasks {
     uint64_t open;        // '{' '['
     uint64_t close;       // '}' ']'
     uint64_t structural;  // '{' '[' '}' ']' ':' ','
+    uint64_t colon;       // ':'
 };
 
 // Classifies 32 bytes given as 8 little-endian u32 (v[j] = bytes 4j..4j+3).
@@ -94,11 +95,11 @@ struct ClassMasks {
 // result for t[w], and shifting it right by 7-w drops it on bit 8k+w: the
 // eight shifted results OR (or add) into the 32-bit mask in byte order.
 GPJ_HD void classify32(const uint32_t v[8], uint32_t& bs, uint32_t& qt, uint32_t& nl, uint32_t& op,
-                       uint32_t& cl, uint32_t& st) {
+                       uint32_t& cl, uint32_t& st, uint32_t& cn) {
     uint32_t t[8];
     transpose4(v[0], v[2], v[4], v[6], t[0], t[1], t[2], t[3]);
     transpose4(v[1], v[3], v[5], v[7], t[4], t[5], t[6], t[7]);
-    bs = qt = nl = op = cl = st = 0;
+    bs = qt = nl = op = cl = st = cn = 0;
 #pragma unroll
     for (int w = 0; w < 8; w++) {
         const uint32_t x = t[w];
@@ -108,7 +109,8 @@ GPJ_HD void classify32(const uint32_t v[8], uint32_t& bs, uint32_t& qt, uint32_t
         const uint32_t fn = eq_bytes(x, 0x0A0A0A0Au);
         const uint32_t fo = eq_bytes(y, 0x7B7B7B7Bu);
         const uint32_t fc = eq_bytes(y, 0x7D7D7D7Du);
-        const uint32_t fs = fo | fc | eq_bytes(x, 0x3A3A3A3Au) | eq_bytes(x, 0x2C2C2C2Cu);
+        const uint32_t fk = eq_bytes(x, 0x3A3A3A3Au);
+        const uint32_t fs = fo | fc | fk | eq_bytes(x, 0x2C2C2C2Cu);
         // flags of different w occupy different bits, so adding equals OR;
         // the high half of f * 2^(25+w) is f >> (7-w) (one multiply-add)
         if (w < 7) {
@@ -119,6 +121,7 @@ GPJ_HD void classify32(const uint32_t v[8], uint32_t& bs, uint32_t& qt, uint32_t
             op += mulhi32(fo, mul);
             cl += mulhi32(fc, mul);
             st += mulhi32(fs, mul);
+            cn += mulhi32(fk, mul);
         } else {
             bs += fb;
             qt += fq;
@@ -126,14 +129,15 @@ GPJ_HD void classify32(const uint32_t v[8], uint32_t& bs, uint32_t& qt, uint32_t
             op += fo;
             cl += fc;
             st += fs;
+            cn += fk;
         }
     }
 }
 
 GPJ_HD ClassMasks classify64(const uint32_t v[16]) {
-    uint32_t b0, q0, n0, o0, c0, s0, b1, q1, n1, o1, c1, s1;
-    classify32(v, b0, q0, n0, o0, c0, s0);
-    classify32(v + 8, b1, q1, n1, o1, c1, s1);
+    uint32_t b0, q0, n0, o0, c0, s0, k0, b1, q1, n1, o1, c1, s1, k1;
+    classify32(v, b0, q0, n0, o0, c0, s0, k0);
+    classify32(v + 8, b1, q1, n1, o1, c1, s1, k1);
     ClassMasks m;
     m.backslash = (static_cast<uint64_t>(b1) << 32) | b0;
     m.quote = (static_cast<uint64_t>(q1) << 32) | q0;
@@ -141,6 +145,7 @@ GPJ_HD ClassMasks classify64(const uint32_t v[16]) {
     m.open = (static_cast<uint64_t>(o1) << 32) | o0;
     m.close = (static_cast<uint64_t>(c1) << 32) | c0;
     m.structural = (static_cast<uint64_t>(s1) << 32) | s0;
+    m.colon = (static_cast<uint64_t>(k1) << 32) | k0;
     return m;
 }
 

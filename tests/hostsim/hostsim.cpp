@@ -188,7 +188,7 @@ int64_t hs_build_index_lines(const uint8_t* f, int64_t n, int num_levels, uint64
 void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t lines,
                     const uint64_t* str, const uint64_t* lvl, int nq, const uint8_t* const* irs,
                     int slots, int64_t* out) {
-    LineView v{f, n, str, lvl, (n + 63) / 64, n};
+    LineView v{f, n, str, lvl, (n + 63) / 64, n, nullptr};
     const int64_t per_query = lines * slots * 2;
     for (int64_t k = 0; k < per_query * nq; k++) out[k] = -1;
     for (int q = 0; q < nq; q++) {
