@@ -4,11 +4,11 @@
 // In newline-delimited JSON every line is a complete value, so at each
 // '\n' the reference's scan state (Sequential.java:36-128: inside-string
 // flag, level counter, escape flag) is (outside, -1, clear) again.  This
-// kernel uses that: the CTA that claims a 16 KiB tile builds the index of
+// kernel uses that: the CTA that owns a 16 KiB tile builds the index of
 // every line that starts in it, starting each line from that state, and runs
 // on past the tile end to finish its last line.  No string or level carry
 // crosses tiles, so CTAs depend on each other only through the newline
-// count, which a wide decoupled look-back resolves after the tile's work.
+// count, which a decoupled look-back resolves off the critical path.
 //
 // The assumption is checked, not trusted: before every '\n' the computed
 // state must be (outside, -1).  If any line breaks it (a raw newline inside
@@ -21,12 +21,20 @@
 // the tile end, and writes every bitmap word whose first byte lies in R_t,
 // computing all 64 bits of it with its own running state.
 //
-// Fused queries: the final string and level masks of the tile and of the
-// first 16 KiB past it stay in shared memory next to the bytes, so the CTA
-// runs the find_value interpreter (interp.cuh) on its own lines there, one
-// (line, query) pair per thread, and writes the offsets.  Lines that do not
-// fit (or whose evaluation would read past the bytes held) are flagged as
-// deferred and the host evaluates them with the find_value kernel.
+// Each CTA is a three-stage pipeline over its tiles (tile blockIdx.x, then
+// every gridDim.x-th):
+//  * copies: 1-D TMA bulk loads of tile + 4 KiB into a ring of three byte
+//    slots, issued one tile ahead;
+//  * index warps (0-7, one 64-byte word per thread): classify, resolve
+//    escapes and strings, split levels, write the index, and leave the final
+//    masks of the tile and its extension in one of two mask slots;
+//  * line warps (8-11): the newline-count look-back, the newline index, and
+//    the find_value interpreter (interp.cuh) on the tile's lines over the
+//    shared-memory masks, one (line, query) pair per thread.
+// The stages hand slots over through mbarriers, so the look-back and the
+// queries of tile k overlap the indexing of tile k+1.  Lines the line warps
+// cannot evaluate from shared memory are flagged and the host evaluates all
+// lines with the find_value kernel instead.
 #include <cstdint>
 
 #include "device_common.cuh"
@@ -39,16 +47,29 @@ namespace gpj {
 
 namespace {
 
-constexpr int64_t kTile = kRoundBytes;  // 16 KiB
-constexpr int kTileWords = kTile / 64;  // 256
-constexpr int kSmemWords = 2 * kTileWords;  // tile + first extension chunk
+constexpr int64_t kTile = kRoundBytes;               // 16 KiB
+constexpr int kTileWords = kTile / 64;               // 256
+constexpr int64_t kExtBytes = 4096;                  // extension loaded with the tile
+constexpr int64_t kSlotBytes = kTile + kExtBytes;    // 20 KiB
+constexpr int kSlotWords = kTileWords + kExtBytes / 64;  // 320
+constexpr int kRing = 3;                             // byte slots
+constexpr int kMaskSlots = 2;
+constexpr int kIndexThreads = 256;                   // warps 0-7
+constexpr int kLineThreads = 128;                    // warps 8-11
+constexpr int kThreads = kIndexThreads + kLineThreads;
+constexpr int kBarIndex = 1;                         // named barrier ids
+constexpr int kBarLines = 2;
 constexpr int64_t kNone = INT64_MAX;
 // Longest run past the tile end a CTA follows to finish its last line; a
 // longer line sends the whole input to the exact kernel.
 constexpr int64_t kMaxExtension = 8ll << 20;
 // Lines of one tile whose starts are kept for the fused queries.
-constexpr int kMaxTileLines = 1024;
+constexpr int kMaxTileLines = 512;
 constexpr unsigned long long kPayload48 = (1ull << 48) - 1;
+
+__device__ __forceinline__ void group_sync(int id, int count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
 
 __device__ __forceinline__ unsigned long long tag48(uint32_t epoch, unsigned long long v) {
     return (static_cast<unsigned long long>(epoch) << 48) | (v & kPayload48);
@@ -111,7 +132,7 @@ __device__ int64_t lookback_newlines(unsigned long long* agg, unsigned long long
                 if (lane == 0) atomicOr(status + 1, kErrLookbackTimeout);
                 break;
             }
-            __nanosleep(32);
+            __nanosleep(64);
             continue;
         }
         int64_t part = lane <= first ? lane_sum : 0;
@@ -126,29 +147,97 @@ __device__ int64_t lookback_newlines(unsigned long long* agg, unsigned long long
     return acc;
 }
 
-// Shared memory of one CTA (dynamic; LV level rows of masks).
+// What the index warps hand to the line warps about one tile.
+struct SlotInfo {
+    int64_t a;   // first line start (kNone: no line starts in the tile)
+    int64_t b;   // end of the last line
+    int64_t hi;  // bytes [tile_start, hi) have final masks in the slot
+    int tile_nl;  // newlines in the tile
+    int byte_slot;
+};
+
 template <int LV>
-struct LShared {
-    uint8_t buf[2][kTile];              // tile, then the first extension chunk (contiguous)
-    uint64_t str[kSmemWords];           // final in-string masks of those words
-    uint64_t colon[kSmemWords];         // ':' outside strings
-    uint64_t lv[LV][kSmemWords];        // final level masks
-    int32_t nlpos[kMaxTileLines];       // offsets of the tile's first newlines
-    uint64_t bar[2];
+struct FShared {
+    uint8_t bytes[kRing][kSlotBytes];
+    uint64_t str[kMaskSlots][kSlotWords];
+    uint64_t colon[kMaskSlots][kSlotWords];
+    uint64_t lv[kMaskSlots][LV][kSlotWords];
+    uint64_t nlmask[kMaskSlots][kTileWords];
+    int32_t nlexcl[kMaskSlots][kTileWords];
+    int32_t nlpos[kMaskSlots][kMaxTileLines];
+    SlotInfo info[kMaskSlots];
+    uint64_t full[kRing];   // TMA landed
+    uint64_t bfree[kRing];  // line warps done with the bytes
+    uint64_t mready[kMaskSlots];
+    uint64_t mfree[kMaskSlots];
     Span span_scratch[kTileWarps];
     int isum[kTileWarps];
     int64_t imin[kTileWarps];
-    int64_t tile;
-    int64_t ext_end;  // b_t
-    int64_t nl_before;
-    int64_t smem_hi;  // bytes [tile_start, smem_hi) have final masks in shared memory
     int carry_s, carry_esc;
     int64_t carry_d;
+    int64_t ext_b;
+    int64_t nl_before;
 };
 
-// Issues the TMA load of [start, start + bytes) into `dst` on `bar` (thread 0).
-__device__ __forceinline__ void load_round(const uint8_t* file, int64_t start, int64_t bytes, uint8_t* dst,
-                                           uint64_t* bar) {
+// Exclusive compose-scan / sum-min over the 256 index threads (named barrier).
+__device__ __forceinline__ Span index_scan_span(Span mine, Span* scratch, Span* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Span incl = mine;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const Span o = shfl_span_up(incl, off);
+        if (lane >= off) incl = span_compose(o, incl);
+    }
+    if (lane == 31) scratch[warp] = incl;
+    Span excl = shfl_span_up(incl, 1);
+    if (lane == 0) excl = span_identity();
+    group_sync(kBarIndex, kIndexThreads);
+    Span prefix = span_identity(), all = span_identity();
+#pragma unroll
+    for (int w = 0; w < kTileWarps; w++) {
+        if (w == warp) prefix = all;
+        all = span_compose(all, scratch[w]);
+    }
+    *total = all;
+    group_sync(kBarIndex, kIndexThreads);  // scratch may be reused after this
+    return span_compose(prefix, excl);
+}
+
+__device__ __forceinline__ int index_sum_min(int x, int64_t y, int* isum, int64_t* imin, int* total,
+                                             int64_t* minimum) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = x;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int o = __shfl_up_sync(~0u, incl, off);
+        if (lane >= off) incl += o;
+    }
+    int64_t mn = y;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const int64_t o = __shfl_xor_sync(~0u, mn, off);
+        mn = o < mn ? o : mn;
+    }
+    if (lane == 31) isum[warp] = incl;
+    if (lane == 0) imin[warp] = mn;
+    group_sync(kBarIndex, kIndexThreads);
+    int before = 0, all = 0;
+    int64_t m = imin[0];
+#pragma unroll
+    for (int w = 0; w < kTileWarps; w++) {
+        if (w < warp) before += isum[w];
+        all += isum[w];
+        m = imin[w] < m ? imin[w] : m;
+    }
+    *total = all;
+    *minimum = m;
+    group_sync(kBarIndex, kIndexThreads);  // scratch may be reused after this
+    return before + incl - x;
+}
+
+// Issues the TMA load of [start, start + bytes) into `dst` on `bar` (one thread).
+__device__ __forceinline__ void load_slot(const uint8_t* file, int64_t start, int64_t bytes, uint8_t* dst,
+                                          uint64_t* bar) {
     const uint32_t bulk = static_cast<uint32_t>(bytes & ~static_cast<int64_t>(15));
     fence_proxy_async_smem();
     if (bulk > 0) {
@@ -160,11 +249,37 @@ __device__ __forceinline__ void load_round(const uint8_t* file, int64_t start, i
     for (int64_t i = bulk; i < bytes; i++) dst[i] = file[start + i];
 }
 
-// Final masks of one word: checks the '\n' bits in `check`, stores the word
-// to shared memory at `slot` (>= 0) and to the global index when `owned`.
+// Loads and classifies the 64-byte word at global position `pos` straight
+// from device memory (long extensions that do not fit the slot).
+__device__ __forceinline__ ClassMasks classify_global(const uint8_t* file, int64_t n, int64_t pos) {
+    uint32_t v[16];
+    if (pos + 64 <= n) {
+        const uint4* src = reinterpret_cast<const uint4*>(file + pos);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint4 q = __ldg(src + i);
+            v[4 * i] = q.x, v[4 * i + 1] = q.y, v[4 * i + 2] = q.z, v[4 * i + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            uint32_t x = 0;
+            for (int b = 0; b < 4; b++) {
+                const int64_t q = pos + 4 * i + b;
+                if (q < n) x |= static_cast<uint32_t>(__ldg(file + q)) << (8 * b);
+            }
+            v[i] = x;
+        }
+    }
+    return classify64(v);
+}
+
+// Final masks of one word: checks the '\n' bits in `check`, keeps the word
+// in mask slot `ms` at `slot` (>= 0) and writes it to the global index when
+// `owned`.
 template <int LV>
-__device__ __forceinline__ void finish_word(const IndexParams& p, LShared<LV>& sh, const ClassMasks& m, uint64_t p0,
-                                            int s_w, int64_t d_w, int64_t word, bool owned, int slot,
+__device__ __forceinline__ void finish_word(const IndexParams& p, FShared<LV>& sh, int ms, const ClassMasks& m,
+                                            uint64_t p0, int s_w, int64_t d_w, int64_t word, bool owned, int slot,
                                             uint64_t valid, uint64_t check) {
     const uint64_t in_str = (p0 ^ (s_w ? ~0ull : 0ull)) & valid;
     const uint64_t open = m.open & ~in_str, close = m.close & ~in_str;
@@ -184,10 +299,10 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, LShared<LV>& s
     uint64_t lv[LV];
     split_levels<LV>(open, close, m.structural & ~in_str, d_w, lv);
     if (slot >= 0) {
-        sh.str[slot] = in_str;
-        sh.colon[slot] = m.colon & ~in_str;
+        sh.str[ms][slot] = in_str;
+        sh.colon[ms][slot] = m.colon & ~in_str;
 #pragma unroll
-        for (int l = 0; l < LV; l++) sh.lv[l][slot] = lv[l];
+        for (int l = 0; l < LV; l++) sh.lv[ms][l][slot] = lv[l];
     }
     if (owned && p.materialize) {
         p.string_index[word] = in_str;
@@ -197,247 +312,340 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, LShared<LV>& s
     }
 }
 
-template <int LV>
-__global__ void __launch_bounds__(kTileThreads) line_index_kernel(IndexParams p) {
-    extern __shared__ __align__(128) uint8_t smem_raw[];
-    LShared<LV>& sh = *reinterpret_cast<LShared<LV>*>(smem_raw);
-    const int tid = threadIdx.x, warp = tid >> 5;
-    unsigned long long* nl_agg = p.tile_state;
-    unsigned long long* nl_inc = p.tile_state + p.ntiles;
-    if (tid == 0) {
-        mbar_init(&sh.bar[0], 1);
-        mbar_init(&sh.bar[1], 1);
-        fence_mbar_init();
-    }
-    uint32_t phase0 = 0, phase1 = 0;
-
-    for (;;) {
-        __syncthreads();  // buffers and shared slots are free
-        if (tid == 0) {
-            const int64_t t = static_cast<int64_t>(atomicAdd(p.tile_counter, 1u));
-            sh.tile = t;
-            if (t < p.ntiles) {
-                const int64_t start = t * kTile;
-                load_round(p.file, start, p.n - start < kTile ? p.n - start : kTile, sh.buf[0], &sh.bar[0]);
+// The long tail of a line that runs past the slot: first '\n' from `from`
+// (warp 0 of the index group); flags lines beyond kMaxExtension.
+__device__ int64_t find_line_end(const IndexParams& p, int64_t from, int64_t tile_end) {
+    const int lane = threadIdx.x & 31;
+    int64_t found = kNone;
+    const int64_t limit = p.n - tile_end > kMaxExtension ? tile_end + kMaxExtension : p.n;
+    for (int64_t base = from; base < limit && found == kNone; base += 512) {
+        const int64_t q = base + 16 * lane;
+        uint64_t nlbits = 0;
+        if (q + 16 <= p.n) {
+            const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.file + q));
+            const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                uint32_t f = eq_bytes(w4[i], 0x0A0A0A0Au);
+                while (f) {
+                    nlbits |= 1ull << (4 * i + ((__ffs(f) - 1) >> 3));
+                    f &= f - 1;
+                }
             }
+        } else {
+            for (int64_t j = q; j < p.n; j++)
+                if (p.file[j] == '\n') nlbits |= 1ull << (j - q);
         }
-        __syncthreads();
-        const int64_t t = sh.tile;
-        if (t >= p.ntiles) break;
-        if (!mbar_wait_bounded(&sh.bar[0], phase0) && tid == 0) atomicOr(p.status + 1, kErrCopyTimeout);
-        phase0 ^= 1;
+        int64_t best = nlbits ? q + ctz64(nlbits) : kNone;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const int64_t o = __shfl_xor_sync(~0u, best, off);
+            best = o < best ? o : best;
+        }
+        found = best;
+    }
+    if (found == kNone && limit < p.n) {
+        if (lane == 0) atomicOr(p.status + 1, kErrLongLine);  // leave the input to the exact kernel
+        return from;
+    }
+    return found == kNone ? p.n : found;
+}
+
+// ---- index warps -------------------------------------------------------------
+template <int LV>
+__device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
+    const int tid = threadIdx.x;  // 0..255
+    unsigned long long* nl_agg = p.tile_state;
+    const int64_t first_tile = blockIdx.x, stride = gridDim.x;
+    if (tid == 0 && first_tile < p.ntiles) {
+        const int64_t start = first_tile * kTile;
+        load_slot(p.file, start, p.n - start < kSlotBytes ? p.n - start : kSlotBytes, sh.bytes[0], &sh.full[0]);
+    }
+    int64_t k = 0;
+    for (int64_t t = first_tile; t < p.ntiles; t += stride, ++k) {
+        const int bs = static_cast<int>(k % kRing), ms = static_cast<int>(k & 1);
+        const uint32_t buse = static_cast<uint32_t>(k / kRing), muse = static_cast<uint32_t>(k >> 1);
+        // start the copy of the next tile (its byte slot was last used three tiles ago)
+        if (tid == 0 && t + stride < p.ntiles) {
+            const int nb = static_cast<int>((k + 1) % kRing);
+            const uint32_t nuse = static_cast<uint32_t>((k + 1) / kRing);
+            if (nuse > 0 && !mbar_wait_bounded(&sh.bfree[nb], (nuse - 1) & 1))
+                atomicOr(p.status + 1, kErrCopyTimeout);
+            const int64_t start = (t + stride) * kTile;
+            load_slot(p.file, start, p.n - start < kSlotBytes ? p.n - start : kSlotBytes, sh.bytes[nb],
+                      &sh.full[nb]);
+        }
+        if (!mbar_wait_bounded(&sh.full[bs], buse & 1) && tid == 0) atomicOr(p.status + 1, kErrCopyTimeout);
+        const uint8_t* buf = sh.bytes[bs];
 
         const int64_t tile_start = t * kTile;
         const int64_t tile_end = p.n - tile_start < kTile ? p.n : tile_start + kTile;
+        const int64_t loaded_end = p.n - tile_start < kSlotBytes ? p.n : tile_start + kSlotBytes;
         const int64_t ws = tile_start + 64 * tid;
-        const uint64_t valid = bits_between(0, p.n - ws);
+        const uint64_t valid = bits_between(0, tile_end - ws);
 
-        // ---- round 0: the tile ---------------------------------------------
-        ClassMasks m = load_classify(sh.buf[0], tid);
+        // ---- the tile's words ---------------------------------------------
+        ClassMasks m = load_classify(buf, tid);
         restrict_masks(m, valid);
         const uint64_t my_newlines = m.newline;
         const int64_t first_local = my_newlines ? 64 * tid + ctz64(my_newlines) : kNone;
         int tile_nl = 0;
         int64_t first_nl = kNone;
-        const int my_nl_excl = block_sum_min(popc64(my_newlines), first_local, sh.isum, sh.imin, &tile_nl, &first_nl);
+        const int my_nl_excl =
+            index_sum_min(popc64(my_newlines), first_local, sh.isum, sh.imin, &tile_nl, &first_nl);
         if (tid == 0) st_release(nl_agg + t, tag48(p.epoch, static_cast<unsigned long long>(tile_nl)));
-        if (p.num_queries > 0) {
+
+        // the mask slot was last used two tiles ago
+        if (muse > 0 && !mbar_wait_bounded(&sh.mfree[ms], (muse - 1) & 1) && tid == 0)
+            atomicOr(p.status + 1, kErrCopyTimeout);
+        sh.nlmask[ms][tid] = my_newlines;
+        sh.nlexcl[ms][tid] = my_nl_excl;
+        {
             uint64_t nm = my_newlines;
-            int k = my_nl_excl;
-            while (nm && k < kMaxTileLines) {
-                sh.nlpos[k++] = 64 * tid + ctz64(nm);
+            int q = my_nl_excl;
+            while (nm && q < kMaxTileLines) {
+                sh.nlpos[ms][q++] = 64 * tid + ctz64(nm);
                 nm &= nm - 1;
             }
         }
 
         const int64_t a_t = t == 0 ? 0 : (first_nl == kNone ? kNone : tile_start + first_nl);
+        int64_t b_t = tile_end, hi = tile_end;
         if (a_t != kNone) {
             const uint64_t mine = valid & bits_between(a_t - ws, 64);
             restrict_masks(m, mine);
-            const int floor = static_cast<int>(a_t - tile_start);
-            const uint32_t cin = escape_carry_in(sh.buf[0], tid, m.backslash, floor, 0);
+            const uint32_t cin = escape_carry_in(buf, tid, m.backslash, static_cast<int>(a_t - tile_start), 0);
             uint32_t cout;
             const uint64_t esc = escaped_mask(m.backslash, cin, &cout);
             const uint64_t quotes = m.quote & ~esc;
             const uint64_t p0 = prefix_xor(quotes);
-            Span sp{popc64(quotes) & 1, popc64(m.open & ~p0) - popc64(m.close & ~p0),
-                    popc64(m.open) - popc64(m.close), 0};
+            const Span sp{popc64(quotes) & 1, popc64(m.open & ~p0) - popc64(m.close & ~p0),
+                          popc64(m.open) - popc64(m.close), 0};
             Span total;
-            const Span ex = block_scan_span(sp, sh.span_scratch, &total);
+            const Span ex = index_scan_span(sp, sh.span_scratch, &total);
             // lines start outside strings at level -1
-            const int s_w = ex.q;
-            const int64_t d_w = -1 + static_cast<int64_t>(ex.dd0);
             const uint64_t check = m.newline & ~(a_t >= ws && a_t < ws + 64 ? (1ull << (a_t - ws)) : 0ull);
-            if (ws < p.n)
-                finish_word<LV>(p, sh, m, p0, s_w, d_w, ws >> 6, ws >= a_t, tid, valid, check);
-            if (tid == kTileThreads - 1) {
-                sh.carry_s = total.q;
-                sh.carry_d = -1 + static_cast<int64_t>(total.dd0);
-                sh.carry_esc = static_cast<int>(cout);
-            }
-            if (tid == 0) {
-                sh.ext_end = tile_end;
-                sh.smem_hi = tile_end;
-            }
-            __syncthreads();
+            if (ws < tile_end)
+                finish_word<LV>(p, sh, ms, m, p0, ex.q, -1 + static_cast<int64_t>(ex.dd0), ws >> 6, ws >= a_t,
+                                tid, valid, check);
+            // state at the tile end (the last thread's word ends there)
+            const int s_in = total.q;
+            const int64_t d_in = -1 + static_cast<int64_t>(total.dd0);
+            if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(cout);
+            group_sync(kBarIndex, kIndexThreads);
+            const int esc_in = sh.carry_esc;
 
-            // ---- extension: finish the last line past the tile end ------------
+            // ---- the extension: finish the last line past the tile end -------
             if (tile_end < p.n) {
-                if (warp == 0) {
-                    // first '\n' at or after tile_end (16 bytes per lane per step)
-                    const int lane = tid & 31;
-                    int64_t found = kNone;
-                    const int64_t limit = p.n - tile_end > kMaxExtension ? tile_end + kMaxExtension : p.n;
-                    for (int64_t base = tile_end; base < limit && found == kNone; base += 512) {
-                        const int64_t q = base + 16 * lane;
-                        uint64_t nlbits = 0;
-                        if (q + 16 <= p.n) {
-                            const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.file + q));
-                            const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                            for (int i = 0; i < 4; i++) {
-                                uint32_t f = eq_bytes(w4[i], 0x0A0A0A0Au);
-                                while (f) {
-                                    nlbits |= 1ull << (4 * i + ((__ffs(f) - 1) >> 3));
-                                    f &= f - 1;
-                                }
-                            }
+                // words [tile_end, loaded_end) are in the slot already
+                const int ext_words = static_cast<int>((loaded_end - tile_end + 63) >> 6);
+                const int64_t ew = tile_end + 64 * tid;
+                const uint64_t evalid = tid < ext_words ? bits_between(0, loaded_end - ew) : 0ull;
+                ClassMasks x{0, 0, 0, 0, 0, 0, 0};
+                if (tid < ext_words) {
+                    x = load_classify(buf, kTileWords + tid);
+                    restrict_masks(x, evalid);
+                }
+                const int64_t x_first = x.newline ? ew + ctz64(x.newline) : kNone;
+                int ext_nl = 0;
+                int64_t first_ext_nl = kNone;
+                (void)index_sum_min(0, x_first, sh.isum, sh.imin, &ext_nl, &first_ext_nl);
+                if (first_ext_nl != kNone || loaded_end == p.n) {
+                    // the line ends inside the loaded extension (or at the end of the file)
+                    b_t = first_ext_nl != kNone ? first_ext_nl : p.n;
+                    hi = b_t;
+                    const int64_t own_end = (b_t + 63) & ~static_cast<int64_t>(63);
+                    const uint32_t xcin =
+                        escape_carry_in(buf, kTileWords + tid, x.backslash, kTileWords * 64, esc_in);
+                    uint32_t xcout;
+                    const uint64_t xesc = escaped_mask(x.backslash, xcin, &xcout);
+                    const uint64_t xq = x.quote & ~xesc;
+                    const uint64_t xp0 = prefix_xor(xq);
+                    const Span xs{popc64(xq) & 1, popc64(x.open & ~xp0) - popc64(x.close & ~xp0),
+                                  popc64(x.open) - popc64(x.close), 0};
+                    Span xtotal;
+                    const Span xex = index_scan_span(xs, sh.span_scratch, &xtotal);
+                    const uint64_t xcheck =
+                        (b_t >= ew && b_t < ew + 64) ? (x.newline & (1ull << (b_t - ew))) : 0ull;
+                    if (ew < own_end && tid < ext_words)
+                        finish_word<LV>(p, sh, ms, x, xp0, s_in ^ xex.q,
+                                        d_in + (s_in ? (xex.ddt - xex.dd0) : xex.dd0), ew >> 6, true,
+                                        kTileWords + tid, evalid, xcheck);
+                    if (b_t == tile_end && tid == 0 && (s_in != 0 || d_in != -1))
+                        atomicOr(p.status + 1, kErrIrregular);
+                } else {
+                    // a long line: continue past the slot straight from device memory;
+                    // no line past the tile end is kept for the queries
+                    if (tid < 32) {
+                        const int64_t e = find_line_end(p, loaded_end, tile_end);
+                        if (tid == 0) sh.ext_b = e;
+                    }
+                    group_sync(kBarIndex, kIndexThreads);
+                    b_t = sh.ext_b;
+                    hi = tile_end;
+                    const int64_t own_end = (b_t + 63) & ~static_cast<int64_t>(63);
+                    int s = s_in, esc = esc_in;
+                    int64_t d = d_in;
+                    for (int64_t cs = tile_end; cs < own_end && cs < p.n; cs += kTile) {
+                        const int64_t cw = cs + 64 * tid;
+                        const uint64_t cvalid = cw < own_end ? bits_between(0, p.n - cw) : 0ull;
+                        ClassMasks c{0, 0, 0, 0, 0, 0, 0};
+                        if (cvalid) {
+                            c = classify_global(p.file, p.n, cw);
+                            restrict_masks(c, cvalid);
+                        }
+                        // escape carry: previous word's trailing run, else the bytes before
+                        const bool all_bs = c.backslash == ~0ull;
+                        const int trail_par = all_bs ? 0 : (clz64(~c.backslash) & 1);
+                        const int prev_par = __shfl_up_sync(~0u, trail_par, 1);
+                        const int prev_all = __shfl_up_sync(~0u, all_bs ? 1 : 0, 1);
+                        uint32_t ccin;
+                        if ((tid & 31) > 0 && !prev_all) {
+                            ccin = static_cast<uint32_t>(prev_par);
                         } else {
-                            for (int64_t k = q; k < p.n; k++)
-                                if (p.file[k] == '\n') nlbits |= 1ull << (k - q);
+                            int run = 0;
+                            int64_t j = cw - 1;
+                            while (j >= cs && __ldg(p.file + j) == '\\') {
+                                ++run;
+                                --j;
+                            }
+                            ccin = static_cast<uint32_t>((run & 1) ^ (j < cs ? esc : 0));
                         }
-                        const int64_t mine_first = nlbits ? q + ctz64(nlbits) : kNone;
-                        int64_t best = mine_first;
-#pragma unroll
-                        for (int off = 16; off > 0; off >>= 1) {
-                            const int64_t o = __shfl_xor_sync(~0u, best, off);
-                            best = o < best ? o : best;
-                        }
-                        found = best;
+                        uint32_t ccout;
+                        const uint64_t cesc = escaped_mask(c.backslash, ccin, &ccout);
+                        const uint64_t cq = c.quote & ~cesc;
+                        const uint64_t cp0 = prefix_xor(cq);
+                        const Span csp{popc64(cq) & 1, popc64(c.open & ~cp0) - popc64(c.close & ~cp0),
+                                       popc64(c.open) - popc64(c.close), 0};
+                        Span ctotal;
+                        const Span cex = index_scan_span(csp, sh.span_scratch, &ctotal);
+                        const uint64_t ccheck =
+                            (b_t >= cw && b_t < cw + 64) ? (c.newline & (1ull << (b_t - cw))) : 0ull;
+                        if (cvalid)
+                            finish_word<LV>(p, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
+                                            cw >> 6, true, -1, cvalid, ccheck);
+                        if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(ccout);
+                        group_sync(kBarIndex, kIndexThreads);
+                        esc = sh.carry_esc;
+                        d += s ? (ctotal.ddt - ctotal.dd0) : ctotal.dd0;
+                        s ^= ctotal.q;
+                        group_sync(kBarIndex, kIndexThreads);
                     }
-                    if (lane == 0) {
-                        if (found == kNone && limit < p.n) {
-                            // a very long line: leave the input to the exact kernel
-                            atomicOr(p.status + 1, kErrLongLine);
-                            found = tile_end;
-                        }
-                        sh.ext_end = found == kNone ? p.n : found;
-                    }
-                }
-                __syncthreads();
-                const int64_t b_t = sh.ext_end;
-                const int64_t own_end = (b_t + 63) & ~static_cast<int64_t>(63);  // words starting before b_t
-                if (b_t == tile_end) {
-                    // the tile ends exactly at the next line: check the state there
-                    if (tid == 0 && (sh.carry_s != 0 || sh.carry_d != -1)) atomicOr(p.status + 1, kErrIrregular);
-                }
-                for (int64_t cs = tile_end; cs < own_end && cs < p.n; cs += kTile) {
-                    const bool first_chunk = cs == tile_end;
-                    const int64_t chunk_end = own_end < p.n ? own_end : p.n;
-                    const int64_t bytes = chunk_end - cs < kTile ? chunk_end - cs : kTile;
-                    const int nwords = static_cast<int>((bytes + 63) >> 6);
-                    if (tid == 0) load_round(p.file, cs, bytes, sh.buf[1], &sh.bar[1]);
-                    if (!mbar_wait_bounded(&sh.bar[1], phase1) && tid == 0)
-                        atomicOr(p.status + 1, kErrCopyTimeout);
-                    phase1 ^= 1;
-                    const int s_in = sh.carry_s;
-                    const int64_t d_in = sh.carry_d;
-                    const int esc_in = sh.carry_esc;
-                    const int64_t cw = cs + 64 * tid;
-                    const uint64_t cvalid = tid < nwords ? bits_between(0, cs + bytes - cw) : 0ull;
-                    ClassMasks e{0, 0, 0, 0, 0, 0, 0};
-                    if (tid < nwords) {
-                        e = load_classify(sh.buf[1], tid);
-                        restrict_masks(e, cvalid);
-                    }
-                    const uint32_t ecin = escape_carry_in(sh.buf[1], tid, e.backslash, 0, esc_in);
-                    uint32_t ecout;
-                    const uint64_t eesc = escaped_mask(e.backslash, ecin, &ecout);
-                    const uint64_t equotes = e.quote & ~eesc;
-                    const uint64_t ep0 = prefix_xor(equotes);
-                    Span esp{popc64(equotes) & 1, popc64(e.open & ~ep0) - popc64(e.close & ~ep0),
-                             popc64(e.open) - popc64(e.close), 0};
-                    Span etotal;
-                    const Span eex = block_scan_span(esp, sh.span_scratch, &etotal);
-                    const int es_w = s_in ^ eex.q;
-                    const int64_t ed_w = d_in + (s_in ? (eex.ddt - eex.dd0) : eex.dd0);
-                    const uint64_t echeck = (b_t >= cw && b_t < cw + 64) ? (e.newline & (1ull << (b_t - cw))) : 0ull;
-                    if (tid < nwords)
-                        finish_word<LV>(p, sh, e, ep0, es_w, ed_w, cw >> 6, true,
-                                        first_chunk ? kTileWords + tid : -1, cvalid, echeck);
-                    __syncthreads();  // everyone read the carry and the buffer
-                    if (tid == nwords - 1) {
-                        sh.carry_s = s_in ^ etotal.q;
-                        sh.carry_d = d_in + (s_in ? (etotal.ddt - etotal.dd0) : etotal.dd0);
-                        sh.carry_esc = static_cast<int>(ecout);
-                    }
-                    // the bytes stay readable for the fused queries only when the
-                    // whole extension fit in this one chunk
-                    if (tid == 0 && first_chunk && own_end <= tile_end + kTile) sh.smem_hi = cs + bytes;
-                    __syncthreads();
                 }
             }
         }
+        if (tid == 0) {
+            SlotInfo& in = sh.info[ms];
+            in.a = a_t;
+            in.b = b_t;
+            in.hi = hi;
+            in.tile_nl = tile_nl;
+            in.byte_slot = bs;
+        }
+        group_sync(kBarIndex, kIndexThreads);
+        if (tid == 0) mbar_arrive(&sh.mready[ms]);
+    }
+}
 
-        // ---- newline index ---------------------------------------------------
-        if (warp == 0) {
-            const int64_t before = lookback_newlines(nl_agg, nl_inc, t, tile_nl, p.epoch, p.status);
-            if (tid == 0) {
+// ---- line warps --------------------------------------------------------------
+template <int LV>
+__device__ void line_warps(const IndexParams& p, FShared<LV>& sh) {
+    const int lt = threadIdx.x - kIndexThreads;  // 0..127
+    unsigned long long* nl_agg = p.tile_state;
+    unsigned long long* nl_inc = p.tile_state + p.ntiles;
+    int64_t k = 0;
+    for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++k) {
+        const int ms = static_cast<int>(k & 1);
+        const uint32_t muse = static_cast<uint32_t>(k >> 1);
+        if (!mbar_wait_bounded(&sh.mready[ms], muse & 1) && lt == 0) atomicOr(p.status + 1, kErrCopyTimeout);
+        const SlotInfo in = sh.info[ms];
+        const int64_t tile_start = t * kTile;
+        if (lt < 32) {
+            const int64_t before = lookback_newlines(nl_agg, nl_inc, t, in.tile_nl, p.epoch, p.status);
+            if (lt == 0) {
                 sh.nl_before = before;
-                if (t == p.ntiles - 1) p.status[0] = static_cast<unsigned long long>(before + tile_nl + 1);
+                if (t == p.ntiles - 1) p.status[0] = static_cast<unsigned long long>(before + in.tile_nl + 1);
                 if (t == 0 && p.newline_cap > 0 && p.materialize) p.newlines[0] = 0;
             }
         }
-        __syncthreads();
+        group_sync(kBarLines, kLineThreads);
         const int64_t nl_before = sh.nl_before;
         if (p.materialize) {
-            uint64_t nm = my_newlines;
-            int64_t idx = 1 + nl_before + my_nl_excl;
-            while (nm) {
-                const int bit = ctz64(nm);
-                if (idx < p.newline_cap) p.newlines[idx] = ws + bit;
-                ++idx;
-                nm &= nm - 1;
+            for (int w = lt; w < kTileWords; w += kLineThreads) {
+                uint64_t nm = sh.nlmask[ms][w];
+                int64_t idx = 1 + nl_before + sh.nlexcl[ms][w];
+                while (nm) {
+                    const int bit = ctz64(nm);
+                    if (idx < p.newline_cap) p.newlines[idx] = tile_start + 64 * w + bit;
+                    ++idx;
+                    nm &= nm - 1;
+                }
             }
         }
-
-        // ---- fused queries over this tile's lines -------------------------------
-        if (p.num_queries > 0 && a_t != kNone) {
-            const int lines = tile_nl + (t == 0 ? 1 : 0);
-            if (tile_nl > kMaxTileLines) {
-                if (tid == 0) atomicOr(p.status + 1, kErrDeferred);
+        if (p.num_queries > 0 && in.a != kNone) {
+            if (in.tile_nl > kMaxTileLines) {
+                if (lt == 0) atomicOr(p.status + 1, kErrDeferred);
             } else {
-                const int64_t b_t = sh.ext_end;
-                const int64_t hi = sh.smem_hi;
-                LineView view{sh.buf[0] - tile_start, p.n, sh.str - (tile_start >> 6),
-                              &sh.lv[0][0] - (tile_start >> 6), kSmemWords, hi, sh.colon - (tile_start >> 6)};
+                const uint8_t* bytes = sh.bytes[in.byte_slot];
+                LineView view{bytes - tile_start, p.n, sh.str[ms] - (tile_start >> 6),
+                              &sh.lv[ms][0][0] - (tile_start >> 6), kSlotWords, in.hi,
+                              sh.colon[ms] - (tile_start >> 6)};
+                const int lines = in.tile_nl + (t == 0 ? 1 : 0);
                 const int items = lines * p.num_queries;
                 const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
-                for (int it = tid; it < items; it += kTileThreads) {
+                const int32_t* nlpos = sh.nlpos[ms];
+                for (int it = lt; it < items; it += kLineThreads) {
                     const int li = it / p.num_queries, q = it - li * p.num_queries;
-                    int64_t start, end, line;
+                    int64_t start, line;
                     if (t == 0) {
-                        start = li == 0 ? 0 : tile_start + sh.nlpos[li - 1];
+                        start = li == 0 ? 0 : tile_start + nlpos[li - 1];
                         line = li;
                     } else {
-                        start = tile_start + sh.nlpos[li];
+                        start = tile_start + nlpos[li];
                         line = 1 + nl_before + li;
                     }
-                    const int nxt = t == 0 ? li : li + 1;  // index in nlpos of the next line's start
-                    end = nxt < tile_nl ? tile_start + sh.nlpos[nxt] : b_t;
+                    const int nxt = t == 0 ? li : li + 1;
+                    const int64_t end = nxt < in.tile_nl ? tile_start + nlpos[nxt] : in.b;
                     if (line >= p.out_lines) {
                         atomicOr(p.status + 1, kErrOutOverflow);
                         continue;
                     }
                     int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + line) * per_line;
-                    for (int64_t k = 0; k < per_line; k++) res[k] = -1;
-                    if (end > hi ||
+                    for (int64_t r = 0; r < per_line; r++) res[r] = -1;
+                    if (end > in.hi ||
                         run_line(view, start, end, p.bytecode + p.offsets[q], res) == kLineDeferred)
                         atomicOr(p.status + 1, kErrDeferred);
                 }
             }
         }
+        group_sync(kBarLines, kLineThreads);
+        if (lt == 0) {
+            mbar_arrive(&sh.mfree[ms]);
+            mbar_arrive(&sh.bfree[in.byte_slot]);
+        }
     }
+}
+
+template <int LV>
+__global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) {
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    FShared<LV>& sh = *reinterpret_cast<FShared<LV>*>(smem_raw);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kRing; i++) {
+            mbar_init(&sh.full[i], 1);
+            mbar_init(&sh.bfree[i], 1);
+        }
+        for (int i = 0; i < kMaskSlots; i++) {
+            mbar_init(&sh.mready[i], 1);
+            mbar_init(&sh.mfree[i], 1);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x < kIndexThreads)
+        index_warps<LV>(p, sh);
+    else
+        line_warps<LV>(p, sh);
 }
 
 template <int LV>
@@ -445,7 +653,7 @@ cudaError_t prepare() {
     static bool done = false;
     if (done) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(line_index_kernel<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(sizeof(LShared<LV>)));
+                                         static_cast<int>(sizeof(FShared<LV>)));
     if (e == cudaSuccess) done = true;
     return e;
 }
@@ -454,8 +662,8 @@ template <int LV>
 int occupancy() {
     if (prepare<LV>() != cudaSuccess) return -1;
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, line_index_kernel<LV>, kTileThreads,
-                                                      sizeof(LShared<LV>)) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, line_index_kernel<LV>, kThreads,
+                                                      sizeof(FShared<LV>)) != cudaSuccess)
         return -1;
     return blocks;
 }
@@ -464,7 +672,7 @@ template <int LV>
 cudaError_t launch(const IndexParams& p, int grid, cudaStream_t stream) {
     cudaError_t e = prepare<LV>();
     if (e != cudaSuccess) return e;
-    line_index_kernel<LV><<<grid, kTileThreads, sizeof(LShared<LV>), stream>>>(p);
+    line_index_kernel<LV><<<grid, kThreads, sizeof(FShared<LV>), stream>>>(p);
     return cudaGetLastError();
 }
 
