@@ -18,6 +18,10 @@ enum DeviceError : unsigned long long {
     kErrOutOverflow = 1ull << 6,      // a line index beyond the result buffer's capacity
 };
 
+// Errors after which waiting for other tiles is pointless (the others are
+// notes for the host: take another path for part or all of the input).
+constexpr unsigned long long kFatalErrors = kErrLookbackTimeout | kErrCopyTimeout | kErrEscapeRun;
+
 // Poll budgets of the bounded waits (each poll also sleeps briefly).
 constexpr unsigned kMaxPolls = 1u << 22;
 

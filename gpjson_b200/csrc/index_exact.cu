@@ -171,7 +171,7 @@ __device__ Carry look_back(unsigned long long* states, int64_t t, const Span& ag
                 // Give up after the poll budget, or at once when another tile
                 // already gave up (its successors would wait for it too).
                 const bool expired = polls > kMaxPolls ||
-                                     ((polls & 1023u) == 0 && ld_acquire(status + 1) != 0);
+                                     ((polls & 1023u) == 0 && (ld_acquire(status + 1) & kFatalErrors) != 0);
                 if (expired) {
                     if (lane == 0) atomicOr(status + 1, kErrLookbackTimeout);
                     break;  // the host reports the error; outputs are not valid

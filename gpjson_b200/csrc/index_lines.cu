@@ -127,7 +127,7 @@ __device__ int64_t lookback_newlines(unsigned long long* agg, unsigned long long
         if (bad_mask & need) {
             ++polls;
             const bool expired =
-                polls > kMaxPolls || ((polls & 1023u) == 0 && ld_acquire(status + 1) != 0);
+                polls > kMaxPolls || ((polls & 1023u) == 0 && (ld_acquire(status + 1) & kFatalErrors) != 0);
             if (expired) {
                 if (lane == 0) atomicOr(status + 1, kErrLookbackTimeout);
                 break;
