@@ -12,6 +12,8 @@ from ctypes import POINTER, c_char_p, c_int, c_int64, c_size_t, c_uint8, c_uint6
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "_native" / "libgpjson_b200.so"
+# A different build of the same library (e.g. for profiling experiments).
+_LIB_OVERRIDE = "GPJSON_B200_LIB"
 
 GPJ_OK = 0
 GPJ_EINVAL = -1
@@ -80,7 +82,9 @@ def load(path: str | Path | None = None) -> ctypes.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    import os
+
+    p = Path(path) if path else Path(os.environ.get(_LIB_OVERRIDE, LIB_PATH))
     if not p.exists():
         raise RuntimeError(
             f"gpjson_b200 native library not found at {p}; build it with "

@@ -86,6 +86,18 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase)
     return false;
 }
 
+// The same for warps that may wait long (a whole pipeline stage): backs off
+// with growing sleeps so idle warps leave the issue slots to working ones.
+__device__ __forceinline__ bool mbar_wait_idle(uint64_t* bar, uint32_t phase) {
+    unsigned sleep_ns = 32;
+    for (unsigned i = 0; i < kMaxPolls; i++) {
+        if (mbar_try_wait(bar, phase)) return true;
+        __nanosleep(sleep_ns);
+        if (sleep_ns < 1024) sleep_ns <<= 1;
+    }
+    return false;
+}
+
 __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
     asm volatile("st.release.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }

@@ -369,7 +369,7 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
         if (tid == 0 && t + stride < p.ntiles) {
             const int nb = static_cast<int>((k + 1) % kRing);
             const uint32_t nuse = static_cast<uint32_t>((k + 1) / kRing);
-            if (nuse > 0 && !mbar_wait_bounded(&sh.bfree[nb], (nuse - 1) & 1))
+            if (nuse > 0 && !mbar_wait_idle(&sh.bfree[nb], (nuse - 1) & 1))
                 atomicOr(p.status + 1, kErrCopyTimeout);
             const int64_t start = (t + stride) * kTile;
             load_slot(p.file, start, p.n - start < kSlotBytes ? p.n - start : kSlotBytes, sh.bytes[nb],
@@ -396,7 +396,7 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
         if (tid == 0) st_release(nl_agg + t, tag48(p.epoch, static_cast<unsigned long long>(tile_nl)));
 
         // the mask slot was last used two tiles ago
-        if (muse > 0 && !mbar_wait_bounded(&sh.mfree[ms], (muse - 1) & 1) && tid == 0)
+        if (muse > 0 && !mbar_wait_idle(&sh.mfree[ms], (muse - 1) & 1) && tid == 0)
             atomicOr(p.status + 1, kErrCopyTimeout);
         sh.nlmask[ms][tid] = my_newlines;
         sh.nlexcl[ms][tid] = my_nl_excl;
@@ -557,7 +557,7 @@ __device__ void line_warps(const IndexParams& p, FShared<LV>& sh) {
     for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++k) {
         const int ms = static_cast<int>(k & 1);
         const uint32_t muse = static_cast<uint32_t>(k >> 1);
-        if (!mbar_wait_bounded(&sh.mready[ms], muse & 1) && lt == 0) atomicOr(p.status + 1, kErrCopyTimeout);
+        if (!mbar_wait_idle(&sh.mready[ms], muse & 1) && lt == 0) atomicOr(p.status + 1, kErrCopyTimeout);
         const SlotInfo in = sh.info[ms];
         const int64_t tile_start = t * kTile;
         if (lt < 32) {
