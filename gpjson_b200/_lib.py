@@ -54,6 +54,10 @@ SIGNATURES: dict[str, tuple] = {
         c_int,
         [c_void_p, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)],
     ),
+    "gpj_build_index_device_noalloc": (
+        c_int,
+        [c_void_p, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)],
+    ),
     "gpj_query": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_void_p), POINTER(c_size_t), c_int, c_void_p, c_int64]),
     "gpj_query_device": (
         c_int,

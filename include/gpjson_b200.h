@@ -146,6 +146,32 @@ int gpj_build_index_device(gpj_ctx *ctx, const void *d_file, int64_t n, int num_
                            uint64_t *d_string_index, uint64_t *d_leveled, int64_t *d_newlines,
                            int64_t newline_cap, int64_t *num_lines);
 
+/* Largest input gpj_build_index_device_noalloc accepts (256 MiB). */
+#define GPJ_NOALLOC_MAX_BYTES (256LL << 20)
+
+/* No counterpart in the reference (its stages allocate through
+ * CUDARuntime/cudaMalloc on every call).  Same index as
+ * gpj_build_index_device, same buffers and results, but it allocates no
+ * memory, host or device, and needs no context: the kernels' scratch (tile
+ * states, tile counter, status words) is one file-scope __device__ array of
+ * about 384 KiB per device, sized for inputs of at most GPJ_NOALLOC_MAX_BYTES;
+ * larger inputs return GPJ_ELIMIT before anything runs.
+ * It works on the calling thread's current device and on `stream` (a
+ * cudaStream_t of that device; NULL = the legacy default stream), and
+ * synchronizes that stream before returning (to read the line count).
+ * The first call on a device looks the array up (cudaGetSymbolAddress) and
+ * sets the kernels' shared-memory attributes; make it outside stream capture
+ * and before any latency-critical call.  All calls on one device share the
+ * array: calls that overlap in time, from two threads or on two streams,
+ * race and give wrong results; the caller serializes them.
+ * Returns GPJ_OK, GPJ_EINVAL, GPJ_ELIMIT (input too large, newline_cap too
+ * small, or an escape run the kernel cannot resolve), GPJ_ECUDA (CUDA error or
+ * a device that is not sm_100) or GPJ_EDEVICE (a kernel wait expired).  There
+ * is no context to carry a message; the code is the whole report. */
+int gpj_build_index_device_noalloc(void *stream, const void *d_file, int64_t n, int num_levels,
+                                   uint64_t *d_string_index, uint64_t *d_leveled,
+                                   int64_t *d_newlines, int64_t newline_cap, int64_t *num_lines);
+
 /* ---- queries ---------------------------------------------------------------- */
 
 /* Evaluates `nq` compiled queries (bytecode from gpj_compile) over every line
