@@ -35,7 +35,7 @@ QUERIES = ["$.user.lang", "$.id", "$.user.followers_count", "$.entities.hashtags
 FILE_BYTES = 1 << 31
 LEVELS = 4
 TILE = 16384
-PROFILE_TRAFFIC = ROOT / "profiles" / "traffic.json"
+PROFILE_TRAFFIC = ROOT / "profiles" / "dram_traffic_tweets_256MiB.json"
 
 
 def parse_args(argv=None):
@@ -48,9 +48,10 @@ def parse_args(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample", type=int, default=512 << 20, help="bytes of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["fused", "index", "separate"], default="fused",
-                    help="fused: index+queries in one launch; index: index only (diagnostic); "
-                         "separate: index launch then the find_value launch")
+    ap.add_argument("--mode", choices=["default", "fused", "index"], default="default",
+                    help="default: gpj_index_query_device as shipped (index kernel, then one find_value "
+                         "launch for all queries); fused: the queries evaluated inside the index kernel; "
+                         "index: index only (diagnostic)")
     return ap.parse_args(argv)
 
 
@@ -71,6 +72,12 @@ def max_over_ranks(value: float, world: int, device=None) -> float:
     t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job_gbs(world: int, bytes_per_rank: int, ms_per_step: float) -> float:
+    """Input GB/s of the whole job: every rank indexes its own file of
+    bytes_per_rank bytes per step; the step time is the slowest rank's."""
+    return world * bytes_per_rank / (ms_per_step / 1000) / 1e9
 
 
 def barrier(world: int, device=None) -> None:
@@ -147,7 +154,7 @@ def measured_peak_gbs() -> tuple[float, str]:
 
 def ncu_traffic(key: str):
     """DRAM bytes per launch of the index kernel from the committed ncu
-    summary (profiles/traffic.json), scaled to this input size."""
+    summary (profiles/dram_traffic_tweets_256MiB.json), scaled to this input size."""
     if not PROFILE_TRAFFIC.exists():
         return None
     try:
@@ -276,18 +283,17 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     lines = f.num_lines
     out = torch.empty((len(QUERIES), lines, slots, 2), dtype=torch.int64, device=device)
 
+    g.set_query_fusion(args.mode == "fused")
+
     def step(ev=None):
-        """One pass: index (4 levels) + the 4 queries fused, input in HBM."""
+        """One pass: index (4 levels) + the 4 queries in one pass over it, input in HBM."""
         if ev:
             ev[0].record(stream)
-        if args.mode == "fused":
+        if args.mode == "index":
+            g._native.check(lib.gpj_index_build(ctx, f._h, LEVELS))
+        else:
             g._native.check(lib.gpj_index_query_device(ctx, f._h, LEVELS, len(compiled), ptrs, lens, slots,
                                                        out.data_ptr(), lines))
-        else:
-            g._native.check(lib.gpj_index_build(ctx, f._h, LEVELS))
-            if args.mode == "separate":
-                g._native.check(lib.gpj_query_device(ctx, f._h, len(compiled), ptrs, lens, slots, out.data_ptr(),
-                                                     out.numel()))
         if ev:
             ev[1].record(stream)
 
@@ -297,6 +303,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
 
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
     launches0 = g.kernel_launches()
+    lib.gpj_reset_timings(ctx)
     clocks = ClockSampler(local)
     clocks.start()
     barrier(world, device)
@@ -311,14 +318,21 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     barrier(world, device)
     clock_info = clocks.stop()
     launches = g.kernel_launches() - launches0
+    # per-kernel device times: the library brackets each kernel phase with
+    # CUDA events on this same stream (gpj_get_timings)
+    phase_ms: dict[str, list[float]] = {}
+    for ph in g.timings()["phases"]:
+        phase_ms.setdefault(ph["name"], []).append(ph["device_ms"])
+    kernel_ms = {k: statistics.mean(v) for k, v in phase_ms.items()}
     total_ms = start.elapsed_time(end)
     pass_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
     total_ms = max_over_ranks(total_ms, world, device)
     ms_per_step = total_ms / args.steps
-    value = world * n / (ms_per_step / 1000) / 1e9
+    value = whole_job_gbs(world, n, ms_per_step)
 
     # correctness spot check of the timed output against one solo pass
     if args.mode != "index":
+        g.set_query_fusion(False)
         solo = f.run(compiled)
         assert np.array_equal(solo, out.cpu().numpy()), "device results differ from a solo pass"
 
@@ -343,13 +357,17 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         assert np.array_equal(res_host.numpy(), out.cpu().numpy()), "e2e results differ"
     e2e_value = world * n / e2e_s / 1e9
 
-    # ---- roofline of the dominant (only) kernel --------------------------------
-    # The fused pass reads the input once and writes the index (string
-    # bitmap, LEVELS level bitmaps, newline offsets) and the query offsets.
+    # ---- roofline of the dominant kernel ----------------------------------------
+    # Algorithmic bytes of one index (+query) pass = the input bytes n (each
+    # byte is read once; the index it writes is reported beside it).  The
+    # dominant kernel is the line-parallel index kernel (phase
+    # "build_index", or "index_and_query" when the queries run inside it).
     peak, peak_kind = measured_peak_gbs()
     words = (n + 63) // 64
-    alg = n + 8 * words * (1 + LEVELS) + 8 * lines + 16 * len(QUERIES) * lines * slots
-    achieved = alg / (pass_ms / 1000) / 1e9
+    index_bytes = 8 * words * (1 + LEVELS) + 8 * lines
+    dom = "index_and_query" if "index_and_query" in kernel_ms else "build_index"
+    dom_ms = kernel_ms[dom]
+    achieved = n / (dom_ms / 1000) / 1e9
     traffic = None
     t = ncu_traffic("line_index_kernel")
     if t and t.get("bytes") and t.get("input_bytes"):
@@ -370,23 +388,26 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         "data": "synthetic",
         "config": {
             "workload": f"tweet-like NDJSON, {n} B per GPU ({lines} lines), one index build ({LEVELS} levels) "
-                        "+ 4 queries fused in one pass",
+                        "+ 4 queries fused in one pass over it",
+            "mode": args.mode,
             "queries": QUERIES,
             "bytes_per_gpu": n,
             "lines_per_gpu": lines,
             "l2": "input larger than L2 (2 GiB vs 126 MB)",
             "parallelism": f"replicas x{world} (one file per GPU)",
         },
-        "kernels_ms": {args.mode: round(pass_ms, 4)},
+        "pass_ms": round(pass_ms, 4),
+        "kernels_ms": {k: round(v, 4) for k, v in kernel_ms.items()},
         "roofline": {
             "bound": "hbm",
-            "kernel": "line_index_kernel (index + 4 queries, one launch)",
+            "kernel": "line_index_kernel" + (" (with the 4 queries)" if dom == "index_and_query" else ""),
             "achieved": round(achieved, 1),
             "peak": peak,
             "unit": "GB/s",
             "frac": round(achieved / peak, 4),
             "traffic": traffic,
-            "algorithmic_bytes": alg,
+            "algorithmic_bytes": n,
+            "index_bytes_written": index_bytes,
             "peak_kind": f"{peak_kind} copy bandwidth",
         },
         "step_frac_of_hbm": round(value / world / peak, 4),

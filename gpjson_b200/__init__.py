@@ -130,7 +130,7 @@ class ResultItem(Sequence):
             return None
         if end < start:
             # The reference builds new byte[end - start] here and fails with
-            # NegativeArraySizeException (ResultItem.java:190).
+            # NegativeArraySizeException (ResultItem.java:47).
             raise GPJSONException(f"result ({start}, {end}) has no end offset")
         return self._array.file_bytes[start:end].decode("utf-8", "replace")
 
@@ -379,6 +379,11 @@ class GPJSON:
         h = c_void_p()
         self._native.check(self._native.lib.gpj_file_from_device(self._native.h, c_void_p(ptr), n, byref(h)))
         return File(self._native, h, keepalive=keepalive)
+
+    def set_query_fusion(self, enabled: bool) -> None:
+        """Evaluate queries inside the index kernel (True) or with one
+        find_value launch after it (False, the default)."""
+        self._native.check(self._native.lib.gpj_set_query_fusion(self._native.h, 1 if enabled else 0))
 
     def set_stream(self, stream_handle: int | None) -> None:
         self._native.check(self._native.lib.gpj_set_stream(self._native.h, c_void_p(stream_handle or 0)))

@@ -49,6 +49,7 @@ struct gpj_ctx {
     int index_occupancy[3] = {0, 0, 0};  // exact kernel, levels <=4, <=8, <=16
     int line_occupancy[3] = {0, 0, 0};   // line-parallel kernel
     int64_t exact_fallbacks = 0;         // builds that needed the exact kernel
+    bool fuse_queries = false;           // evaluate queries inside the index kernel
     int query_occupancy = 0;
 
     // pinned staging for file reads
@@ -195,6 +196,7 @@ struct FusedQueries {
     int nq = 0;
     int slots = 0;
     const uint8_t* bytecode = nullptr;
+    int bytecode_bytes = 0;
     const int32_t* offsets = nullptr;
     int64_t* out = nullptr;
     int64_t out_lines = 0;  // query stride of `out`
@@ -229,6 +231,7 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
     if (fq && fq->nq > 0) {
         fused.num_queries = fq->nq;
         fused.bytecode = fq->bytecode;
+        fused.bytecode_bytes = fq->bytecode_bytes;
         fused.offsets = fq->offsets;
         fused.slots = fq->slots;
         fused.out = fq->out;
@@ -404,12 +407,27 @@ int index_and_query(gpj_ctx* ctx, gpj_file* f, int num_levels, int nq, const uin
     if (depth > num_levels)
         return fail(ctx, GPJ_ELIMIT, "queries need " + std::to_string(depth) + " levels, the index is built with " +
                                          std::to_string(num_levels));
+    if (!ctx->fuse_queries) {
+        // index kernel, then one find_value launch for all queries
+        rc = index_pass(ctx, f, num_levels, nullptr, nullptr);
+        if (rc) return rc;
+        if (lines_needed) *lines_needed = f->num_lines;
+        if (f->num_lines > out_lines)
+            return fail(ctx, GPJ_ELIMIT, "result buffer holds " + std::to_string(out_lines) +
+                                             " lines, the file has " + std::to_string(f->num_lines));
+        const double t1 = now_ms();
+        GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+        rc = launch_query(ctx, f, nq, slots, d_out, out_lines);
+        if (rc) return rc;
+        return end_phase(ctx, "find_value", t1);
+    }
     FusedQueries fq;
     fq.nq = nq;
     fq.slots = slots;
     const size_t header = ((static_cast<size_t>(nq) * 4 + 15) / 16) * 16;
     fq.offsets = reinterpret_cast<const int32_t*>(f->d_ir);
     fq.bytecode = f->d_ir + header;
+    fq.bytecode_bytes = static_cast<int>(f->ir_host.size() - header);
     fq.out = d_out;
     fq.out_lines = out_lines;
     bool done = false;
@@ -536,6 +554,13 @@ void gpj_destroy(gpj_ctx* ctx) {
 }
 
 const char* gpj_last_error(const gpj_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+int gpj_set_query_fusion(gpj_ctx* ctx, int enabled) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    ctx->fuse_queries = enabled != 0;
+    return GPJ_OK;
+}
 
 int gpj_set_stream(gpj_ctx* ctx, void* stream) {
     int rc = check_ctx(ctx);

@@ -32,6 +32,7 @@ struct IndexParams {
     // Queries evaluated in the same pass (line-parallel kernel only; 0 = none).
     int num_queries;
     const uint8_t* bytecode;  // all queries back to back
+    int bytecode_bytes;       // total length of `bytecode`
     const int32_t* offsets;   // start of query q in `bytecode`
     int slots;
     int64_t* out;       // [num_queries][out_lines][slots][2]

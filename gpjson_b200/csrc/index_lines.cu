@@ -30,7 +30,8 @@
 //    masks of the tile and its extension in one of two mask slots;
 //  * line warps (8-11): the newline-count look-back, the newline index, and
 //    the find_value interpreter (interp.cuh) on the tile's lines over the
-//    shared-memory masks, one (line, query) pair per thread.
+//    shared-memory masks, one (line, query) pair per thread, a warp's lanes
+//    on one query.
 // The stages hand slots over through mbarriers, so the look-back and the
 // queries of tile k overlap the indexing of tile k+1.  Lines the line warps
 // cannot evaluate from shared memory are flagged and the host evaluates all
@@ -65,6 +66,10 @@ constexpr int64_t kNone = INT64_MAX;
 constexpr int64_t kMaxExtension = 8ll << 20;
 // Lines of one tile whose starts are kept for the fused queries.
 constexpr int kMaxTileLines = 512;
+// Bytecode of the fused queries kept in shared memory (else read from
+// device memory).
+constexpr int kIrBytes = 2048;
+constexpr int kIrQueries = 256;
 constexpr unsigned long long kPayload48 = (1ull << 48) - 1;
 
 __device__ __forceinline__ void group_sync(int id, int count) {
@@ -165,6 +170,11 @@ struct FShared {
     uint64_t nlmask[kMaskSlots][kTileWords];
     int32_t nlexcl[kMaskSlots][kTileWords];
     int32_t nlpos[kMaskSlots][kMaxTileLines];
+    // interpreter state of the line threads (PackedLevels), level-major
+    int32_t lvl_end[LV + 1][kLineThreads];
+    int32_t lvl_idx[LV + 1][kLineThreads];
+    uint8_t ir[kIrBytes];
+    int32_t ir_off[kIrQueries];
     SlotInfo info[kMaskSlots];
     uint64_t full[kRing];   // TMA landed
     uint64_t bfree[kRing];  // line warps done with the bytes
@@ -553,6 +563,15 @@ __device__ void line_warps(const IndexParams& p, FShared<LV>& sh) {
     const int lt = threadIdx.x - kIndexThreads;  // 0..127
     unsigned long long* nl_agg = p.tile_state;
     unsigned long long* nl_inc = p.tile_state + p.ntiles;
+    // the queries' bytecode, from shared memory when it fits
+    const bool ir_local = p.num_queries > 0 && p.num_queries <= kIrQueries && p.bytecode_bytes <= kIrBytes;
+    if (ir_local) {
+        for (int i = lt; i < p.bytecode_bytes; i += kLineThreads) sh.ir[i] = p.bytecode[i];
+        for (int i = lt; i < p.num_queries; i += kLineThreads) sh.ir_off[i] = p.offsets[i];
+        group_sync(kBarLines, kLineThreads);
+    }
+    const uint8_t* ir_base = ir_local ? sh.ir : p.bytecode;
+    const int32_t* ir_off = ir_local ? sh.ir_off : p.offsets;
     int64_t k = 0;
     for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++k) {
         const int ms = static_cast<int>(k & 1);
@@ -591,11 +610,16 @@ __device__ void line_warps(const IndexParams& p, FShared<LV>& sh) {
                               &sh.lv[ms][0][0] - (tile_start >> 6), kSlotWords, in.hi,
                               sh.colon[ms] - (tile_start >> 6)};
                 const int lines = in.tile_nl + (t == 0 ? 1 : 0);
-                const int items = lines * p.num_queries;
+                // a warp runs one query on up to 32 lines, so its lanes follow
+                // the same opcode sequence
+                const int chunks = (lines + 31) >> 5;
+                const int tasks = chunks * p.num_queries;
                 const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
                 const int32_t* nlpos = sh.nlpos[ms];
-                for (int it = lt; it < items; it += kLineThreads) {
-                    const int li = it / p.num_queries, q = it - li * p.num_queries;
+                for (int task = lt >> 5; task < tasks; task += kLineThreads / 32) {
+                    const int q = task / chunks;
+                    const int li = ((task - q * chunks) << 5) + (lt & 31);
+                    if (li >= lines) continue;
                     int64_t start, line;
                     if (t == 0) {
                         start = li == 0 ? 0 : tile_start + nlpos[li - 1];
@@ -612,8 +636,9 @@ __device__ void line_warps(const IndexParams& p, FShared<LV>& sh) {
                     }
                     int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + line) * per_line;
                     for (int64_t r = 0; r < per_line; r++) res[r] = -1;
+                    PackedLevels lv{&sh.lvl_end[0][lt], &sh.lvl_idx[0][lt], kLineThreads, LV + 1, start};
                     if (end > in.hi ||
-                        run_line(view, start, end, p.bytecode + p.offsets[q], res) == kLineDeferred)
+                        run_line_with(view, start, end, ir_base + ir_off[q], res, lv) == kLineDeferred)
                         atomicOr(p.status + 1, kErrDeferred);
                 }
             }

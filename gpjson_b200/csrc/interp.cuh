@@ -105,19 +105,59 @@ GPJ_HD uint32_t read_varint(const uint8_t* ir, int& pc) {
     return v | (b << shift);
 }
 
+// Per-level state of the interpreter: level_ends[k] (the end of the value
+// entered at level k, -1 unknown) and current_index[k] (the array element
+// counter, -1 before the array's '[' is reached).
+//
+// In registers/local memory, for every level a query may reach.
+struct LocalLevels {
+    int64_t ends[kLevelSlots];
+    int64_t index[kLevelSlots];
+    GPJ_HD void reset(int64_t line_end) {
+        ends[0] = line_end;
+#pragma unroll
+        for (int k = 1; k < kLevelSlots; k++) ends[k] = -1;
+#pragma unroll
+        for (int k = 0; k < kLevelSlots; k++) index[k] = -1;
+    }
+    GPJ_HD int64_t end(int k) const { return ends[k]; }
+    GPJ_HD void set_end(int k, int64_t v) { ends[k] = v; }
+    GPJ_HD int64_t idx(int k) const { return index[k]; }
+    GPJ_HD void set_idx(int k, int64_t v) { index[k] = v; }
+};
+
+// In caller-provided storage (e.g. shared memory, entries `stride` apart),
+// as 32-bit offsets from the line start: for lines shorter than 2 GiB and
+// queries no deeper than `slots - 1` levels.
+struct PackedLevels {
+    int32_t* ends;
+    int32_t* index;
+    int stride;
+    int slots;
+    int64_t origin;
+    static constexpr int32_t kUnset = INT32_MIN;
+    GPJ_HD void reset(int64_t line_end) {
+        ends[0] = static_cast<int32_t>(line_end - origin);
+        for (int k = 1; k < slots; k++) ends[k * stride] = kUnset;
+        for (int k = 0; k < slots; k++) index[k * stride] = -1;
+    }
+    GPJ_HD int64_t end(int k) const {
+        const int32_t v = ends[k * stride];
+        return v == kUnset ? -1 : origin + v;
+    }
+    GPJ_HD void set_end(int k, int64_t v) { ends[k * stride] = v < 0 ? kUnset : static_cast<int32_t>(v - origin); }
+    GPJ_HD int64_t idx(int k) const { return index[k * stride]; }
+    GPJ_HD void set_idx(int k, int64_t v) { index[k * stride] = static_cast<int32_t>(v); }
+};
+
 // Runs validated bytecode `ir` on the line [line_start, line_end) and writes
 // (start, end) pairs to res[2*k], res[2*k+1] for the k-th STORE_RESULT.
 // res must hold -1 on entry.  Returns kLineDeferred when the view ends
-// before the line's evaluation does.
-GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
-                    int64_t* res) {
-    int64_t level_ends[kLevelSlots];
-    int64_t current_index[kLevelSlots];
-    level_ends[0] = line_end;
-#pragma unroll
-    for (int k = 1; k < kLevelSlots; k++) level_ends[k] = -1;
-#pragma unroll
-    for (int k = 0; k < kLevelSlots; k++) current_index[k] = -1;
+// before the line's evaluation does.  `lv` holds the per-level state.
+template <typename Levels>
+GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
+                         int64_t* res, Levels& lv) {
+    lv.reset(line_end);
 
     const uint8_t* file = v.file;
     const int64_t n = v.n;
@@ -130,7 +170,7 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
     bool execute = true;
 
     int64_t j = line_start;
-    while (j < level_ends[cur] && j < n) {
+    while (j < lv.end(cur) && j < n) {
         while (execute) {
             type = ir[pc++];
             switch (type) {
@@ -140,21 +180,21 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
                     while (j < hi && is_ws(file[j])) ++j;  // [bounded] stops at end of file
                     if (j >= hi && skip_end) return kLineDeferred;
                     res[2 * result_index] = j;
-                    res[2 * result_index + 1] = level_ends[cur];
+                    res[2 * result_index + 1] = lv.end(cur);
                     ++result_index;
                     break;
                 case 2:  // MOVE_UP (:83-90)
-                    if (level_ends[cur] < 0) return kLineDone;  // [bounded] would continue at j=-1
-                    j = level_ends[cur];
-                    level_ends[cur] = -1;
+                    if (lv.end(cur) < 0) return kLineDone;  // [bounded] would continue at j=-1
+                    j = lv.end(cur);
+                    lv.set_end(cur, -1);
                     --cur;
                     break;
                 case 3: {  // MOVE_DOWN (:91-111): end of the value = next structural one level up
                     ++cur;
-                    if (level_ends[cur] == -1) {
-                        const int64_t lim = level_ends[cur - 1];
+                    if (lv.end(cur) == -1) {
+                        const int64_t lim = lv.end(cur - 1);
                         const int64_t m = next_bit(v.levels + v.level_size * (cur - 1), j + 1, lim);
-                        if (m < lim) level_ends[cur] = m;
+                        if (m < lim) lv.set_end(cur, m);
                     }
                     break;
                 }
@@ -166,7 +206,7 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
                     break;
                 case 5:  // MOVE_TO_INDEX (:131-169)
                     want_index = read_varint(ir, pc);
-                    if (current_index[cur] == -1) {
+                    if (lv.idx(cur) == -1) {
                         for (;;) {  // [bounded] only whitespace may precede '['
                             if (j >= hi) return skip_end;
                             const uint8_t c = file[j];
@@ -174,7 +214,7 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
                             if (!is_ws(c)) return kLineDone;
                             ++j;
                         }
-                        current_index[cur] = 0;
+                        lv.set_idx(cur, 0);
                     }
                     if (want_index == 0) {
                         ++j;
@@ -189,7 +229,7 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
                     pc += static_cast<int>(want_len);
                     while (j < hi && is_ws(file[j])) ++j;  // [bounded]
                     if (j >= hi && skip_end) return kLineDeferred;
-                    if (level_ends[cur] - j != want_len) return kLineDone;
+                    if (lv.end(cur) - j != want_len) return kLineDone;
                     for (int64_t k = 0; k < want_len; k++)
                         if (want[k] != file[j + k]) return kLineDone;
                     break;
@@ -201,8 +241,8 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
 
         // Searching: j is a candidate position ([bounded] only inside the file).
         if (j < hi) {
-            const uint64_t* lv = v.levels + v.level_size * cur;
-            const bool structural = (lv[j >> 6] >> (j & 63)) & 1u;
+            const uint64_t* bits = v.levels + v.level_size * cur;
+            const bool structural = (bits[j >> 6] >> (j & 63)) & 1u;
             if (type == 4) {  // key match at a structural ':' (:225-251)
                 if (structural && file[j] == ':') {
                     const int64_t string_end = prev_bit(v.string_index, j - 1, line_start);
@@ -220,15 +260,17 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
                 }
             } else if (type == 5) {  // index match at a structural ',' (:252-259)
                 if (structural && file[j] == ',') {
-                    ++current_index[cur];
-                    if (want_index == current_index[cur]) execute = true;
+                    const int64_t count = lv.idx(cur) + 1;
+                    lv.set_idx(cur, count);
+                    if (want_index == count) execute = true;
                 }
             }
         }
         ++j;
         if (!execute) {
             // Nothing happens until the next structural bit of this level.
-            const int64_t lim = level_ends[cur] < n ? level_ends[cur] : n;
+            const int64_t end = lv.end(cur);
+            const int64_t lim = end < n ? end : n;
             if (j < lim) {
                 if (v.colon)
                     j = next_bit_filtered(v.levels + v.level_size * cur, v.colon, type != 4, j, lim);
@@ -238,6 +280,11 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
         }
     }
     return kLineDone;
+}
+
+GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir, int64_t* res) {
+    LocalLevels lv;
+    return run_line_with(v, line_start, line_end, ir, res, lv);
 }
 
 }  // namespace gpj

@@ -44,7 +44,7 @@ extern "C" {
 #define GPJ_EUNSUPPORTED (-3) /* UnsupportedJSONPathException; GPJSON would fall back to
                                  Jayway JsonPath on the CPU (QueryFunction.java:122-128),
                                  which this library does not provide */
-#define GPJ_ECUDA (-4)        /* a CUDA runtime call failed (GPJSONException.java:64-70) */
+#define GPJ_ECUDA (-4)        /* a CUDA runtime call failed (GPJSONException.java:33-39) */
 #define GPJ_ENOMEM (-5)       /* device or pinned-host allocation failed */
 #define GPJ_EIO (-6)          /* the input file could not be opened or read */
 #define GPJ_ELIMIT (-7)       /* a documented limit was exceeded */
@@ -53,7 +53,7 @@ extern "C" {
 
 /* Limits kept from the reference. */
 #define GPJ_MAX_QUERIES 255   /* QueryFunction.java:74-77 */
-#define GPJ_MAX_LEVELS 16     /* LeveledBitmapsIndex.java:168,183-185 */
+#define GPJ_MAX_LEVELS 16     /* LeveledBitmapsIndex.java:16,31-33 */
 
 typedef struct gpj_ctx gpj_ctx;
 typedef struct gpj_file gpj_file;
@@ -76,6 +76,14 @@ const char *gpj_last_error(const gpj_ctx *ctx);
  * the context's own stream).  The reference runs everything synchronously on
  * the legacy default stream (CUDARuntime.java:388). */
 int gpj_set_stream(gpj_ctx *ctx, void *stream);
+
+/* How gpj_index_query_device and gpj_query_paths evaluate queries: 0 (the
+ * default) builds the index with one kernel and then evaluates all queries
+ * with one find_value launch; 1 evaluates them inside the index kernel, on
+ * the tile's masks in shared memory, where the input allows (well-formed
+ * NDJSON, lines that fit a tile's look-ahead) and finishes the rest with
+ * find_value.  Results are identical either way. */
+int gpj_set_query_fusion(gpj_ctx *ctx, int enabled);
 
 /* Library version string, e.g. "gpjson_b200 0.1 sm_100a". */
 const char *gpj_version(void);

@@ -9,9 +9,9 @@
  * Parity status: pinned.  The restatement follows
  *   gpjson/src/main/java/com/koenv/gpjson/sequential/Sequential.java
  * line by line, widened to 64-bit offsets, and is checked against the
- * reference's own known answers (QueryFunctionTest.java:147-259) and
- * fixture-derived stage expectations (StringIndexTest.java:368-453,
- * NewlineIndexTest.java:245-278, LeveledBitmapsIndexTest.java:94-163).
+ * reference's own known answers (QueryFunctionTest.java:86-198) and
+ * fixture-derived stage expectations (StringIndexTest.java:109-175,
+ * NewlineIndexTest.java:81-115, LeveledBitmapsIndexTest.java:94-164).
  *
  * Where the reference is undefined (Java exception, device assert or
  * out-of-bounds access) this oracle fixes one behaviour and the CUDA path

@@ -40,7 +40,8 @@ def hostsim():
     L.hs_build_index_lines.restype = ctypes.c_int64
     L.hs_build_index_lines.argtypes = [P, ctypes.c_int64, ctypes.c_int, P, P, P, ctypes.c_int64]
     L.hs_find_values.restype = None
-    L.hs_find_values.argtypes = [P, ctypes.c_int64, P, ctypes.c_int64, P, P, ctypes.c_int, P, ctypes.c_int, P]
+    L.hs_find_values.argtypes = [P, ctypes.c_int64, P, ctypes.c_int64, P, P, ctypes.c_int, P, ctypes.c_int, P, P,
+                                 ctypes.c_int]
     L.hs_escaped_mask.restype = ctypes.c_uint64
     L.hs_escaped_mask.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
     return L

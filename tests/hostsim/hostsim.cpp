@@ -184,18 +184,28 @@ int64_t hs_build_index_lines(const uint8_t* f, int64_t n, int num_levels, uint64
 }
 
 // Runs each query's bytecode on every line with the device interpreter.
-// out: [nq][lines][slots][2], filled with -1 here.
+// out: [nq][lines][slots][2], filled with -1 here.  `colon` (may be null)
+// is the bitmap of ':' outside strings that the fused kernel's key searches
+// jump along; `packed` selects the 32-bit level state the fused kernel keeps
+// in shared memory.
 void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t lines,
                     const uint64_t* str, const uint64_t* lvl, int nq, const uint8_t* const* irs,
-                    int slots, int64_t* out) {
-    LineView v{f, n, str, lvl, (n + 63) / 64, n, nullptr};
+                    int slots, int64_t* out, const uint64_t* colon, int packed) {
+    LineView v{f, n, str, lvl, (n + 63) / 64, n, colon};
     const int64_t per_query = lines * slots * 2;
     for (int64_t k = 0; k < per_query * nq; k++) out[k] = -1;
+    int32_t ends[kLevelSlots], index[kLevelSlots];
     for (int q = 0; q < nq; q++) {
         for (int64_t i = 0; i < lines; i++) {
             const int64_t start = nl[i];
             const int64_t end = i + 1 < lines ? nl[i + 1] : n;
-            run_line(v, start, end, irs[q], out + q * per_query + i * slots * 2);
+            int64_t* res = out + q * per_query + i * slots * 2;
+            if (packed) {
+                PackedLevels lv{ends, index, 1, kLevelSlots, start};
+                run_line_with(v, start, end, irs[q], res, lv);
+            } else {
+                run_line(v, start, end, irs[q], res);
+            }
         }
     }
 }

@@ -55,17 +55,24 @@ def test_multiple_paths_one_call(gpjson):
 
 
 def run_gpu(gpjson, data: bytes, paths: list[str]) -> np.ndarray:
-    """Both device paths: the fused index+query pass (gpj_query_paths) and
-    the separate index build + find_value kernel (gpj_query); they must agree."""
+    """Every device path: gpj_query_paths with the queries evaluated inside
+    the index kernel and after it, and the separate index build + find_value
+    call (gpj_query); they must agree."""
     compiled = [gj.compile_path(p) for p in paths]
     f = gpjson.load_bytes(data)
     try:
-        fused = f.query_paths(paths)
+        two_pass = f.query_paths(paths)
+        gpjson.set_query_fusion(True)
+        try:
+            fused = f.query_paths(paths)
+        finally:
+            gpjson.set_query_fusion(False)
         f.build_index(max(c.max_depth for c in compiled))
         separate = f.run(compiled)
     finally:
         f.release()
-    assert np.array_equal(fused, separate), "fused and separate query paths differ"
+    assert np.array_equal(fused, separate), "in-kernel and separate query paths differ"
+    assert np.array_equal(two_pass, separate), "two-pass and separate query paths differ"
     return fused
 
 
@@ -149,9 +156,16 @@ def test_fused_device_entry(gpjson):
         lines = f.num_lines
         out = torch.full((len(compiled), lines, 1, 2), 7, dtype=torch.int64, device="cuda")
         torch.cuda.synchronize()
-        for _ in range(2):
-            f.index_and_query_device(compiled, 4, out.data_ptr(), lines)
-            assert np.array_equal(out.cpu().numpy(), oracle.query(data, TWEET_PATHS))
+        want = oracle.query(data, TWEET_PATHS)
+        for fusion in (False, True, False):
+            gpjson.set_query_fusion(fusion)
+            try:
+                for _ in range(2):
+                    out.fill_(7)
+                    f.index_and_query_device(compiled, 4, out.data_ptr(), lines)
+                    assert np.array_equal(out.cpu().numpy(), want), fusion
+            finally:
+                gpjson.set_query_fusion(False)
         small = torch.empty((len(compiled), lines - 1, 1, 2), dtype=torch.int64, device="cuda")
         with pytest.raises(gj.GPJSONException):
             f.index_and_query_device(compiled, 4, small.data_ptr(), lines - 1)

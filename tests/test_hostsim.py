@@ -114,6 +114,15 @@ def test_line_parallel_rejects_irregular(hostsim):
     check_index(hostsim, good[:cut] + b'\n{"s":"\\\\\\"\\\\","t":[{}]}' + good[cut:], 4, expect_regular=True)
 
 
+def colon_bitmap(f: np.ndarray, strings: np.ndarray) -> np.ndarray:
+    """':' bytes outside strings, one bit per byte (the fused kernel's colon mask)."""
+    words = strings.size
+    in_str = np.unpackbits(strings.view(np.uint8), bitorder="little")[: f.size].astype(bool)
+    bits = np.zeros(words * 64, dtype=np.uint8)
+    bits[: f.size] = (f == ord(":")) & ~in_str
+    return np.packbits(bits, bitorder="little").view(np.uint64).copy()
+
+
 def test_interpreter_matches_oracle(hostsim):
     rng = random.Random(3)
     base = [
@@ -139,9 +148,12 @@ def test_interpreter_matches_oracle(hostsim):
             want = oracle.find_value(data, idx.newlines, idx.strings, idx.levels, depth, ir, slots)
             f = np.frombuffer(data, dtype=np.uint8)
             irb = np.frombuffer(ir, dtype=np.uint8)
-            got = np.empty_like(want)
             ptrs = (ctypes.c_void_p * 1)(irb.ctypes.data)
-            hostsim.hs_find_values(f.ctypes.data, f.size, idx.newlines.ctypes.data, len(idx.newlines),
-                                   idx.strings.ctypes.data, idx.levels.ctypes.data, 1, ptrs, slots,
-                                   got.ctypes.data)
-            assert np.array_equal(got, want), (path, data[:120])
+            colon = colon_bitmap(f, idx.strings)
+            # plain, with the fused kernel's colon jumps, and with its packed level state
+            for colon_ptr, packed in ((None, 0), (colon.ctypes.data, 0), (colon.ctypes.data, 1)):
+                got = np.empty_like(want)
+                hostsim.hs_find_values(f.ctypes.data, f.size, idx.newlines.ctypes.data, len(idx.newlines),
+                                       idx.strings.ctypes.data, idx.levels.ctypes.data, 1, ptrs, slots,
+                                       got.ctypes.data, colon_ptr, packed)
+                assert np.array_equal(got, want), (path, data[:120], colon_ptr is not None, packed)

@@ -15,24 +15,24 @@ from tests.conftest import GOLDEN, fixture_bytes
 SIMPLE = "query_gpu_function/simple_single_line.ldjson"
 NOT_FOUND = "query_gpu_function/not_found_in_current_level.ldjson"
 
-# QueryFunctionTest.java:147-228: (path, values over all lines and slots)
+# QueryFunctionTest.java:86-167: (path, values over all lines and slots)
 KNOWN_ANSWERS = [
-    ("$.user.lang", ['"nl"']),  # :148-153
-    ("$.user.id", ["8723"]),  # :156-161
-    ("$.user.foo", [None]),  # :164-169
-    ("$.apple.lang", [None]),  # :172-177
-    ("$.user.values[0]", ['"12"']),  # :180-185
-    ("$.user.values[2]", ["14"]),  # :188-193
-    ("$.user.values[8]", [None]),  # :196-201
-    ("$.user.values[0:3]", ['"12"', '"13"', "14"]),  # :204-211
-    ("$.user.values[2:4]", ["14", '"15"']),  # :214-220
-    ("$.user.lang[?(@ == 'nl')]", ['"nl"']),  # :223-228
+    ("$.user.lang", ['"nl"']),  # :86-92
+    ("$.user.id", ["8723"]),  # :94-100
+    ("$.user.foo", [None]),  # :102-108
+    ("$.apple.lang", [None]),  # :110-116
+    ("$.user.values[0]", ['"12"']),  # :118-124
+    ("$.user.values[2]", ["14"]),  # :126-132
+    ("$.user.values[8]", [None]),  # :134-140
+    ("$.user.values[0:3]", ['"12"', '"13"', "14"]),  # :142-150
+    ("$.user.values[2:4]", ["14", '"15"']),  # :152-159
+    ("$.user.lang[?(@ == 'nl')]", ['"nl"']),  # :161-167
 ]
 
 
 def values(data: bytes, offsets: np.ndarray) -> list:
-    """resultToValues (QueryFunctionTest.java:273-291) over ResultItem
-    semantics (ResultItem.java:180-194)."""
+    """resultToValues (QueryFunctionTest.java:212-230) over ResultItem
+    semantics (ResultItem.java:32-52)."""
     out = []
     for start, end in offsets.reshape(-1, 2):
         out.append(None if start == -1 else data[start:end].decode("utf-8"))
@@ -46,7 +46,7 @@ def test_known_answers(path, expected):
 
 
 def test_key_not_found_in_current_level():
-    # QueryFunctionTest.java:231-259: $.a.a has no non-null value
+    # QueryFunctionTest.java:169-198: $.a.a has no non-null value
     data = fixture_bytes(NOT_FOUND)
     assert all(v is None for v in values(data, oracle.query(data, ["$.a.a"])))
 
