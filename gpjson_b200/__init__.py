@@ -373,6 +373,14 @@ class GPJSON:
         )
         return File(self._native, h, host_bytes=bytes(arr.tobytes()) if arr.size < (1 << 26) else arr)
 
+    def load_bytes_indexed(self, data: bytes | bytearray | memoryview | np.ndarray, num_levels: int) -> File:
+        """gpj_file_from_host_indexed: copy and index in one pipelined call."""
+        arr = np.frombuffer(data, dtype=np.uint8) if not isinstance(data, np.ndarray) else data
+        h = c_void_p()
+        self._native.check(self._native.lib.gpj_file_from_host_indexed(
+            self._native.h, arr.ctypes.data, arr.size, num_levels, byref(h)))
+        return File(self._native, h, host_bytes=bytes(arr.tobytes()) if arr.size < (1 << 26) else arr)
+
     def from_device(self, ptr: int, n: int, keepalive=None) -> File:
         """Wraps n bytes already in device memory (e.g. a torch uint8 tensor's
         data_ptr()); `keepalive` is held for the File's lifetime."""

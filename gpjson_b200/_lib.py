@@ -59,6 +59,7 @@ SIGNATURES: dict[str, tuple] = {
         [c_void_p, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)],
     ),
     "gpj_set_query_fusion": (c_int, [c_void_p, c_int]),
+    "gpj_file_from_host_indexed": (c_int, [c_void_p, c_void_p, c_int64, c_int, POINTER(c_void_p)]),
     "gpj_query": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_void_p), POINTER(c_size_t), c_int, c_void_p, c_int64]),
     "gpj_query_device": (
         c_int,

@@ -37,6 +37,12 @@ struct gpj_ctx {
     int sms = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // host-to-device copies overlapped with indexing
+    // Device buffers come from this stream-ordered pool; freed blocks stay
+    // reserved for the next file instead of going back to the driver.
+    cudaMemPool_t pool = nullptr;
+    std::vector<cudaEvent_t> chunk_events;  // one per loaded chunk
+    cudaEvent_t ev_ready = nullptr;
     std::string err;
 
     // scratch of the index kernel
@@ -112,10 +118,12 @@ int cuda_fail(gpj_ctx* ctx, cudaError_t e, const char* what) {
         if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call); \
     } while (0)
 
+// Stream-ordered allocation from the context's pool on the context's stream
+// (other streams that touch the buffer wait for an event recorded after it).
 template <typename T>
 int device_alloc(gpj_ctx* ctx, T** p, size_t count, const char* what) {
     void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16));
+    cudaError_t e = cudaMallocFromPoolAsync(&q, std::max<size_t>(count * sizeof(T), 16), ctx->pool, ctx->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return cuda_fail(ctx, e, what);
@@ -125,8 +133,8 @@ int device_alloc(gpj_ctx* ctx, T** p, size_t count, const char* what) {
 }
 
 template <typename T>
-void device_free(T*& p) {
-    if (p) cudaFree(p);
+void device_free(gpj_ctx* ctx, T*& p) {
+    if (p) cudaFreeAsync(p, ctx->stream);
     p = nullptr;
 }
 
@@ -149,7 +157,7 @@ int end_phase(gpj_ctx* ctx, const char* name, double host_start) {
 int ensure_tile_state(gpj_ctx* ctx, int64_t ntiles) {
     const int64_t words = 3 * ntiles;
     if (words > ctx->tile_state_words) {
-        device_free(ctx->d_tile_state);
+        device_free(ctx, ctx->d_tile_state);
         ctx->tile_state_words = 0;
         const int64_t cap = std::max<int64_t>(words, 3 * 4096);
         int rc = device_alloc(ctx, &ctx->d_tile_state, static_cast<size_t>(cap), "cudaMalloc(tile state)");
@@ -191,6 +199,17 @@ int launch_index(gpj_ctx* ctx, bool exact, const gpj::IndexParams& base) {
     return GPJ_OK;
 }
 
+// Maps the error word of an index launch to a status code and message.
+int status_error(gpj_ctx* ctx, unsigned long long errs) {
+    if (!(errs & ~(gpj::kErrDeferred | gpj::kErrOutOverflow))) return GPJ_OK;
+    std::string m = "index kernel reported:";
+    if (errs & gpj::kErrLookbackTimeout) m += " look-back wait expired;";
+    if (errs & gpj::kErrCopyTimeout) m += " TMA copy wait expired;";
+    if (errs & gpj::kErrEscapeRun) m += " a backslash run longer than 64 KiB crosses a 16 KiB tile boundary;";
+    if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) m += " unexpected line check failure;";
+    return fail(ctx, (errs & gpj::kErrEscapeRun) ? GPJ_ELIMIT : GPJ_EDEVICE, m);
+}
+
 // Queries evaluated by the index pass (packed bytecode already on device).
 struct FusedQueries {
     int nq = 0;
@@ -227,6 +246,9 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
     p.newlines = d_nl;
     p.newline_cap = nl_cap;
     p.materialize = 1;
+    p.tile_begin = 0;
+    p.tile_end = p.ntiles;
+    p.avail = n;
     gpj::IndexParams fused = p;
     if (fq && fq->nq > 0) {
         fused.num_queries = fq->nq;
@@ -248,15 +270,8 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
         if (rc) return rc;
         errs = ctx->h_status[1];
     }
-    if (errs & ~(gpj::kErrDeferred | gpj::kErrOutOverflow)) {
-        std::string m = "index kernel reported:";
-        if (errs & gpj::kErrLookbackTimeout) m += " look-back wait expired;";
-        if (errs & gpj::kErrCopyTimeout) m += " TMA copy wait expired;";
-        if (errs & gpj::kErrEscapeRun)
-            m += " a backslash run longer than 64 KiB crosses a 16 KiB tile boundary;";
-        if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) m += " unexpected line check failure;";
-        return fail(ctx, (errs & gpj::kErrEscapeRun) ? GPJ_ELIMIT : GPJ_EDEVICE, m);
-    }
+    rc = status_error(ctx, errs);
+    if (rc) return rc;
     *lines = static_cast<int64_t>(ctx->h_status[0]);
     if (queries_done && fq && fq->nq > 0)
         *queries_done = !exact && !(errs & (gpj::kErrDeferred | gpj::kErrOutOverflow)) && *lines <= fq->out_lines;
@@ -302,7 +317,7 @@ int upload_queries(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, 
     *depth_needed = deepest;
     if (packed == f->ir_host && f->d_ir) return GPJ_OK;
     if (packed.size() > f->d_ir_cap) {
-        device_free(f->d_ir);
+        device_free(ctx, f->d_ir);
         f->d_ir_cap = 0;
         int rc = device_alloc(ctx, &f->d_ir, packed.size() * 2, "cudaMalloc(bytecode)");
         if (rc) return rc;
@@ -351,7 +366,7 @@ int ensure_index_buffers(gpj_ctx* ctx, gpj_file* f, int num_levels) {
     if (!f->d_str && (rc = device_alloc(ctx, &f->d_str, static_cast<size_t>(f->words), "cudaMalloc(string index)")))
         return rc;
     if (f->lvl_cap < num_levels) {
-        device_free(f->d_lvl);
+        device_free(ctx, f->d_lvl);
         f->lvl_cap = 0;
         rc = device_alloc(ctx, &f->d_lvl, static_cast<size_t>(f->words) * num_levels, "cudaMalloc(leveled bitmaps)");
         if (rc) return rc;
@@ -379,7 +394,7 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
                    queries_done);
     if (rc) return rc;
     if (lines > f->nl_cap) {  // more lines than the first guess: size exactly and rebuild
-        device_free(f->d_nl);
+        device_free(ctx, f->d_nl);
         f->nl_cap = lines;
         rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(lines), "cudaMalloc(newline index)");
         if (rc) return rc;
@@ -388,6 +403,107 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
         if (rc) return rc;
     }
     rc = end_phase(ctx, fq && fq->nq ? "index_and_query" : "build_index", t0);
+    if (rc) return rc;
+    f->num_lines = lines;
+    f->num_levels = num_levels;
+    f->indexed = true;
+    return GPJ_OK;
+}
+
+// Bytes copied per step of load_and_index; a multiple of the tile size.
+constexpr int64_t kLoadChunk = 64ll << 20;
+
+// Copies n host bytes into f->d_owned in chunks on the copy stream and
+// indexes chunk k with the line-parallel kernel as soon as chunk k + 1 has
+// landed (a line starting in chunk k ends in chunk k + 1 unless it is longer
+// than a chunk), so the copy and the index build overlap.  Inputs the line
+// kernel cannot index this way (not NDJSON, or a line longer than a chunk)
+// are indexed again from the complete copy by run_index.
+int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_levels) {
+    const int64_t n = f->n;
+    int rc = ensure_index_buffers(ctx, f, num_levels);
+    if (rc) return rc;
+    f->indexed = false;
+    const double t0 = now_ms();
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    const int64_t nchunks = (n + kLoadChunk - 1) / kLoadChunk;
+    int64_t lines = 0;
+    if (nchunks <= 1) {
+        if (n > 0)
+            GPJ_CUDA(ctx, cudaMemcpyAsync(f->d_owned, host, static_cast<size_t>(n), cudaMemcpyHostToDevice,
+                                          ctx->stream));
+        rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
+        if (rc) return rc;
+    } else {
+        while (static_cast<int64_t>(ctx->chunk_events.size()) < nchunks) {
+            cudaEvent_t e = nullptr;
+            GPJ_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            ctx->chunk_events.push_back(e);
+        }
+        gpj::IndexParams p{};
+        p.file = f->d_data;
+        p.n = n;
+        p.ntiles = (n + gpj::kIndexTileBytes - 1) / gpj::kIndexTileBytes;
+        p.string_index = f->d_str;
+        p.leveled = f->d_lvl;
+        p.level_size = f->words;
+        p.num_levels = num_levels;
+        p.newlines = f->d_nl;
+        p.newline_cap = f->nl_cap;
+        p.materialize = 1;
+        rc = ensure_tile_state(ctx, p.ntiles);  // one epoch for all launches of this build
+        if (rc) return rc;
+        GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned int), ctx->stream));
+        GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
+        p.tile_state = ctx->d_tile_state;
+        p.tile_counter = ctx->d_counter;
+        p.status = ctx->d_status;
+        p.epoch = ctx->epoch;
+        // the copies start once the buffers exist (pool allocations are ordered on ctx->stream)
+        GPJ_CUDA(ctx, cudaEventRecord(ctx->ev_ready, ctx->stream));
+        GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0));
+        const int64_t tiles_per_chunk = kLoadChunk / gpj::kIndexTileBytes;
+        const int occ = ctx->line_occupancy[occupancy_slot(num_levels)];
+        auto launch_chunk = [&](int64_t k) -> int {
+            p.tile_begin = k * tiles_per_chunk;
+            p.tile_end = std::min(p.ntiles, (k + 1) * tiles_per_chunk);
+            p.avail = std::min(n, (k + 2) * kLoadChunk);
+            GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->chunk_events[std::min(k + 1, nchunks - 1)], 0));
+            const int64_t grid = std::min<int64_t>(p.tile_end - p.tile_begin, static_cast<int64_t>(ctx->sms) * occ);
+            GPJ_CUDA(ctx, gpj::launch_line_index_kernel(p, static_cast<int>(grid), ctx->stream));
+            ctx->launches++;
+            return GPJ_OK;
+        };
+        for (int64_t k = 0; k < nchunks; k++) {
+            const int64_t pos = k * kLoadChunk;
+            const size_t len = static_cast<size_t>(std::min(kLoadChunk, n - pos));
+            GPJ_CUDA(ctx, cudaMemcpyAsync(f->d_owned + pos, host + pos, len, cudaMemcpyHostToDevice, ctx->copy_stream));
+            GPJ_CUDA(ctx, cudaEventRecord(ctx->chunk_events[k], ctx->copy_stream));
+            if (k >= 1 && (rc = launch_chunk(k - 1))) return rc;
+        }
+        if ((rc = launch_chunk(nchunks - 1))) return rc;
+        GPJ_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(unsigned long long),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        const unsigned long long errs = ctx->h_status[1];
+        lines = static_cast<int64_t>(ctx->h_status[0]);
+        if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) {
+            // the whole input is on the device now: index it in one launch (exact fallback inside)
+            rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
+            if (rc) return rc;
+        } else if ((rc = status_error(ctx, errs))) {
+            return rc;
+        }
+    }
+    if (lines > f->nl_cap) {  // more lines than the first guess: size exactly and rebuild
+        device_free(ctx, f->d_nl);
+        f->nl_cap = lines;
+        rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(lines), "cudaMalloc(newline index)");
+        if (rc) return rc;
+        rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
+        if (rc) return rc;
+    }
+    rc = end_phase(ctx, "load_and_index", t0);
     if (rc) return rc;
     f->num_lines = lines;
     f->num_levels = num_levels;
@@ -480,7 +596,7 @@ int query_common(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, co
 
 int ensure_out(gpj_ctx* ctx, gpj_file* f, size_t elems) {
     if (elems <= f->d_out_cap) return GPJ_OK;
-    device_free(f->d_out);
+    device_free(ctx, f->d_out);
     f->d_out_cap = 0;
     int rc = device_alloc(ctx, &f->d_out, elems, "cudaMalloc(results)");
     if (rc) return rc;
@@ -520,6 +636,20 @@ int gpj_create(int device, gpj_ctx** out) {
     if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess)
         return bail(e, "cudaStreamCreate");
     ctx->stream = ctx->own_stream;
+    if ((e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(e, "cudaStreamCreate(copy)");
+    if ((e = cudaEventCreateWithFlags(&ctx->ev_ready, cudaEventDisableTiming)) != cudaSuccess)
+        return bail(e, "cudaEventCreate");
+    {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if ((e = cudaMemPoolCreate(&ctx->pool, &props)) != cudaSuccess) return bail(e, "cudaMemPoolCreate");
+        uint64_t keep = UINT64_MAX;  // freed blocks stay in the pool until gpj_destroy
+        if ((e = cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess)
+            return bail(e, "cudaMemPoolSetAttribute");
+    }
     if ((e = cudaMalloc(&ctx->d_counter, 16)) != cudaSuccess) return bail(e, "cudaMalloc(counter)");
     if ((e = cudaMalloc(&ctx->d_status, 16)) != cudaSuccess) return bail(e, "cudaMalloc(status)");
     if ((e = cudaMallocHost(&ctx->h_status, 16)) != cudaSuccess) return bail(e, "cudaMallocHost(status)");
@@ -541,10 +671,21 @@ int gpj_create(int device, gpj_ctx** out) {
 void gpj_destroy(gpj_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
-    if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
-    device_free(ctx->d_tile_state);
-    device_free(ctx->d_counter);
-    device_free(ctx->d_status);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream) {
+        ctx->stream = ctx->own_stream;
+        device_free(ctx, ctx->d_tile_state);
+        cudaStreamSynchronize(ctx->own_stream);
+    }
+    if (ctx->d_counter) cudaFree(ctx->d_counter);
+    if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->copy_stream) {
+        cudaStreamSynchronize(ctx->copy_stream);
+        cudaStreamDestroy(ctx->copy_stream);
+    }
+    for (cudaEvent_t e : ctx->chunk_events) cudaEventDestroy(e);
+    if (ctx->ev_ready) cudaEventDestroy(ctx->ev_ready);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -565,6 +706,8 @@ int gpj_set_query_fusion(gpj_ctx* ctx, int enabled) {
 int gpj_set_stream(gpj_ctx* ctx, void* stream) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
+    // work (and pool frees) queued on the old stream finish first
+    GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
     return GPJ_OK;
 }
@@ -635,6 +778,30 @@ int gpj_file_from_host(gpj_ctx* ctx, const void* data, int64_t n, gpj_file** out
         return cuda_fail(ctx, e, "cudaMemcpyAsync(file)");
     }
     rc = end_phase(ctx, "copy_file", t0);
+    if (rc) {
+        gpj_file_release(f);
+        return rc;
+    }
+    *out = f;
+    return GPJ_OK;
+}
+
+int gpj_file_from_host_indexed(gpj_ctx* ctx, const void* data, int64_t n, int num_levels, gpj_file** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out || n < 0 || (n > 0 && !data)) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (num_levels < 1 || num_levels > GPJ_MAX_LEVELS)
+        return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(num_levels));
+    gpj_file* f = nullptr;
+    rc = make_file(ctx, n, &f);
+    if (rc) return rc;
+    rc = device_alloc(ctx, &f->d_owned, static_cast<size_t>(n), "cudaMalloc(file)");
+    if (rc) {
+        delete f;
+        return rc;
+    }
+    f->d_data = f->d_owned;
+    rc = load_and_index(ctx, f, static_cast<const uint8_t*>(data), num_levels);
     if (rc) {
         gpj_file_release(f);
         return rc;
@@ -724,12 +891,15 @@ void gpj_file_release(gpj_file* f) {
         cudaSetDevice(f->ctx->device);
         cudaStreamSynchronize(f->ctx->stream);
     }
-    device_free(f->d_owned);
-    device_free(f->d_str);
-    device_free(f->d_lvl);
-    device_free(f->d_nl);
-    device_free(f->d_ir);
-    device_free(f->d_out);
+    if (f->ctx) {
+        gpj_ctx* ctx = f->ctx;
+        device_free(ctx, f->d_owned);
+        device_free(ctx, f->d_str);
+        device_free(ctx, f->d_lvl);
+        device_free(ctx, f->d_nl);
+        device_free(ctx, f->d_ir);
+        device_free(ctx, f->d_out);
+    }
     delete f;
 }
 

@@ -144,6 +144,9 @@ extern "C" int gpj_build_index_device_noalloc(void* stream_handle, const void* d
     p.newlines = d_newlines;
     p.newline_cap = newline_cap;
     p.materialize = 1;
+    p.tile_begin = 0;
+    p.tile_end = p.ntiles;
+    p.avail = n;
 
     unsigned long long status[2] = {0, 0};
     int rc = launch(d, false, p, stream, status);

@@ -28,6 +28,15 @@ struct IndexParams {
     unsigned long long* status;      // [0] line count, [1] error bits (zeroed before)
     uint32_t epoch;                  // 1..65535
     int materialize;                 // write string_index / leveled / newlines
+    // Line-parallel kernel only: this launch indexes tiles [tile_begin,
+    // tile_end) (earlier tiles were indexed by earlier launches of the same
+    // build, with the same epoch), and only bytes [0, avail) of the file may
+    // be read (the rest may still be on its way from the host; avail is n or
+    // a multiple of 64 at or past the end of the last tile's following
+    // tile).  A line that runs past `avail` is flagged kErrLongLine.
+    int64_t tile_begin;
+    int64_t tile_end;
+    int64_t avail;
 
     // Queries evaluated in the same pass (line-parallel kernel only; 0 = none).
     int num_queries;

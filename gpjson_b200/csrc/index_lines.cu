@@ -36,6 +36,7 @@
 // queries of tile k overlap the indexing of tile k+1.  Lines the line warps
 // cannot evaluate from shared memory are flagged and the host evaluates all
 // lines with the find_value kernel instead.
+#include <atomic>
 #include <cstdint>
 
 #include "device_common.cuh"
@@ -327,7 +328,8 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, FShared<LV>& s
 __device__ int64_t find_line_end(const IndexParams& p, int64_t from, int64_t tile_end) {
     const int lane = threadIdx.x & 31;
     int64_t found = kNone;
-    const int64_t limit = p.n - tile_end > kMaxExtension ? tile_end + kMaxExtension : p.n;
+    int64_t limit = p.n - tile_end > kMaxExtension ? tile_end + kMaxExtension : p.n;
+    if (limit > p.avail) limit = p.avail;
     for (int64_t base = from; base < limit && found == kNone; base += 512) {
         const int64_t q = base + 16 * lane;
         uint64_t nlbits = 0;
@@ -366,23 +368,24 @@ template <int LV>
 __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
     const int tid = threadIdx.x;  // 0..255
     unsigned long long* nl_agg = p.tile_state;
-    const int64_t first_tile = blockIdx.x, stride = gridDim.x;
-    if (tid == 0 && first_tile < p.ntiles) {
+    const int64_t first_tile = p.tile_begin + blockIdx.x, stride = gridDim.x;
+    if (tid == 0 && first_tile < p.tile_end) {
         const int64_t start = first_tile * kTile;
-        load_slot(p.file, start, p.n - start < kSlotBytes ? p.n - start : kSlotBytes, sh.bytes[0], &sh.full[0]);
+        load_slot(p.file, start, p.avail - start < kSlotBytes ? p.avail - start : kSlotBytes, sh.bytes[0],
+                  &sh.full[0]);
     }
     int64_t k = 0;
-    for (int64_t t = first_tile; t < p.ntiles; t += stride, ++k) {
+    for (int64_t t = first_tile; t < p.tile_end; t += stride, ++k) {
         const int bs = static_cast<int>(k % kRing), ms = static_cast<int>(k & 1);
         const uint32_t buse = static_cast<uint32_t>(k / kRing), muse = static_cast<uint32_t>(k >> 1);
         // start the copy of the next tile (its byte slot was last used three tiles ago)
-        if (tid == 0 && t + stride < p.ntiles) {
+        if (tid == 0 && t + stride < p.tile_end) {
             const int nb = static_cast<int>((k + 1) % kRing);
             const uint32_t nuse = static_cast<uint32_t>((k + 1) / kRing);
             if (nuse > 0 && !mbar_wait_idle(&sh.bfree[nb], (nuse - 1) & 1))
                 atomicOr(p.status + 1, kErrCopyTimeout);
             const int64_t start = (t + stride) * kTile;
-            load_slot(p.file, start, p.n - start < kSlotBytes ? p.n - start : kSlotBytes, sh.bytes[nb],
+            load_slot(p.file, start, p.avail - start < kSlotBytes ? p.avail - start : kSlotBytes, sh.bytes[nb],
                       &sh.full[nb]);
         }
         if (!mbar_wait_bounded(&sh.full[bs], buse & 1) && tid == 0) atomicOr(p.status + 1, kErrCopyTimeout);
@@ -390,7 +393,7 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
 
         const int64_t tile_start = t * kTile;
         const int64_t tile_end = p.n - tile_start < kTile ? p.n : tile_start + kTile;
-        const int64_t loaded_end = p.n - tile_start < kSlotBytes ? p.n : tile_start + kSlotBytes;
+        const int64_t loaded_end = p.avail - tile_start < kSlotBytes ? p.avail : tile_start + kSlotBytes;
         const int64_t ws = tile_start + 64 * tid;
         const uint64_t valid = bits_between(0, tile_end - ws);
 
@@ -573,7 +576,7 @@ __device__ void line_warps(const IndexParams& p, FShared<LV>& sh) {
     const uint8_t* ir_base = ir_local ? sh.ir : p.bytecode;
     const int32_t* ir_off = ir_local ? sh.ir_off : p.offsets;
     int64_t k = 0;
-    for (int64_t t = blockIdx.x; t < p.ntiles; t += gridDim.x, ++k) {
+    for (int64_t t = p.tile_begin + blockIdx.x; t < p.tile_end; t += gridDim.x, ++k) {
         const int ms = static_cast<int>(k & 1);
         const uint32_t muse = static_cast<uint32_t>(k >> 1);
         if (!mbar_wait_idle(&sh.mready[ms], muse & 1) && lt == 0) atomicOr(p.status + 1, kErrCopyTimeout);
@@ -673,13 +676,19 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
         line_warps<LV>(p, sh);
 }
 
+// Raises the kernel's dynamic shared memory limit, once per device (the
+// attribute belongs to the kernel's instance on the current device).
 template <int LV>
 cudaError_t prepare() {
-    static bool done = false;
-    if (done) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(line_index_kernel<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(sizeof(FShared<LV>)));
-    if (e == cudaSuccess) done = true;
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (done.load() & bit)) return cudaSuccess;
+    e = cudaFuncSetAttribute(line_index_kernel<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(sizeof(FShared<LV>)));
+    if (e == cudaSuccess && bit) done.fetch_or(bit);
     return e;
 }
 

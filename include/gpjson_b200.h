@@ -109,6 +109,17 @@ int gpj_file_open(gpj_ctx *ctx, const char *filename, gpj_file **out);
 /* Copies `n` bytes of host memory into device memory as an input file. */
 int gpj_file_from_host(gpj_ctx *ctx, const void *data, int64_t n, gpj_file **out);
 
+/* gpj_file_from_host followed by gpj_index_build, pipelined: the input is
+ * copied in 64 MiB chunks on a second stream while the index kernel indexes
+ * each chunk as soon as the chunk after it has arrived, so the copy and the
+ * index build overlap (the reference reads and copies the whole file before
+ * its first kernel, QueryFunction.java:316-335).  Same index as
+ * gpj_index_build; inputs that are not line-delimited, or have lines longer
+ * than a chunk, are indexed again once the copy is complete.  Page-locked
+ * host memory gives the fastest copies. */
+int gpj_file_from_host_indexed(gpj_ctx *ctx, const void *data, int64_t n, int num_levels,
+                               gpj_file **out);
+
 /* Wraps `n` bytes that are already in device memory (not copied, not freed).
  * `d_data` must be 16-byte aligned and stay valid until gpj_file_release. */
 int gpj_file_from_device(gpj_ctx *ctx, const void *d_data, int64_t n, gpj_file **out);

@@ -138,3 +138,40 @@ def test_index_is_repeatable(gpjson):
             assert all(np.array_equal(a, b) for a, b in zip(first, again))
     finally:
         f.release()
+
+
+def indexes_of(f, levels):
+    return f.newline_index(), f.string_index(), f.leveled_bitmaps(levels)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ndjson", "long_line", "newline_in_string"])
+def test_pipelined_load_and_index(gpjson, case):
+    """gpj_file_from_host_indexed (64 MiB chunks copied while earlier chunks
+    are indexed) equals the plain copy + index build, including inputs that
+    need the rebuild: a line longer than a chunk, a raw newline in a string."""
+    base = datagen.tweets(150 << 20)
+    if case == "ndjson":
+        data = base
+    else:
+        cut = int(np.flatnonzero(base[100 << 20:] == 10)[0]) + (100 << 20)
+        if case == "long_line":
+            extra = b'{"k":"' + b"x" * (70 << 20) + b'"}'
+        else:
+            extra = b'{"k": "a' + bytes([10]) + b'b"}'
+        data = np.concatenate([base[: cut + 1], np.frombuffer(extra + b"\n", dtype=np.uint8), base[cut + 1:]])
+    levels = 4
+    f = gpjson.load_bytes(data)
+    g = gpjson.load_bytes_indexed(data, levels)
+    try:
+        f.build_index(levels)
+        want = indexes_of(f, levels)
+        got = indexes_of(g, levels)
+        for a, b, what in zip(got, want, ("newlines", "strings", "levels")):
+            assert np.array_equal(a, b), what
+    finally:
+        f.release()
+        g.release()
+    if case == "ndjson":
+        ref = oracle.Index(data[: 8 << 20].tobytes(), levels)
+        assert np.array_equal(want[0][: len(ref.newlines)], ref.newlines)
