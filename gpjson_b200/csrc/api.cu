@@ -249,7 +249,9 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
     p.tile_begin = 0;
     p.tile_end = p.ntiles;
     p.avail = n;
-    gpj::IndexParams fused = p;
+    gpj::IndexParams fused = p;  // the line-parallel kernel's launch (its own tile size)
+    fused.ntiles = (n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+    fused.tile_end = fused.ntiles;
     if (fq && fq->nq > 0) {
         fused.num_queries = fq->nq;
         fused.bytecode = fq->bytecode;
@@ -410,8 +412,8 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
     return GPJ_OK;
 }
 
-// Bytes copied per step of load_and_index; a multiple of the tile size.
-constexpr int64_t kLoadChunk = 64ll << 20;
+// Bytes copied per step of load_and_index: 5461 line-kernel tiles (~64 MiB).
+constexpr int64_t kLoadChunk = gpj::kLineTileBytes * 5461;
 
 // Copies n host bytes into f->d_owned in chunks on the copy stream and
 // indexes chunk k with the line-parallel kernel as soon as chunk k + 1 has
@@ -443,7 +445,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         gpj::IndexParams p{};
         p.file = f->d_data;
         p.n = n;
-        p.ntiles = (n + gpj::kIndexTileBytes - 1) / gpj::kIndexTileBytes;
+        p.ntiles = (n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
         p.string_index = f->d_str;
         p.leveled = f->d_lvl;
         p.level_size = f->words;
@@ -462,7 +464,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         // the copies start once the buffers exist (pool allocations are ordered on ctx->stream)
         GPJ_CUDA(ctx, cudaEventRecord(ctx->ev_ready, ctx->stream));
         GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0));
-        const int64_t tiles_per_chunk = kLoadChunk / gpj::kIndexTileBytes;
+        const int64_t tiles_per_chunk = kLoadChunk / gpj::kLineTileBytes;
         const int occ = ctx->line_occupancy[occupancy_slot(num_levels)];
         auto launch_chunk = [&](int64_t k) -> int {
             p.tile_begin = k * tiles_per_chunk;

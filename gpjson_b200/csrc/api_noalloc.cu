@@ -27,6 +27,9 @@ namespace {
 
 constexpr int64_t kMaxBytes = GPJ_NOALLOC_MAX_BYTES;
 constexpr int64_t kMaxTiles = kMaxBytes / gpj::kIndexTileBytes;  // 16384
+// 3 words per exact-kernel tile also cover the line kernel's 2 per (smaller) tile
+static_assert(3 * kMaxTiles >= 2 * ((kMaxBytes + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes),
+              "tile states for both kernels");
 constexpr int64_t kCounterWord = 3 * kMaxTiles;
 constexpr int64_t kStatusWord = kCounterWord + 2;
 constexpr int64_t kScratchWords = kStatusWord + 2;  // 49156 words, 384 KiB
@@ -148,8 +151,12 @@ extern "C" int gpj_build_index_device_noalloc(void* stream_handle, const void* d
     p.tile_end = p.ntiles;
     p.avail = n;
 
+    gpj::IndexParams lp = p;  // the line-parallel kernel's launch (its own tile size)
+    lp.ntiles = (n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+    lp.tile_end = lp.ntiles;
+
     unsigned long long status[2] = {0, 0};
-    int rc = launch(d, false, p, stream, status);
+    int rc = launch(d, false, lp, stream, status);
     if (rc) return rc;
     if (status[1] & (gpj::kErrIrregular | gpj::kErrLongLine)) {
         rc = launch(d, true, p, stream, status);

@@ -7,7 +7,10 @@
 
 namespace gpj {
 
-constexpr int64_t kIndexTileBytes = 16384;
+constexpr int64_t kIndexTileBytes = 16384;  // exact kernel
+// The line-parallel kernel owns 12 KiB per tile and reads 4 KiB past it, so
+// that a tile and its look-ahead are one 64-byte word per index thread.
+constexpr int64_t kLineTileBytes = 12288;
 // The escape state at a tile start is found by scanning back over the bytes
 // before it; a backslash run longer than this crossing a tile start is
 // reported as an error (kErrEscapeRun) instead of being resolved.

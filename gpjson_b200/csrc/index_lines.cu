@@ -4,9 +4,10 @@
 // In newline-delimited JSON every line is a complete value, so at each
 // '\n' the reference's scan state (Sequential.java:36-128: inside-string
 // flag, level counter, escape flag) is (outside, -1, clear) again.  This
-// kernel uses that: the CTA that owns a 16 KiB tile builds the index of
+// kernel uses that: the CTA that owns a 12 KiB tile builds the index of
 // every line that starts in it, starting each line from that state, and runs
-// on past the tile end to finish its last line.  No string or level carry
+// on past the tile end to finish its last line (in the 4 KiB look-ahead
+// loaded with the tile, or from device memory for longer lines).  No string or level carry
 // crosses tiles, so CTAs depend on each other only through the newline
 // count, which a decoupled look-back resolves off the critical path.
 //
@@ -23,11 +24,13 @@
 //
 // Each CTA is a three-stage pipeline over its tiles (tile blockIdx.x, then
 // every gridDim.x-th):
-//  * copies: 1-D TMA bulk loads of tile + 4 KiB into a ring of three byte
-//    slots, issued one tile ahead;
-//  * index warps (0-7, one 64-byte word per thread): classify, resolve
-//    escapes and strings, split levels, write the index, and leave the final
-//    masks of the tile and its extension in one of two mask slots;
+//  * copies: 1-D TMA bulk loads of tile + look-ahead (16 KiB) into a ring
+//    of three byte slots, issued one tile ahead;
+//  * index warps (0-7, one 64-byte word of the slot per thread): classify,
+//    resolve escapes and strings, one block scan with a reset at newlines
+//    (line starts, newline counts and each word's state at once), split
+//    levels, write the index, and leave the final masks of the tile and its
+//    look-ahead in one of two mask slots;
 //  * line warps (8-11): the newline-count look-back, the newline index, and
 //    the find_value interpreter (interp.cuh) on the tile's lines over the
 //    shared-memory masks, one (line, query) pair per thread, a warp's lanes
@@ -49,11 +52,12 @@ namespace gpj {
 
 namespace {
 
-constexpr int64_t kTile = kRoundBytes;               // 16 KiB
-constexpr int kTileWords = kTile / 64;               // 256
-constexpr int64_t kExtBytes = 4096;                  // extension loaded with the tile
-constexpr int64_t kSlotBytes = kTile + kExtBytes;    // 20 KiB
-constexpr int kSlotWords = kTileWords + kExtBytes / 64;  // 320
+constexpr int64_t kTile = kLineTileBytes;            // 12 KiB owned per tile
+constexpr int kTileWords = kTile / 64;               // 192
+constexpr int64_t kExtBytes = 4096;                  // look-ahead loaded with the tile
+constexpr int64_t kSlotBytes = kTile + kExtBytes;    // 16 KiB: one word per index thread
+constexpr int kSlotWords = kTileWords + kExtBytes / 64;  // 256
+static_assert(kSlotWords == 256 && kSlotBytes == kRoundBytes, "one slot word per index thread");
 constexpr int kRing = 3;                             // byte slots
 constexpr int kMaskSlots = 2;
 constexpr int kIndexThreads = 256;                   // warps 0-7
@@ -162,6 +166,44 @@ struct SlotInfo {
     int byte_slot;
 };
 
+// Summary of a word for the tile scan: the Span arithmetic of word_ops.cuh
+// plus a reset at newlines.  A word holding a '\n' starts a line there; in
+// NDJSON every line starts outside strings at level -1, so the state after
+// such a word is known absolutely from its bytes past its first '\n'
+// (reset = 1, d0 = the level after the word).  Otherwise (reset = 0) d0 and
+// dt are the relative level changes of Span.  The exclusive scan of a word
+// then says whether a line starts before it in the tile (reset set) and, if
+// so, its state: composing from the last reset is exact because the kernel
+// checks the state at every later '\n' (a mismatch sends the input to the
+// exact kernel).  nl counts newlines.
+struct RSpan {
+    int32_t rq;  // 2 * reset + quote parity
+    int32_t d0;
+    int32_t dt;
+    int32_t nl;
+};
+
+__device__ __forceinline__ RSpan rspan_compose(const RSpan& a, const RSpan& b) {
+    const int aq = a.rq & 1;
+    RSpan r;
+    r.nl = a.nl + b.nl;
+    if (b.rq & 2) {
+        r.rq = b.rq;
+        r.d0 = b.d0;
+        r.dt = 0;
+    } else {
+        r.rq = (a.rq & 2) | (aq ^ (b.rq & 1));
+        r.d0 = a.d0 + (aq ? b.dt - b.d0 : b.d0);
+        r.dt = (a.rq & 2) ? 0 : a.dt + b.dt;
+    }
+    return r;
+}
+
+__device__ __forceinline__ RSpan shfl_rspan_up(const RSpan& v, int off) {
+    return RSpan{__shfl_up_sync(~0u, v.rq, off), __shfl_up_sync(~0u, v.d0, off), __shfl_up_sync(~0u, v.dt, off),
+                 __shfl_up_sync(~0u, v.nl, off)};
+}
+
 template <int LV>
 struct FShared {
     uint8_t bytes[kRing][kSlotBytes];
@@ -182,11 +224,11 @@ struct FShared {
     uint64_t mready[kMaskSlots];
     uint64_t mfree[kMaskSlots];
     Span span_scratch[kTileWarps];
-    int isum[kTileWarps];
-    int64_t imin[kTileWarps];
-    int carry_s, carry_esc;
-    int64_t carry_d;
-    int64_t ext_b;
+    RSpan rscan[2][kTileWarps];  // tile scan, alternating between tiles
+    int carry_esc;
+    int64_t first_line;  // start of the tile's first line (its first '\n')
+    int64_t ext_b;       // end of the tile's last line when it ends in the look-ahead
+    int64_t long_b;
     int64_t nl_before;
 };
 
@@ -214,36 +256,29 @@ __device__ __forceinline__ Span index_scan_span(Span mine, Span* scratch, Span* 
     return span_compose(prefix, excl);
 }
 
-__device__ __forceinline__ int index_sum_min(int x, int64_t y, int* isum, int64_t* imin, int* total,
-                                             int64_t* minimum) {
+// Exclusive RSpan scan over the 256 index threads, in word order; one
+// named barrier.  `scratch` must not be reused by the next tile (the caller
+// alternates two).
+__device__ __forceinline__ RSpan index_scan_rspan(RSpan mine, RSpan* scratch, RSpan* total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int incl = x;
+    RSpan incl = mine;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-        const int o = __shfl_up_sync(~0u, incl, off);
-        if (lane >= off) incl += o;
+        const RSpan o = shfl_rspan_up(incl, off);
+        if (lane >= off) incl = rspan_compose(o, incl);
     }
-    int64_t mn = y;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        const int64_t o = __shfl_xor_sync(~0u, mn, off);
-        mn = o < mn ? o : mn;
-    }
-    if (lane == 31) isum[warp] = incl;
-    if (lane == 0) imin[warp] = mn;
+    if (lane == 31) scratch[warp] = incl;
+    RSpan excl = shfl_rspan_up(incl, 1);
+    if (lane == 0) excl = RSpan{0, 0, 0, 0};
     group_sync(kBarIndex, kIndexThreads);
-    int before = 0, all = 0;
-    int64_t m = imin[0];
+    RSpan prefix{0, 0, 0, 0}, all{0, 0, 0, 0};
 #pragma unroll
     for (int w = 0; w < kTileWarps; w++) {
-        if (w < warp) before += isum[w];
-        all += isum[w];
-        m = imin[w] < m ? imin[w] : m;
+        if (w == warp) prefix = all;
+        all = rspan_compose(all, scratch[w]);
     }
     *total = all;
-    *minimum = m;
-    group_sync(kBarIndex, kIndexThreads);  // scratch may be reused after this
-    return before + incl - x;
+    return rspan_compose(prefix, excl);
 }
 
 // Issues the TMA load of [start, start + bytes) into `dst` on `bar` (one thread).
@@ -395,155 +430,156 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
         const int64_t tile_end = p.n - tile_start < kTile ? p.n : tile_start + kTile;
         const int64_t loaded_end = p.avail - tile_start < kSlotBytes ? p.avail : tile_start + kSlotBytes;
         const int64_t ws = tile_start + 64 * tid;
-        const uint64_t valid = bits_between(0, tile_end - ws);
 
-        // ---- the tile's words ---------------------------------------------
+        // ---- one round over the slot: the tile's words and the look-ahead after it
+        // One scan gives the tile's line starts, newline counts and every
+        // word's state; the look-ahead words finish the tile's last line.
+        const bool ahead = tid >= kTileWords;  // a word past the tile end
+        const uint64_t valid = bits_between(0, (ahead ? loaded_end : tile_end) - ws);
         ClassMasks m = load_classify(buf, tid);
         restrict_masks(m, valid);
-        const uint64_t my_newlines = m.newline;
-        const int64_t first_local = my_newlines ? 64 * tid + ctz64(my_newlines) : kNone;
-        int tile_nl = 0;
-        int64_t first_nl = kNone;
-        const int my_nl_excl =
-            index_sum_min(popc64(my_newlines), first_local, sh.isum, sh.imin, &tile_nl, &first_nl);
+        // Escapes: a backslash run never crosses a '\n', so for every byte at
+        // or after the tile's first line start the run found inside the slot
+        // is the whole run (floor 0, parity 0 is exact there).
+        const uint32_t cin = escape_carry_in(buf, tid, m.backslash, 0, 0);
+        uint32_t cout;
+        const uint64_t esc = escaped_mask(m.backslash, cin, &cout);
+        const uint64_t quotes = m.quote & ~esc;
+        const uint64_t p0 = prefix_xor(quotes);
+        const bool has_nl = m.newline != 0;
+        const int f = has_nl ? ctz64(m.newline) : 0;
+        const uint64_t after = has_nl ? (f == 63 ? 0ull : (~0ull << (f + 1))) : ~0ull;
+        // in-string bits past the first '\n' when a line starts there
+        const uint64_t pa = (p0 ^ (((p0 >> f) & 1ull) ? ~0ull : 0ull)) & after;
+        RSpan mine;
+        // newlines of the tile count in the low 16 bits, of the look-ahead above
+        mine.nl = ahead ? (popc64(m.newline) << 16) : popc64(m.newline);
+        if (has_nl && !ahead) {  // only the tile's own newlines start lines here
+            mine.rq = 2 | (popc64(quotes & after) & 1);
+            mine.d0 = -1 + popc64(m.open & after & ~pa) - popc64(m.close & after & ~pa);
+            mine.dt = 0;
+        } else {
+            mine.rq = popc64(quotes) & 1;
+            mine.d0 = popc64(m.open & ~p0) - popc64(m.close & ~p0);
+            mine.dt = popc64(m.open) - popc64(m.close);
+        }
+        if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(cout);
+        RSpan total;
+        RSpan ex = index_scan_rspan(mine, sh.rscan[k & 1], &total);
+        if (t == 0) {  // the file's first line starts at byte 0
+            const RSpan init{2, -1, 0, 0};
+            ex = rspan_compose(init, ex);
+            total = rspan_compose(init, total);
+        }
+        const int tile_nl = total.nl & 0xFFFF;
+        const int ahead_nl = total.nl >> 16;
+        const bool lines_here = (total.rq & 2) != 0;  // a line starts in this tile
         if (tid == 0) st_release(nl_agg + t, tag48(p.epoch, static_cast<unsigned long long>(tile_nl)));
 
         // the mask slot was last used two tiles ago
         if (muse > 0 && !mbar_wait_idle(&sh.mfree[ms], (muse - 1) & 1) && tid == 0)
             atomicOr(p.status + 1, kErrCopyTimeout);
-        sh.nlmask[ms][tid] = my_newlines;
-        sh.nlexcl[ms][tid] = my_nl_excl;
-        {
-            uint64_t nm = my_newlines;
-            int q = my_nl_excl;
+        if (!ahead) {
+            const int excl = ex.nl & 0xFFFF;
+            sh.nlmask[ms][tid] = m.newline;
+            sh.nlexcl[ms][tid] = excl;
+            uint64_t nm = m.newline;
+            int q = excl;
             while (nm && q < kMaxTileLines) {
                 sh.nlpos[ms][q++] = 64 * tid + ctz64(nm);
                 nm &= nm - 1;
             }
+            if (ex.rq & 2) {
+                // every byte of the word belongs to lines that start in this tile
+                if (ws < tile_end)
+                    finish_word<LV>(p, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, tid, valid, m.newline);
+            } else if (has_nl) {
+                // the tile's first line starts at byte f of this word
+                sh.first_line = ws + f;
+                ClassMasks mm = m;
+                restrict_masks(mm, after);
+                finish_word<LV>(p, sh, ms, mm, pa, 0, -1, ws >> 6, f == 0, tid, valid, m.newline & after);
+            }
+        } else if (lines_here && (ex.nl >> 16) == 0 && valid) {
+            // No '\n' between the tile end and this word: the tile's last line
+            // runs into it.  The line ends at this word's first '\n' (the only
+            // one checked here); a word that starts with it belongs to the next tile.
+            if (has_nl) sh.ext_b = ws + f;
+            if (!(has_nl && f == 0))
+                finish_word<LV>(p, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, tid, valid,
+                                has_nl ? (1ull << f) : 0ull);
         }
+        group_sync(kBarIndex, kIndexThreads);  // the tile's masks are complete in the slot
 
-        const int64_t a_t = t == 0 ? 0 : (first_nl == kNone ? kNone : tile_start + first_nl);
+        const int64_t a_t = t == 0 ? 0 : (lines_here ? sh.first_line : kNone);
         int64_t b_t = tile_end, hi = tile_end;
-        if (a_t != kNone) {
-            const uint64_t mine = valid & bits_between(a_t - ws, 64);
-            restrict_masks(m, mine);
-            const uint32_t cin = escape_carry_in(buf, tid, m.backslash, static_cast<int>(a_t - tile_start), 0);
-            uint32_t cout;
-            const uint64_t esc = escaped_mask(m.backslash, cin, &cout);
-            const uint64_t quotes = m.quote & ~esc;
-            const uint64_t p0 = prefix_xor(quotes);
-            const Span sp{popc64(quotes) & 1, popc64(m.open & ~p0) - popc64(m.close & ~p0),
-                          popc64(m.open) - popc64(m.close), 0};
-            Span total;
-            const Span ex = index_scan_span(sp, sh.span_scratch, &total);
-            // lines start outside strings at level -1
-            const uint64_t check = m.newline & ~(a_t >= ws && a_t < ws + 64 ? (1ull << (a_t - ws)) : 0ull);
-            if (ws < tile_end)
-                finish_word<LV>(p, sh, ms, m, p0, ex.q, -1 + static_cast<int64_t>(ex.dd0), ws >> 6, ws >= a_t,
-                                tid, valid, check);
-            // state at the tile end (the last thread's word ends there)
-            const int s_in = total.q;
-            const int64_t d_in = -1 + static_cast<int64_t>(total.dd0);
-            if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(cout);
-            group_sync(kBarIndex, kIndexThreads);
-            const int esc_in = sh.carry_esc;
-
-            // ---- the extension: finish the last line past the tile end -------
-            if (tile_end < p.n) {
-                // words [tile_end, loaded_end) are in the slot already
-                const int ext_words = static_cast<int>((loaded_end - tile_end + 63) >> 6);
-                const int64_t ew = tile_end + 64 * tid;
-                const uint64_t evalid = tid < ext_words ? bits_between(0, loaded_end - ew) : 0ull;
-                ClassMasks x{0, 0, 0, 0, 0, 0, 0};
-                if (tid < ext_words) {
-                    x = load_classify(buf, kTileWords + tid);
-                    restrict_masks(x, evalid);
+        if (lines_here && tile_end < p.n) {
+            if (ahead_nl > 0) {
+                b_t = sh.ext_b;
+                hi = b_t;
+            } else if (loaded_end == p.n) {
+                b_t = p.n;
+                hi = p.n;
+            } else {
+                // a line longer than the look-ahead: continue past the slot
+                // straight from device memory
+                const int s_in = total.rq & 1;
+                const int64_t d_in = total.d0;
+                const int esc_in = sh.carry_esc;
+                if (tid < 32) {
+                    const int64_t e2 = find_line_end(p, loaded_end, tile_end);
+                    if (tid == 0) sh.long_b = e2;
                 }
-                const int64_t x_first = x.newline ? ew + ctz64(x.newline) : kNone;
-                int ext_nl = 0;
-                int64_t first_ext_nl = kNone;
-                (void)index_sum_min(0, x_first, sh.isum, sh.imin, &ext_nl, &first_ext_nl);
-                if (first_ext_nl != kNone || loaded_end == p.n) {
-                    // the line ends inside the loaded extension (or at the end of the file)
-                    b_t = first_ext_nl != kNone ? first_ext_nl : p.n;
-                    hi = b_t;
-                    const int64_t own_end = (b_t + 63) & ~static_cast<int64_t>(63);
-                    const uint32_t xcin =
-                        escape_carry_in(buf, kTileWords + tid, x.backslash, kTileWords * 64, esc_in);
-                    uint32_t xcout;
-                    const uint64_t xesc = escaped_mask(x.backslash, xcin, &xcout);
-                    const uint64_t xq = x.quote & ~xesc;
-                    const uint64_t xp0 = prefix_xor(xq);
-                    const Span xs{popc64(xq) & 1, popc64(x.open & ~xp0) - popc64(x.close & ~xp0),
-                                  popc64(x.open) - popc64(x.close), 0};
-                    Span xtotal;
-                    const Span xex = index_scan_span(xs, sh.span_scratch, &xtotal);
-                    const uint64_t xcheck =
-                        (b_t >= ew && b_t < ew + 64) ? (x.newline & (1ull << (b_t - ew))) : 0ull;
-                    if (ew < own_end && tid < ext_words)
-                        finish_word<LV>(p, sh, ms, x, xp0, s_in ^ xex.q,
-                                        d_in + (s_in ? (xex.ddt - xex.dd0) : xex.dd0), ew >> 6, true,
-                                        kTileWords + tid, evalid, xcheck);
-                    if (b_t == tile_end && tid == 0 && (s_in != 0 || d_in != -1))
-                        atomicOr(p.status + 1, kErrIrregular);
-                } else {
-                    // a long line: continue past the slot straight from device memory;
-                    // no line past the tile end is kept for the queries
-                    if (tid < 32) {
-                        const int64_t e = find_line_end(p, loaded_end, tile_end);
-                        if (tid == 0) sh.ext_b = e;
+                group_sync(kBarIndex, kIndexThreads);
+                b_t = sh.long_b;
+                hi = loaded_end;
+                const int64_t own_end = (b_t + 63) & ~static_cast<int64_t>(63);
+                int s = s_in, esc = esc_in;
+                int64_t d = d_in;
+                for (int64_t cs = loaded_end; cs < own_end && cs < p.n; cs += kRoundBytes) {
+                    const int64_t cw = cs + 64 * tid;
+                    const uint64_t cvalid = cw < own_end ? bits_between(0, p.n - cw) : 0ull;
+                    ClassMasks c{0, 0, 0, 0, 0, 0, 0};
+                    if (cvalid) {
+                        c = classify_global(p.file, p.n, cw);
+                        restrict_masks(c, cvalid);
                     }
+                    // escape carry: previous word's trailing run, else the bytes before
+                    const bool all_bs = c.backslash == ~0ull;
+                    const int trail_par = all_bs ? 0 : (clz64(~c.backslash) & 1);
+                    const int prev_par = __shfl_up_sync(~0u, trail_par, 1);
+                    const int prev_all = __shfl_up_sync(~0u, all_bs ? 1 : 0, 1);
+                    uint32_t ccin;
+                    if ((tid & 31) > 0 && !prev_all) {
+                        ccin = static_cast<uint32_t>(prev_par);
+                    } else {
+                        int run = 0;
+                        int64_t j = cw - 1;
+                        while (j >= cs && __ldg(p.file + j) == '\\') {
+                            ++run;
+                            --j;
+                        }
+                        ccin = static_cast<uint32_t>((run & 1) ^ (j < cs ? esc : 0));
+                    }
+                    uint32_t ccout;
+                    const uint64_t cesc = escaped_mask(c.backslash, ccin, &ccout);
+                    const uint64_t cq = c.quote & ~cesc;
+                    const uint64_t cp0 = prefix_xor(cq);
+                    const Span csp{popc64(cq) & 1, popc64(c.open & ~cp0) - popc64(c.close & ~cp0),
+                                   popc64(c.open) - popc64(c.close), 0};
+                    Span ctotal;
+                    const Span cex = index_scan_span(csp, sh.span_scratch, &ctotal);
+                    const uint64_t ccheck =
+                        (b_t >= cw && b_t < cw + 64) ? (c.newline & (1ull << (b_t - cw))) : 0ull;
+                    if (cvalid)
+                        finish_word<LV>(p, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
+                                        cw >> 6, true, -1, cvalid, ccheck);
+                    if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(ccout);
                     group_sync(kBarIndex, kIndexThreads);
-                    b_t = sh.ext_b;
-                    hi = tile_end;
-                    const int64_t own_end = (b_t + 63) & ~static_cast<int64_t>(63);
-                    int s = s_in, esc = esc_in;
-                    int64_t d = d_in;
-                    for (int64_t cs = tile_end; cs < own_end && cs < p.n; cs += kTile) {
-                        const int64_t cw = cs + 64 * tid;
-                        const uint64_t cvalid = cw < own_end ? bits_between(0, p.n - cw) : 0ull;
-                        ClassMasks c{0, 0, 0, 0, 0, 0, 0};
-                        if (cvalid) {
-                            c = classify_global(p.file, p.n, cw);
-                            restrict_masks(c, cvalid);
-                        }
-                        // escape carry: previous word's trailing run, else the bytes before
-                        const bool all_bs = c.backslash == ~0ull;
-                        const int trail_par = all_bs ? 0 : (clz64(~c.backslash) & 1);
-                        const int prev_par = __shfl_up_sync(~0u, trail_par, 1);
-                        const int prev_all = __shfl_up_sync(~0u, all_bs ? 1 : 0, 1);
-                        uint32_t ccin;
-                        if ((tid & 31) > 0 && !prev_all) {
-                            ccin = static_cast<uint32_t>(prev_par);
-                        } else {
-                            int run = 0;
-                            int64_t j = cw - 1;
-                            while (j >= cs && __ldg(p.file + j) == '\\') {
-                                ++run;
-                                --j;
-                            }
-                            ccin = static_cast<uint32_t>((run & 1) ^ (j < cs ? esc : 0));
-                        }
-                        uint32_t ccout;
-                        const uint64_t cesc = escaped_mask(c.backslash, ccin, &ccout);
-                        const uint64_t cq = c.quote & ~cesc;
-                        const uint64_t cp0 = prefix_xor(cq);
-                        const Span csp{popc64(cq) & 1, popc64(c.open & ~cp0) - popc64(c.close & ~cp0),
-                                       popc64(c.open) - popc64(c.close), 0};
-                        Span ctotal;
-                        const Span cex = index_scan_span(csp, sh.span_scratch, &ctotal);
-                        const uint64_t ccheck =
-                            (b_t >= cw && b_t < cw + 64) ? (c.newline & (1ull << (b_t - cw))) : 0ull;
-                        if (cvalid)
-                            finish_word<LV>(p, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
-                                            cw >> 6, true, -1, cvalid, ccheck);
-                        if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(ccout);
-                        group_sync(kBarIndex, kIndexThreads);
-                        esc = sh.carry_esc;
-                        d += s ? (ctotal.ddt - ctotal.dd0) : ctotal.dd0;
-                        s ^= ctotal.q;
-                        group_sync(kBarIndex, kIndexThreads);
-                    }
+                    esc = sh.carry_esc;
+                    d += s ? (ctotal.ddt - ctotal.dd0) : ctotal.dd0;
+                    s ^= ctotal.q;
+                    group_sync(kBarIndex, kIndexThreads);
                 }
             }
         }
@@ -554,9 +590,8 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
             in.hi = hi;
             in.tile_nl = tile_nl;
             in.byte_slot = bs;
+            mbar_arrive(&sh.mready[ms]);  // the masks were complete at the barrier above
         }
-        group_sync(kBarIndex, kIndexThreads);
-        if (tid == 0) mbar_arrive(&sh.mready[ms]);
     }
 }
 
