@@ -54,6 +54,7 @@ struct gpj_ctx {
     uint32_t epoch = 0;
     int index_occupancy[3] = {0, 0, 0};  // exact kernel, levels <=4, <=8, <=16
     int line_occupancy[3] = {0, 0, 0};   // line-parallel kernel
+    int tile_occupancy[3] = {0, 0, 0};   // its standalone form (index builds without queries)
     int64_t exact_fallbacks = 0;         // builds that needed the exact kernel
     bool fuse_queries = false;           // evaluate queries inside the index kernel
     int query_occupancy = 0;
@@ -221,6 +222,56 @@ struct FusedQueries {
     int64_t out_lines = 0;  // query stride of `out`
 };
 
+// Scratch of a standalone index build: the '\n' bitmap, the newline count
+// and the newline offset of every tile (pool allocations, freed after the build).
+struct TileScratch {
+    uint64_t* bits = nullptr;
+    int32_t* counts = nullptr;
+    int64_t* offsets = nullptr;
+};
+
+int alloc_tile_scratch(gpj_ctx* ctx, int64_t n, TileScratch* ts) {
+    const int64_t ntiles = (n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+    int rc = device_alloc(ctx, &ts->bits, static_cast<size_t>((n + 63) / 64), "cudaMalloc(newline bitmap)");
+    if (!rc) rc = device_alloc(ctx, &ts->counts, static_cast<size_t>(ntiles), "cudaMalloc(tile counts)");
+    if (!rc) rc = device_alloc(ctx, &ts->offsets, static_cast<size_t>(ntiles), "cudaMalloc(tile offsets)");
+    return rc;
+}
+
+void free_tile_scratch(gpj_ctx* ctx, TileScratch* ts) {
+    device_free(ctx, ts->bits);
+    device_free(ctx, ts->counts);
+    device_free(ctx, ts->offsets);
+}
+
+// Parameters of the standalone index kernel over tiles [tile_begin, tile_end).
+void set_tile_range(gpj::IndexParams* p, int64_t tile_begin, int64_t tile_end, int64_t avail) {
+    p->tile_begin = tile_begin;
+    p->tile_end = tile_end;
+    p->avail = avail;
+}
+
+int launch_tiles(gpj_ctx* ctx, const gpj::IndexParams& p) {
+    const int occ = ctx->tile_occupancy[occupancy_slot(p.num_levels)];
+    const int64_t grid = std::min<int64_t>(p.tile_end - p.tile_begin, static_cast<int64_t>(ctx->sms) * occ);
+    GPJ_CUDA(ctx, gpj::launch_tile_index_kernel(p, static_cast<int>(grid), ctx->stream));
+    ctx->launches++;
+    return GPJ_OK;
+}
+
+// The newline index from the tiles' bitmap and counts; on return h_status
+// holds the status words (line count, error bits).
+int finish_tiles(gpj_ctx* ctx, const gpj::IndexParams& p, const TileScratch& ts) {
+    const int64_t ntiles = (p.n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+    const int64_t grid = std::min<int64_t>((ntiles + 7) / 8, static_cast<int64_t>(ctx->sms) * 8);
+    GPJ_CUDA(ctx, gpj::launch_newline_index(p, ts.offsets, static_cast<int>(grid), ctx->stream));
+    ctx->launches += 2;
+    GPJ_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GPJ_OK;
+}
+
 // Builds the index with the line-parallel kernel (evaluating `fq` in the
 // same pass when given), and again with the exact kernel when the input is
 // not well-formed NDJSON.  *lines receives the line count; *queries_done
@@ -261,8 +312,25 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
         fused.out = fq->out;
         fused.out_lines = fq->out_lines;
     }
-    int rc = launch_index(ctx, false, fused);
-    if (rc) return rc;
+    int rc;
+    if (fq && fq->nq > 0) {
+        rc = launch_index(ctx, false, fused);
+        if (rc) return rc;
+    } else {
+        // index only: the standalone kernel, then the newline index
+        TileScratch ts;
+        rc = alloc_tile_scratch(ctx, n, &ts);
+        if (!rc) {
+            GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
+            fused.newline_bits = ts.bits;
+            fused.tile_newlines = ts.counts;
+            fused.status = ctx->d_status;
+            rc = launch_tiles(ctx, fused);
+            if (!rc) rc = finish_tiles(ctx, fused, ts);
+        }
+        free_tile_scratch(ctx, &ts);
+        if (rc) return rc;
+    }
     unsigned long long errs = ctx->h_status[1];
     bool exact = false;
     if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) {
@@ -453,40 +521,41 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         p.newlines = f->d_nl;
         p.newline_cap = f->nl_cap;
         p.materialize = 1;
-        rc = ensure_tile_state(ctx, p.ntiles);  // one epoch for all launches of this build
-        if (rc) return rc;
-        GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned int), ctx->stream));
+        TileScratch ts;
+        rc = alloc_tile_scratch(ctx, n, &ts);
+        if (rc) {
+            free_tile_scratch(ctx, &ts);
+            return rc;
+        }
         GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
-        p.tile_state = ctx->d_tile_state;
-        p.tile_counter = ctx->d_counter;
         p.status = ctx->d_status;
-        p.epoch = ctx->epoch;
+        p.newline_bits = ts.bits;
+        p.tile_newlines = ts.counts;
         // the copies start once the buffers exist (pool allocations are ordered on ctx->stream)
         GPJ_CUDA(ctx, cudaEventRecord(ctx->ev_ready, ctx->stream));
         GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0));
         const int64_t tiles_per_chunk = kLoadChunk / gpj::kLineTileBytes;
-        const int occ = ctx->line_occupancy[occupancy_slot(num_levels)];
         auto launch_chunk = [&](int64_t k) -> int {
-            p.tile_begin = k * tiles_per_chunk;
-            p.tile_end = std::min(p.ntiles, (k + 1) * tiles_per_chunk);
-            p.avail = std::min(n, (k + 2) * kLoadChunk);
+            set_tile_range(&p, k * tiles_per_chunk, std::min(p.ntiles, (k + 1) * tiles_per_chunk),
+                           std::min(n, (k + 2) * kLoadChunk));
             GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->chunk_events[std::min(k + 1, nchunks - 1)], 0));
-            const int64_t grid = std::min<int64_t>(p.tile_end - p.tile_begin, static_cast<int64_t>(ctx->sms) * occ);
-            GPJ_CUDA(ctx, gpj::launch_line_index_kernel(p, static_cast<int>(grid), ctx->stream));
-            ctx->launches++;
-            return GPJ_OK;
+            return launch_tiles(ctx, p);
         };
-        for (int64_t k = 0; k < nchunks; k++) {
+        for (int64_t k = 0; k < nchunks && !rc; k++) {
             const int64_t pos = k * kLoadChunk;
             const size_t len = static_cast<size_t>(std::min(kLoadChunk, n - pos));
-            GPJ_CUDA(ctx, cudaMemcpyAsync(f->d_owned + pos, host + pos, len, cudaMemcpyHostToDevice, ctx->copy_stream));
-            GPJ_CUDA(ctx, cudaEventRecord(ctx->chunk_events[k], ctx->copy_stream));
-            if (k >= 1 && (rc = launch_chunk(k - 1))) return rc;
+            cudaError_t e = cudaMemcpyAsync(f->d_owned + pos, host + pos, len, cudaMemcpyHostToDevice, ctx->copy_stream);
+            if (e == cudaSuccess) e = cudaEventRecord(ctx->chunk_events[k], ctx->copy_stream);
+            if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemcpyAsync(file chunk)");
+            if (!rc && k >= 1) rc = launch_chunk(k - 1);
         }
-        if ((rc = launch_chunk(nchunks - 1))) return rc;
-        GPJ_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(unsigned long long),
-                                      cudaMemcpyDeviceToHost, ctx->stream));
-        GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        if (!rc) rc = launch_chunk(nchunks - 1);
+        if (!rc) rc = finish_tiles(ctx, p, ts);
+        free_tile_scratch(ctx, &ts);
+        if (rc) {
+            cudaStreamSynchronize(ctx->copy_stream);
+            return rc;
+        }
         const unsigned long long errs = ctx->h_status[1];
         lines = static_cast<int64_t>(ctx->h_status[0]);
         if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) {
@@ -662,6 +731,8 @@ int gpj_create(int device, gpj_ctx** out) {
         ctx->index_occupancy[i] = gpj::index_kernel_max_ctas_per_sm(levels[i]);
         if (ctx->index_occupancy[i] < 1) return bail(cudaGetLastError(), "index kernel occupancy");
         ctx->line_occupancy[i] = gpj::line_index_max_ctas_per_sm(levels[i]);
+        ctx->tile_occupancy[i] = gpj::tile_index_max_ctas_per_sm(levels[i]);
+        if (ctx->tile_occupancy[i] < 1) return bail(cudaGetLastError(), "tile index kernel occupancy");
         if (ctx->line_occupancy[i] < 1) return bail(cudaGetLastError(), "line index kernel occupancy");
     }
     ctx->query_occupancy = gpj::find_value_max_ctas_per_sm();

@@ -40,6 +40,10 @@ struct IndexParams {
     int64_t tile_begin;
     int64_t tile_end;
     int64_t avail;
+    // Standalone index kernel only: the '\n' bitmap (ceil(n/64) words) and
+    // the newline count of every tile, in place of the newline index.
+    uint64_t* newline_bits;
+    int32_t* tile_newlines;
 
     // Queries evaluated in the same pass (line-parallel kernel only; 0 = none).
     int num_queries;
@@ -61,5 +65,19 @@ int index_kernel_max_ctas_per_sm(int num_levels);
 // the exact kernel must be used.  tile_state needs 2 * ntiles words.
 cudaError_t launch_line_index_kernel(const IndexParams& p, int grid, cudaStream_t stream);
 int line_index_max_ctas_per_sm(int num_levels);
+
+// Standalone form of the line-parallel kernel for index builds without
+// in-kernel queries: the index warps alone (three CTAs per SM), no tile
+// depending on another; writes string index and leveled bitmaps, and
+// newline_bits + tile_newlines instead of the newline index (same error
+// flags).  launch_newline_index then builds the newline index.
+cudaError_t launch_tile_index_kernel(const IndexParams& p, int grid, cudaStream_t stream);
+int tile_index_max_ctas_per_sm(int num_levels);
+
+// Newline index from newline_bits and tile_newlines (tiles of
+// kLineTileBytes): exclusive offsets of the tile counts into `offsets`
+// (ntiles entries), then every tile's '\n' positions; writes status[0] =
+// newlines + 1 and at most newline_cap entries.  Two launches, one stream.
+cudaError_t launch_newline_index(const IndexParams& p, int64_t* offsets, int grid, cudaStream_t stream);
 
 }  // namespace gpj

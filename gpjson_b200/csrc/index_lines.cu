@@ -232,6 +232,18 @@ struct FShared {
     int64_t nl_before;
 };
 
+// Shared memory of the standalone index kernel (no line warps, no queries).
+struct TShared {
+    uint8_t bytes[kRing][kSlotBytes];
+    uint64_t full[kRing];
+    Span span_scratch[kTileWarps];
+    RSpan rscan[2][kTileWarps];
+    int carry_esc;
+    int64_t first_line;
+    int64_t ext_b;
+    int64_t long_b;
+};
+
 // Exclusive compose-scan / sum-min over the 256 index threads (named barrier).
 __device__ __forceinline__ Span index_scan_span(Span mine, Span* scratch, Span* total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -323,8 +335,8 @@ __device__ __forceinline__ ClassMasks classify_global(const uint8_t* file, int64
 // Final masks of one word: checks the '\n' bits in `check`, keeps the word
 // in mask slot `ms` at `slot` (>= 0) and writes it to the global index when
 // `owned`.
-template <int LV>
-__device__ __forceinline__ void finish_word(const IndexParams& p, FShared<LV>& sh, int ms, const ClassMasks& m,
+template <int LV, bool kMasks, class Sh>
+__device__ __forceinline__ void finish_word(const IndexParams& p, Sh& sh, int ms, const ClassMasks& m,
                                             uint64_t p0, int s_w, int64_t d_w, int64_t word, bool owned, int slot,
                                             uint64_t valid, uint64_t check) {
     const uint64_t in_str = (p0 ^ (s_w ? ~0ull : 0ull)) & valid;
@@ -344,11 +356,13 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, FShared<LV>& s
     if (!owned && slot < 0) return;
     uint64_t lv[LV];
     split_levels<LV>(open, close, m.structural & ~in_str, d_w, lv);
-    if (slot >= 0) {
-        sh.str[ms][slot] = in_str;
-        sh.colon[ms][slot] = m.colon & ~in_str;
+    if constexpr (kMasks) {
+        if (slot >= 0) {
+            sh.str[ms][slot] = in_str;
+            sh.colon[ms][slot] = m.colon & ~in_str;
 #pragma unroll
-        for (int l = 0; l < LV; l++) sh.lv[ms][l][slot] = lv[l];
+            for (int l = 0; l < LV; l++) sh.lv[ms][l][slot] = lv[l];
+        }
     }
     if (owned && p.materialize) {
         p.string_index[word] = in_str;
@@ -399,8 +413,12 @@ __device__ int64_t find_line_end(const IndexParams& p, int64_t from, int64_t til
 }
 
 // ---- index warps -------------------------------------------------------------
-template <int LV>
-__device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
+// kLines: line warps run beside these warps (FShared: newline index by
+// look-back, in-kernel queries); otherwise the kernel is these warps alone
+// (TShared) and writes the newline bitmap and per-tile newline counts, from
+// which newline_index.cu builds the newline index.
+template <int LV, bool kLines, class Sh>
+__device__ void index_warps(const IndexParams& p, Sh& sh) {
     const int tid = threadIdx.x;  // 0..255
     unsigned long long* nl_agg = p.tile_state;
     const int64_t first_tile = p.tile_begin + blockIdx.x, stride = gridDim.x;
@@ -417,8 +435,10 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
         if (tid == 0 && t + stride < p.tile_end) {
             const int nb = static_cast<int>((k + 1) % kRing);
             const uint32_t nuse = static_cast<uint32_t>((k + 1) / kRing);
-            if (nuse > 0 && !mbar_wait_idle(&sh.bfree[nb], (nuse - 1) & 1))
-                atomicOr(p.status + 1, kErrCopyTimeout);
+            if constexpr (kLines) {
+                if (nuse > 0 && !mbar_wait_idle(&sh.bfree[nb], (nuse - 1) & 1))
+                    atomicOr(p.status + 1, kErrCopyTimeout);
+            }
             const int64_t start = (t + stride) * kTile;
             load_slot(p.file, start, p.avail - start < kSlotBytes ? p.avail - start : kSlotBytes, sh.bytes[nb],
                       &sh.full[nb]);
@@ -435,6 +455,7 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
         // One scan gives the tile's line starts, newline counts and every
         // word's state; the look-ahead words finish the tile's last line.
         const bool ahead = tid >= kTileWords;  // a word past the tile end
+        const int slot = kLines ? tid : -1;    // masks kept in shared memory for the line warps
         const uint64_t valid = bits_between(0, (ahead ? loaded_end : tile_end) - ws);
         ClassMasks m = load_classify(buf, tid);
         restrict_masks(m, valid);
@@ -474,31 +495,38 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
         const int tile_nl = total.nl & 0xFFFF;
         const int ahead_nl = total.nl >> 16;
         const bool lines_here = (total.rq & 2) != 0;  // a line starts in this tile
-        if (tid == 0) st_release(nl_agg + t, tag48(p.epoch, static_cast<unsigned long long>(tile_nl)));
-
-        // the mask slot was last used two tiles ago
-        if (muse > 0 && !mbar_wait_idle(&sh.mfree[ms], (muse - 1) & 1) && tid == 0)
-            atomicOr(p.status + 1, kErrCopyTimeout);
+        if constexpr (kLines) {
+            if (tid == 0) st_release(nl_agg + t, tag48(p.epoch, static_cast<unsigned long long>(tile_nl)));
+            // the mask slot was last used two tiles ago
+            if (muse > 0 && !mbar_wait_idle(&sh.mfree[ms], (muse - 1) & 1) && tid == 0)
+                atomicOr(p.status + 1, kErrCopyTimeout);
+        } else {
+            if (tid == 0) p.tile_newlines[t] = tile_nl;
+        }
         if (!ahead) {
-            const int excl = ex.nl & 0xFFFF;
-            sh.nlmask[ms][tid] = m.newline;
-            sh.nlexcl[ms][tid] = excl;
-            uint64_t nm = m.newline;
-            int q = excl;
-            while (nm && q < kMaxTileLines) {
-                sh.nlpos[ms][q++] = 64 * tid + ctz64(nm);
-                nm &= nm - 1;
+            if constexpr (kLines) {
+                const int excl = ex.nl & 0xFFFF;
+                sh.nlmask[ms][tid] = m.newline;
+                sh.nlexcl[ms][tid] = excl;
+                uint64_t nm = m.newline;
+                int q = excl;
+                while (nm && q < kMaxTileLines) {
+                    sh.nlpos[ms][q++] = 64 * tid + ctz64(nm);
+                    nm &= nm - 1;
+                }
+            } else {
+                if (ws < tile_end) p.newline_bits[ws >> 6] = m.newline;
             }
             if (ex.rq & 2) {
                 // every byte of the word belongs to lines that start in this tile
                 if (ws < tile_end)
-                    finish_word<LV>(p, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, tid, valid, m.newline);
+                    finish_word<LV, kLines>(p, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, slot, valid, m.newline);
             } else if (has_nl) {
                 // the tile's first line starts at byte f of this word
                 sh.first_line = ws + f;
                 ClassMasks mm = m;
                 restrict_masks(mm, after);
-                finish_word<LV>(p, sh, ms, mm, pa, 0, -1, ws >> 6, f == 0, tid, valid, m.newline & after);
+                finish_word<LV, kLines>(p, sh, ms, mm, pa, 0, -1, ws >> 6, f == 0, slot, valid, m.newline & after);
             }
         } else if (lines_here && (ex.nl >> 16) == 0 && valid) {
             // No '\n' between the tile end and this word: the tile's last line
@@ -506,7 +534,7 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
             // one checked here); a word that starts with it belongs to the next tile.
             if (has_nl) sh.ext_b = ws + f;
             if (!(has_nl && f == 0))
-                finish_word<LV>(p, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, tid, valid,
+                finish_word<LV, kLines>(p, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, slot, valid,
                                 has_nl ? (1ull << f) : 0ull);
         }
         group_sync(kBarIndex, kIndexThreads);  // the tile's masks are complete in the slot
@@ -572,7 +600,7 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
                     const uint64_t ccheck =
                         (b_t >= cw && b_t < cw + 64) ? (c.newline & (1ull << (b_t - cw))) : 0ull;
                     if (cvalid)
-                        finish_word<LV>(p, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
+                        finish_word<LV, kLines>(p, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
                                         cw >> 6, true, -1, cvalid, ccheck);
                     if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(ccout);
                     group_sync(kBarIndex, kIndexThreads);
@@ -583,14 +611,19 @@ __device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
                 }
             }
         }
-        if (tid == 0) {
-            SlotInfo& in = sh.info[ms];
-            in.a = a_t;
-            in.b = b_t;
-            in.hi = hi;
-            in.tile_nl = tile_nl;
-            in.byte_slot = bs;
-            mbar_arrive(&sh.mready[ms]);  // the masks were complete at the barrier above
+        if constexpr (kLines) {
+            if (tid == 0) {
+                SlotInfo& in = sh.info[ms];
+                in.a = a_t;
+                in.b = b_t;
+                in.hi = hi;
+                in.tile_nl = tile_nl;
+                in.byte_slot = bs;
+                mbar_arrive(&sh.mready[ms]);  // the masks were complete at the barrier above
+            }
+        } else {
+            (void)a_t;
+            (void)hi;
         }
     }
 }
@@ -706,57 +739,98 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
     }
     __syncthreads();
     if (threadIdx.x < kIndexThreads)
-        index_warps<LV>(p, sh);
+        index_warps<LV, true>(p, sh);
     else
         line_warps<LV>(p, sh);
 }
 
-// Raises the kernel's dynamic shared memory limit, once per device (the
-// attribute belongs to the kernel's instance on the current device).
+// Index only: the index warps alone, three CTAs per SM; no tile waits for
+// another, since the newline index is built afterwards from the counts.
 template <int LV>
-cudaError_t prepare() {
-    static std::atomic<unsigned long long> done{0};
+__global__ void __launch_bounds__(kIndexThreads, 3) tile_index_kernel(IndexParams p) {
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    TShared& sh = *reinterpret_cast<TShared*>(smem_raw);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kRing; i++) mbar_init(&sh.full[i], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    index_warps<LV, false>(p, sh);
+}
+
+// Raises a kernel's dynamic shared memory limit, once per device (the
+// attribute belongs to the kernel's instance on the current device).
+template <class Kernel>
+cudaError_t prepare(Kernel kernel, size_t smem, std::atomic<unsigned long long>& done) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
     if (bit && (done.load() & bit)) return cudaSuccess;
-    e = cudaFuncSetAttribute(line_index_kernel<LV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(sizeof(FShared<LV>)));
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e == cudaSuccess && bit) done.fetch_or(bit);
     return e;
 }
 
-template <int LV>
+template <int LV, bool kLines>
+struct KernelOf {
+    static void* fn() {
+        return kLines ? reinterpret_cast<void*>(line_index_kernel<LV>) : reinterpret_cast<void*>(tile_index_kernel<LV>);
+    }
+    static size_t smem() { return kLines ? sizeof(FShared<LV>) : sizeof(TShared); }
+    static int threads() { return kLines ? kThreads : kIndexThreads; }
+    static std::atomic<unsigned long long>& done() {
+        static std::atomic<unsigned long long> d{0};
+        return d;
+    }
+};
+
+template <int LV, bool kLines>
 int occupancy() {
-    if (prepare<LV>() != cudaSuccess) return -1;
+    using K = KernelOf<LV, kLines>;
+    if (prepare(K::fn(), K::smem(), K::done()) != cudaSuccess) return -1;
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, line_index_kernel<LV>, kThreads,
-                                                      sizeof(FShared<LV>)) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, K::fn(), K::threads(), K::smem()) != cudaSuccess)
         return -1;
     return blocks;
 }
 
-template <int LV>
+template <int LV, bool kLines>
 cudaError_t launch(const IndexParams& p, int grid, cudaStream_t stream) {
-    cudaError_t e = prepare<LV>();
+    using K = KernelOf<LV, kLines>;
+    cudaError_t e = prepare(K::fn(), K::smem(), K::done());
     if (e != cudaSuccess) return e;
-    line_index_kernel<LV><<<grid, kThreads, sizeof(FShared<LV>), stream>>>(p);
+    if (kLines)
+        line_index_kernel<LV><<<grid, kThreads, sizeof(FShared<LV>), stream>>>(p);
+    else
+        tile_index_kernel<LV><<<grid, kIndexThreads, sizeof(TShared), stream>>>(p);
     return cudaGetLastError();
 }
 
 }  // namespace
 
 int line_index_max_ctas_per_sm(int lv) {
-    if (lv <= 4) return occupancy<4>();
-    if (lv <= 8) return occupancy<8>();
-    return occupancy<16>();
+    if (lv <= 4) return occupancy<4, true>();
+    if (lv <= 8) return occupancy<8, true>();
+    return occupancy<16, true>();
 }
 
 cudaError_t launch_line_index_kernel(const IndexParams& p, int grid, cudaStream_t stream) {
-    if (p.num_levels <= 4) return launch<4>(p, grid, stream);
-    if (p.num_levels <= 8) return launch<8>(p, grid, stream);
-    return launch<16>(p, grid, stream);
+    if (p.num_levels <= 4) return launch<4, true>(p, grid, stream);
+    if (p.num_levels <= 8) return launch<8, true>(p, grid, stream);
+    return launch<16, true>(p, grid, stream);
+}
+
+int tile_index_max_ctas_per_sm(int lv) {
+    if (lv <= 4) return occupancy<4, false>();
+    if (lv <= 8) return occupancy<8, false>();
+    return occupancy<16, false>();
+}
+
+cudaError_t launch_tile_index_kernel(const IndexParams& p, int grid, cudaStream_t stream) {
+    if (p.num_levels <= 4) return launch<4, false>(p, grid, stream);
+    if (p.num_levels <= 8) return launch<8, false>(p, grid, stream);
+    return launch<16, false>(p, grid, stream);
 }
 
 }  // namespace gpj
