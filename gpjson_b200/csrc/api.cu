@@ -234,7 +234,9 @@ int alloc_tile_scratch(gpj_ctx* ctx, int64_t n, TileScratch* ts) {
     const int64_t ntiles = (n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
     int rc = device_alloc(ctx, &ts->bits, static_cast<size_t>((n + 63) / 64), "cudaMalloc(newline bitmap)");
     if (!rc) rc = device_alloc(ctx, &ts->counts, static_cast<size_t>(ntiles), "cudaMalloc(tile counts)");
-    if (!rc) rc = device_alloc(ctx, &ts->offsets, static_cast<size_t>(ntiles), "cudaMalloc(tile offsets)");
+    if (!rc)
+        rc = device_alloc(ctx, &ts->offsets, static_cast<size_t>(gpj::newline_offsets_words(ntiles)),
+                          "cudaMalloc(tile offsets)");
     return rc;
 }
 
@@ -480,8 +482,8 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
     return GPJ_OK;
 }
 
-// Bytes copied per step of load_and_index: 5461 line-kernel tiles (~64 MiB).
-constexpr int64_t kLoadChunk = gpj::kLineTileBytes * 5461;
+// Bytes copied per step of load_and_index: 4681 line-kernel tiles (~64 MiB).
+constexpr int64_t kLoadChunk = gpj::kLineTileBytes * 4681;
 
 // Copies n host bytes into f->d_owned in chunks on the copy stream and
 // indexes chunk k with the line-parallel kernel as soon as chunk k + 1 has

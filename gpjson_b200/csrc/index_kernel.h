@@ -8,9 +8,9 @@
 namespace gpj {
 
 constexpr int64_t kIndexTileBytes = 16384;  // exact kernel
-// The line-parallel kernel owns 12 KiB per tile and reads 4 KiB past it, so
+// The line-parallel kernel owns 14 KiB per tile and reads 2 KiB past it, so
 // that a tile and its look-ahead are one 64-byte word per index thread.
-constexpr int64_t kLineTileBytes = 12288;
+constexpr int64_t kLineTileBytes = 14336;
 // The escape state at a tile start is found by scanning back over the bytes
 // before it; a backslash run longer than this crossing a tile start is
 // reported as an error (kErrEscapeRun) instead of being resolved.
@@ -75,9 +75,11 @@ cudaError_t launch_tile_index_kernel(const IndexParams& p, int grid, cudaStream_
 int tile_index_max_ctas_per_sm(int num_levels);
 
 // Newline index from newline_bits and tile_newlines (tiles of
-// kLineTileBytes): exclusive offsets of the tile counts into `offsets`
-// (ntiles entries), then every tile's '\n' positions; writes status[0] =
+// kLineTileBytes): offsets of the tile counts within blocks of 1024 tiles
+// and the block sums into `offsets` (newline_offsets_words(ntiles)
+// entries), then every tile's '\n' positions; writes status[0] =
 // newlines + 1 and at most newline_cap entries.  Two launches, one stream.
 cudaError_t launch_newline_index(const IndexParams& p, int64_t* offsets, int grid, cudaStream_t stream);
+inline int64_t newline_offsets_words(int64_t ntiles) { return ntiles + (ntiles + 1023) / 1024; }
 
 }  // namespace gpj

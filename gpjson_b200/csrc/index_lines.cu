@@ -4,9 +4,9 @@
 // In newline-delimited JSON every line is a complete value, so at each
 // '\n' the reference's scan state (Sequential.java:36-128: inside-string
 // flag, level counter, escape flag) is (outside, -1, clear) again.  This
-// kernel uses that: the CTA that owns a 12 KiB tile builds the index of
+// kernel uses that: the CTA that owns a 14 KiB tile builds the index of
 // every line that starts in it, starting each line from that state, and runs
-// on past the tile end to finish its last line (in the 4 KiB look-ahead
+// on past the tile end to finish its last line (in the 2 KiB look-ahead
 // loaded with the tile, or from device memory for longer lines).  No string or level carry
 // crosses tiles, so CTAs depend on each other only through the newline
 // count, which a decoupled look-back resolves off the critical path.
@@ -52,9 +52,9 @@ namespace gpj {
 
 namespace {
 
-constexpr int64_t kTile = kLineTileBytes;            // 12 KiB owned per tile
-constexpr int kTileWords = kTile / 64;               // 192
-constexpr int64_t kExtBytes = 4096;                  // look-ahead loaded with the tile
+constexpr int64_t kTile = kLineTileBytes;            // 14 KiB owned per tile
+constexpr int kTileWords = kTile / 64;               // 224
+constexpr int64_t kExtBytes = 2048;                  // look-ahead loaded with the tile
 constexpr int64_t kSlotBytes = kTile + kExtBytes;    // 16 KiB: one word per index thread
 constexpr int kSlotWords = kTileWords + kExtBytes / 64;  // 256
 static_assert(kSlotWords == 256 && kSlotBytes == kRoundBytes, "one slot word per index thread");
