@@ -352,6 +352,59 @@ class File:
             pass
 
 
+def _result_array(lib, r) -> np.ndarray:
+    """Copies a gpj_result into int64 [nq][lines][slots][2] and releases it."""
+    try:
+        nq, lines, slots = lib.gpj_result_num_queries(r), lib.gpj_result_num_lines(r), lib.gpj_result_slots(r)
+        count = nq * lines * slots * 2
+        ptr = lib.gpj_result_offsets(r)
+        buf = (ctypes.c_int64 * count).from_address(ptr) if count else []
+        return np.array(buf, dtype=np.int64, copy=True).reshape(nq, lines, slots, 2)
+    finally:
+        lib.gpj_result_release(r)
+
+
+class Batch:
+    """gpj_batch: many (file, paths) requests indexed and evaluated together
+    (one index launch for the files that need it, one find_value launch, one
+    copy back).  Each request's results equal File.query_paths on its file."""
+
+    def __init__(self, native: "_Native"):
+        self._native = native
+        self._h = c_void_p()
+        native.check(native.lib.gpj_batch_create(native.h, byref(self._h)))
+        self._files: list[File] = []  # kept alive until the batch is cleared
+
+    def add(self, file: "File", paths: list[str]) -> int:
+        arr = (c_char_p * len(paths))(*[p.encode("utf-8") for p in paths])
+        item = c_int()
+        self._native.check(self._native.lib.gpj_batch_add(self._h, file._h, len(paths), arr, byref(item)))
+        self._files.append(file)
+        return item.value
+
+    def run(self) -> None:
+        self._native.check(self._native.lib.gpj_batch_run(self._h))
+
+    def result(self, item: int) -> np.ndarray:
+        """int64 [nq][lines][slots][2] of request `item`."""
+        r = c_void_p()
+        self._native.check(self._native.lib.gpj_batch_result(self._h, item, byref(r)))
+        return _result_array(self._native.lib, r)
+
+    def __len__(self) -> int:
+        return self._native.lib.gpj_batch_size(self._h)
+
+    def clear(self) -> None:
+        self._native.lib.gpj_batch_clear(self._h)
+        self._files.clear()
+
+    def release(self) -> None:
+        if self._h:
+            self._native.lib.gpj_batch_release(self._h)
+            self._h = c_void_p()
+            self._files.clear()
+
+
 class GPJSON:
     """The library object of GPJSONLibrary.java: members ``query`` and
     ``exportTimings``."""
@@ -387,6 +440,9 @@ class GPJSON:
         h = c_void_p()
         self._native.check(self._native.lib.gpj_file_from_device(self._native.h, c_void_p(ptr), n, byref(h)))
         return File(self._native, h, keepalive=keepalive)
+
+    def batch(self) -> Batch:
+        return Batch(self._native)
 
     def set_query_fusion(self, enabled: bool) -> None:
         """Evaluate queries inside the index kernel (True) or with one

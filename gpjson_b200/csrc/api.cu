@@ -99,6 +99,28 @@ struct gpj_result {
     std::vector<int64_t> offsets;
 };
 
+// Requests (file, paths) evaluated together by gpj_batch_run.
+struct gpj_batch {
+    gpj_ctx* ctx = nullptr;
+    struct Item {
+        gpj_file* file = nullptr;
+        std::vector<gpj::CompiledPath> queries;
+        int file_slot = -1;  // index into `files` after a run
+        int q0 = 0;          // first of the item's queries in its file's query list
+    };
+    struct FileRun {
+        gpj_file* file = nullptr;
+        std::vector<const gpj::CompiledPath*> queries;
+        int depth = 0, slots = 1;
+        int64_t lines = 0;
+        size_t out_offset = 0;  // elements into `results`
+    };
+    std::vector<Item> items;
+    std::vector<FileRun> files;
+    std::vector<int64_t> results;
+    bool ran = false;
+};
+
 namespace {
 
 int fail(gpj_ctx* ctx, int code, const std::string& msg) {
@@ -1186,5 +1208,314 @@ void gpj_reset_timings(gpj_ctx* ctx) {
 }
 
 int64_t gpj_kernel_launches(const gpj_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+}  // extern "C"
+
+// ---- batches ---------------------------------------------------------------------
+
+namespace {
+
+// Indexes the batch's files whose resident index is missing or too shallow:
+// one standalone index launch over all their tiles, one newline pass, one
+// status read-back.  Files the batch launch cannot index (not line-delimited,
+// a line longer than the look-ahead allows, more lines than estimated) are
+// indexed again alone.
+int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
+    std::vector<gpj_file*> need;
+    int levels = 1;
+    for (auto& fr : files) {
+        gpj_file* f = fr.file;
+        if (!f->indexed || f->num_levels < fr.depth) {
+            need.push_back(f);
+            levels = std::max(levels, fr.depth);
+        }
+    }
+    if (need.empty()) return GPJ_OK;
+    const double t0 = now_ms();
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    std::vector<gpj::TileFile> tf;
+    std::vector<gpj::LineFile> lf;
+    std::vector<gpj_file*> batched;
+    int64_t total_tiles = 0, total_words = 0;
+    int rc = GPJ_OK;
+    for (gpj_file* f : need) {
+        if ((rc = ensure_index_buffers(ctx, f, levels))) return rc;
+        f->indexed = false;
+        if (f->n == 0) continue;  // indexed alone below
+        batched.push_back(f);
+        total_tiles += (f->n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+        total_words += f->words;
+    }
+    const int nb = static_cast<int>(batched.size());
+    if (nb > 0) {
+        uint64_t* bits = nullptr;
+        int32_t* counts = nullptr;
+        int64_t* offsets = nullptr;
+        unsigned long long* status = nullptr;
+        gpj::TileFile* d_tf = nullptr;
+        gpj::LineFile* d_lf = nullptr;
+        rc = device_alloc(ctx, &bits, static_cast<size_t>(total_words), "cudaMalloc(batch newline bitmaps)");
+        if (!rc) rc = device_alloc(ctx, &counts, static_cast<size_t>(total_tiles), "cudaMalloc(batch tile counts)");
+        if (!rc)
+            rc = device_alloc(ctx, &offsets, static_cast<size_t>(gpj::newline_offsets_words(total_tiles)),
+                              "cudaMalloc(batch tile offsets)");
+        if (!rc) rc = device_alloc(ctx, &status, static_cast<size_t>(2 * nb), "cudaMalloc(batch status)");
+        if (!rc) rc = device_alloc(ctx, &d_tf, static_cast<size_t>(nb), "cudaMalloc(batch files)");
+        if (!rc) rc = device_alloc(ctx, &d_lf, static_cast<size_t>(nb), "cudaMalloc(batch line files)");
+        std::vector<unsigned long long> h_status(2 * static_cast<size_t>(nb));
+        if (!rc) {
+            int64_t tile = 0, word = 0;
+            for (int i = 0; i < nb; i++) {
+                gpj_file* f = batched[i];
+                const int64_t ntiles = (f->n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+                tf.push_back(gpj::TileFile{f->d_data, f->n, f->n, f->d_str, f->d_lvl, f->words, bits + word,
+                                           status + 2 * i, tile});
+                lf.push_back(gpj::LineFile{bits + word, f->words, f->d_nl, f->nl_cap, status + 2 * i, tile, ntiles});
+                tile += ntiles;
+                word += f->words;
+            }
+            cudaError_t e = cudaMemsetAsync(status, 0, 2 * sizeof(unsigned long long) * nb, ctx->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_tf, tf.data(), sizeof(gpj::TileFile) * nb, cudaMemcpyHostToDevice, ctx->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_lf, lf.data(), sizeof(gpj::LineFile) * nb, cudaMemcpyHostToDevice, ctx->stream);
+            if (e == cudaSuccess) {
+                gpj::IndexParams p{};
+                p.num_levels = levels;
+                p.materialize = 1;
+                p.tile_begin = 0;
+                p.tile_end = total_tiles;
+                p.batch = d_tf;
+                p.batch_files = nb;
+                p.status = ctx->d_status;
+                p.tile_newlines = counts;
+                const int occ = ctx->tile_occupancy[occupancy_slot(levels)];
+                const int64_t grid = std::min<int64_t>(total_tiles, static_cast<int64_t>(ctx->sms) * occ);
+                e = gpj::launch_tile_index_kernel(p, static_cast<int>(grid), ctx->stream);
+                ctx->launches++;
+            }
+            if (e == cudaSuccess) {
+                const int64_t grid = std::min<int64_t>((total_tiles + 7) / 8, static_cast<int64_t>(ctx->sms) * 8);
+                e = gpj::launch_newline_index_batch(counts, total_tiles, d_lf, nb, offsets, static_cast<int>(grid),
+                                                    ctx->stream);
+                ctx->launches += 2;
+            }
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(h_status.data(), status, 2 * sizeof(unsigned long long) * nb,
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            if (e != cudaSuccess) rc = cuda_fail(ctx, e, "batch index");
+        }
+        device_free(ctx, bits);
+        device_free(ctx, counts);
+        device_free(ctx, offsets);
+        device_free(ctx, status);
+        device_free(ctx, d_tf);
+        device_free(ctx, d_lf);
+        if (rc) return rc;
+        if ((rc = status_error(ctx, ctx->h_status[1]))) return rc;
+        for (int i = 0; i < nb; i++) {
+            gpj_file* f = batched[i];
+            const unsigned long long errs = h_status[2 * i + 1];
+            const int64_t lines = static_cast<int64_t>(h_status[2 * i]);
+            if ((errs & (gpj::kErrIrregular | gpj::kErrLongLine)) || lines > f->nl_cap) continue;  // alone below
+            if ((rc = status_error(ctx, errs))) return rc;
+            f->num_lines = lines;
+            f->num_levels = levels;
+            f->indexed = true;
+        }
+    }
+    for (gpj_file* f : need)
+        if (!f->indexed && (rc = index_pass(ctx, f, levels, nullptr, nullptr))) return rc;
+    return end_phase(ctx, "batch_index", t0);
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpj_batch_create(gpj_ctx* ctx, gpj_batch** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    gpj_batch* b = new (std::nothrow) gpj_batch;
+    if (!b) return fail(ctx, GPJ_ENOMEM, "out of host memory");
+    b->ctx = ctx;
+    *out = b;
+    return GPJ_OK;
+}
+
+int gpj_batch_add(gpj_batch* b, gpj_file* f, int nq, const char* const* paths, int* item) {
+    if (!b) return GPJ_EINVAL;
+    gpj_ctx* ctx = b->ctx;
+    if (!f || !paths || nq < 1 || !item) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (nq > GPJ_MAX_QUERIES) return fail(ctx, GPJ_ELIMIT, "Maximum size of queries is 255");
+    int dev = -1;
+    if (f->ctx) dev = f->ctx->device;
+    if (dev != ctx->device) return fail(ctx, GPJ_EINVAL, "file is on another device");
+    gpj_batch::Item it;
+    it.file = f;
+    for (int i = 0; i < nq; i++) {
+        try {
+            it.queries.push_back(gpj::compile_path(paths[i] ? paths[i] : ""));
+        } catch (const gpj::PathError& e) {
+            if (e.unsupported)
+                return fail(ctx, GPJ_EUNSUPPORTED, "Unsupported JSON path (" + std::to_string(i) + "): " + e.what());
+            return fail(ctx, GPJ_EPARSE, "Failed to parse JSON path (" + std::to_string(i) + "): " + e.what());
+        }
+        if (it.queries.back().max_depth > GPJ_MAX_LEVELS)
+            return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(it.queries.back().max_depth));
+    }
+    b->items.push_back(std::move(it));
+    b->ran = false;
+    *item = static_cast<int>(b->items.size() - 1);
+    return GPJ_OK;
+}
+
+int gpj_batch_run(gpj_batch* b) {
+    if (!b) return GPJ_EINVAL;
+    gpj_ctx* ctx = b->ctx;
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    b->files.clear();
+    b->results.clear();
+    b->ran = false;
+    for (auto& it : b->items) {
+        int slot = -1;
+        for (size_t i = 0; i < b->files.size(); i++)
+            if (b->files[i].file == it.file) slot = static_cast<int>(i);
+        if (slot < 0) {
+            b->files.emplace_back();
+            b->files.back().file = it.file;
+            slot = static_cast<int>(b->files.size() - 1);
+        }
+        auto& fr = b->files[slot];
+        it.file_slot = slot;
+        it.q0 = static_cast<int>(fr.queries.size());
+        for (auto& q : it.queries) {
+            fr.queries.push_back(&q);
+            fr.depth = std::max(fr.depth, q.max_depth);
+            fr.slots = std::max(fr.slots, q.num_results);
+        }
+    }
+    if (b->files.empty()) return GPJ_OK;
+    if ((rc = batch_index(ctx, b->files))) return rc;
+
+    // one find_value launch over every line of every file
+    const double t0 = now_ms();
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    std::vector<uint8_t> blob;  // per file: [int32 offsets (16-byte padded)][bytecode]
+    std::vector<size_t> blob_at(b->files.size());
+    size_t total_out = 0;
+    int64_t total_lines = 0;
+    for (size_t i = 0; i < b->files.size(); i++) {
+        auto& fr = b->files[i];
+        const size_t nq = fr.queries.size();
+        blob_at[i] = blob.size();
+        const size_t header = ((nq * 4 + 15) / 16) * 16;
+        blob.resize(blob.size() + header, 0);
+        size_t code = 0;
+        for (size_t q = 0; q < nq; q++) {
+            const int32_t off = static_cast<int32_t>(code);
+            std::memcpy(blob.data() + blob_at[i] + 4 * q, &off, 4);
+            blob.insert(blob.end(), fr.queries[q]->bytecode.begin(), fr.queries[q]->bytecode.end());
+            code += fr.queries[q]->bytecode.size();
+        }
+        blob.resize((blob.size() + 15) / 16 * 16, 0);
+        fr.lines = fr.file->num_lines;
+        fr.out_offset = total_out;
+        total_out += nq * static_cast<size_t>(fr.lines) * fr.slots * 2;
+        total_lines += fr.lines;
+    }
+    uint8_t* d_blob = nullptr;
+    int64_t* d_out = nullptr;
+    gpj::QueryFile* d_qf = nullptr;
+    rc = device_alloc(ctx, &d_blob, blob.size(), "cudaMalloc(batch bytecode)");
+    if (!rc) rc = device_alloc(ctx, &d_out, std::max<size_t>(total_out, 1), "cudaMalloc(batch results)");
+    if (!rc) rc = device_alloc(ctx, &d_qf, b->files.size(), "cudaMalloc(batch query files)");
+    if (!rc) {
+        std::vector<gpj::QueryFile> qf;
+        int64_t line = 0;
+        for (size_t i = 0; i < b->files.size(); i++) {
+            auto& fr = b->files[i];
+            gpj_file* f = fr.file;
+            const size_t nq = fr.queries.size();
+            const size_t header = ((nq * 4 + 15) / 16) * 16;
+            qf.push_back(gpj::QueryFile{f->d_data, f->n, f->d_nl, fr.lines, f->d_str, f->d_lvl, f->words,
+                                        d_blob + blob_at[i] + header,
+                                        reinterpret_cast<const int32_t*>(d_blob + blob_at[i]),
+                                        static_cast<int>(nq), fr.slots, d_out + fr.out_offset, fr.lines, line});
+            line += fr.lines;
+        }
+        cudaError_t e = cudaMemcpyAsync(d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_qf, qf.data(), sizeof(gpj::QueryFile) * qf.size(), cudaMemcpyHostToDevice,
+                                ctx->stream);
+        if (e == cudaSuccess && total_lines > 0) {
+            const int64_t grid =
+                std::max<int64_t>(1, std::min<int64_t>((total_lines + 255) / 256, static_cast<int64_t>(ctx->sms) * 8));
+            e = gpj::launch_find_value_batch(d_qf, static_cast<int>(qf.size()), total_lines, static_cast<int>(grid),
+                                             ctx->stream);
+            ctx->launches++;
+        }
+        try {
+            b->results.resize(total_out);
+        } catch (const std::bad_alloc&) {
+            rc = fail(ctx, GPJ_ENOMEM, "out of host memory for results");
+        }
+        if (!rc && e == cudaSuccess && total_out > 0)
+            e = cudaMemcpyAsync(b->results.data(), d_out, total_out * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "batch query");
+    }
+    device_free(ctx, d_blob);
+    device_free(ctx, d_out);
+    device_free(ctx, d_qf);
+    if (rc) return rc;
+    rc = end_phase(ctx, "batch_query", t0);
+    if (rc) return rc;
+    b->ran = true;
+    return GPJ_OK;
+}
+
+int gpj_batch_result(gpj_batch* b, int item, gpj_result** out) {
+    if (!b) return GPJ_EINVAL;
+    gpj_ctx* ctx = b->ctx;
+    if (!out || item < 0 || item >= static_cast<int>(b->items.size())) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (!b->ran) return fail(ctx, GPJ_ESTATE, "batch has not run since its last change");
+    const auto& it = b->items[item];
+    const auto& fr = b->files[it.file_slot];
+    gpj_result* r = new (std::nothrow) gpj_result;
+    if (!r) return fail(ctx, GPJ_ENOMEM, "out of host memory");
+    r->nq = static_cast<int64_t>(it.queries.size());
+    r->lines = fr.lines;
+    r->slots = fr.slots;
+    const size_t per_query = static_cast<size_t>(fr.lines) * fr.slots * 2;
+    const int64_t* src = b->results.data() + fr.out_offset + it.q0 * per_query;
+    try {
+        r->offsets.assign(src, src + r->nq * per_query);
+    } catch (const std::bad_alloc&) {
+        delete r;
+        return fail(ctx, GPJ_ENOMEM, "out of host memory for results");
+    }
+    *out = r;
+    return GPJ_OK;
+}
+
+int gpj_batch_size(const gpj_batch* b) { return b ? static_cast<int>(b->items.size()) : -1; }
+
+void gpj_batch_clear(gpj_batch* b) {
+    if (!b) return;
+    b->items.clear();
+    b->files.clear();
+    b->results.clear();
+    b->ran = false;
+}
+
+void gpj_batch_release(gpj_batch* b) { delete b; }
 
 }  // extern "C"

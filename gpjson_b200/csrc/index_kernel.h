@@ -16,6 +16,22 @@ constexpr int64_t kLineTileBytes = 14336;
 // reported as an error (kErrEscapeRun) instead of being resolved.
 constexpr int64_t kEscapeScanBytes = 1 << 16;
 
+// The file a tile of the standalone index kernel belongs to.  A build over
+// one file uses IndexParams' own fields; a batch passes one entry per file,
+// tiles numbered consecutively over the files (tile_begin = the file's first
+// tile), positions and outputs relative to the file.
+struct TileFile {
+    const uint8_t* file;
+    int64_t n;
+    int64_t avail;            // bytes [0, avail) readable
+    uint64_t* string_index;
+    uint64_t* leveled;        // num_levels * level_size words
+    int64_t level_size;
+    uint64_t* newline_bits;
+    unsigned long long* status;  // [0] line count, [1] error bits
+    int64_t tile_begin;
+};
+
 struct IndexParams {
     const uint8_t* file;
     int64_t n;
@@ -44,6 +60,12 @@ struct IndexParams {
     // the newline count of every tile, in place of the newline index.
     uint64_t* newline_bits;
     int32_t* tile_newlines;
+    // Standalone kernel over a batch of files (batch_files > 0): tiles
+    // [tile_begin, tile_end) of the whole batch, file table `batch`
+    // (ascending tile_begin); status then reports errors that concern no
+    // single file (wait timeouts).
+    const TileFile* batch;
+    int batch_files;
 
     // Queries evaluated in the same pass (line-parallel kernel only; 0 = none).
     int num_queries;
@@ -81,5 +103,21 @@ int tile_index_max_ctas_per_sm(int num_levels);
 // newlines + 1 and at most newline_cap entries.  Two launches, one stream.
 cudaError_t launch_newline_index(const IndexParams& p, int64_t* offsets, int grid, cudaStream_t stream);
 inline int64_t newline_offsets_words(int64_t ntiles) { return ntiles + (ntiles + 1023) / 1024; }
+
+// Where the newline index of one file of a batch goes.
+struct LineFile {
+    const uint64_t* newline_bits;
+    int64_t words;               // ceil(n / 64)
+    int64_t* newlines;
+    int64_t cap;                 // entries `newlines` holds
+    unsigned long long* status;  // [0] receives the line count
+    int64_t tile_begin;          // the file's first tile in the batch
+    int64_t ntiles;
+};
+
+// Newline indexes of a batch (tile_newlines of all its tiles, ascending
+// tile_begin in `files`, a device array of nfiles entries).
+cudaError_t launch_newline_index_batch(const int32_t* tile_newlines, int64_t total_tiles, const LineFile* files,
+                                       int nfiles, int64_t* offsets, int grid, cudaStream_t stream);
 
 }  // namespace gpj

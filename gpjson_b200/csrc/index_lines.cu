@@ -207,6 +207,7 @@ __device__ __forceinline__ RSpan shfl_rspan_up(const RSpan& v, int off) {
 template <int LV>
 struct FShared {
     uint8_t bytes[kRing][kSlotBytes];
+    TileFile desc[kRing];  // the file of the tile in each byte slot
     uint64_t str[kMaskSlots][kSlotWords];
     uint64_t colon[kMaskSlots][kSlotWords];
     uint64_t lv[kMaskSlots][LV][kSlotWords];
@@ -235,6 +236,7 @@ struct FShared {
 // Shared memory of the standalone index kernel (no line warps, no queries).
 struct TShared {
     uint8_t bytes[kRing][kSlotBytes];
+    TileFile desc[kRing];
     uint64_t full[kRing];
     Span span_scratch[kTileWarps];
     RSpan rscan[2][kTileWarps];
@@ -336,20 +338,21 @@ __device__ __forceinline__ ClassMasks classify_global(const uint8_t* file, int64
 // in mask slot `ms` at `slot` (>= 0) and writes it to the global index when
 // `owned`.
 template <int LV, bool kMasks, class Sh>
-__device__ __forceinline__ void finish_word(const IndexParams& p, Sh& sh, int ms, const ClassMasks& m,
+__device__ __forceinline__ void finish_word(const IndexParams& p, const TileFile& F, Sh& sh, int ms,
+                                            const ClassMasks& m,
                                             uint64_t p0, int s_w, int64_t d_w, int64_t word, bool owned, int slot,
                                             uint64_t valid, uint64_t check) {
     const uint64_t in_str = (p0 ^ (s_w ? ~0ull : 0ull)) & valid;
     const uint64_t open = m.open & ~in_str, close = m.close & ~in_str;
     if (check) {
         // every checked '\n' must be outside strings at level -1
-        if (check & in_str) atomicOr(p.status + 1, kErrIrregular);
+        if (check & in_str) atomicOr(F.status + 1, kErrIrregular);
         uint64_t c = check;
         while (c) {
             const int bit = ctz64(c);
             const uint64_t below = (1ull << bit) - 1;
             const int64_t d = d_w + popc64(open & below) - popc64(close & below);
-            if (d != -1) atomicOr(p.status + 1, kErrIrregular);
+            if (d != -1) atomicOr(F.status + 1, kErrIrregular);
             c &= c - 1;
         }
     }
@@ -365,16 +368,16 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, Sh& sh, int ms
         }
     }
     if (owned && p.materialize) {
-        p.string_index[word] = in_str;
+        F.string_index[word] = in_str;
 #pragma unroll
         for (int l = 0; l < LV; l++)
-            if (l < p.num_levels) p.leveled[p.level_size * l + word] = lv[l];
+            if (l < p.num_levels) F.leveled[F.level_size * l + word] = lv[l];
     }
 }
 
 // The long tail of a line that runs past the slot: first '\n' from `from`
 // (warp 0 of the index group); flags lines beyond kMaxExtension.
-__device__ int64_t find_line_end(const IndexParams& p, int64_t from, int64_t tile_end) {
+__device__ int64_t find_line_end(const TileFile& p, int64_t from, int64_t tile_end) {
     const int lane = threadIdx.x & 31;
     int64_t found = kNone;
     int64_t limit = p.n - tile_end > kMaxExtension ? tile_end + kMaxExtension : p.n;
@@ -412,6 +415,36 @@ __device__ int64_t find_line_end(const IndexParams& p, int64_t from, int64_t til
     return found == kNone ? p.n : found;
 }
 
+// The file of (batch-wide) tile t.
+__device__ __forceinline__ void fetch_tile_file(const IndexParams& p, int64_t t, TileFile* out) {
+    if (p.batch_files == 0) {
+        *out = TileFile{p.file,     p.n,     p.avail,        p.string_index, p.leveled,
+                        p.level_size, p.newline_bits, p.status, 0};
+        return;
+    }
+    int lo = 0, hi = p.batch_files - 1;  // last file with tile_begin <= t
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.batch[mid].tile_begin <= t)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    *out = p.batch[lo];
+}
+
+// Starts the TMA copy of tile t into byte slot `slot` (one thread); the
+// tile's file goes into sh.desc[slot] before the copy's mbarrier arrive, so
+// the threads that wait for the copy also see it.
+template <class Sh>
+__device__ __forceinline__ void start_tile(const IndexParams& p, Sh& sh, int64_t t, int slot) {
+    TileFile& F = sh.desc[slot];
+    fetch_tile_file(p, t, &F);
+    const int64_t start = (t - F.tile_begin) * kTile;
+    load_slot(F.file, start, F.avail - start < kSlotBytes ? F.avail - start : kSlotBytes, sh.bytes[slot],
+              &sh.full[slot]);
+}
+
 // ---- index warps -------------------------------------------------------------
 // kLines: line warps run beside these warps (FShared: newline index by
 // look-back, in-kernel queries); otherwise the kernel is these warps alone
@@ -422,11 +455,7 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
     const int tid = threadIdx.x;  // 0..255
     unsigned long long* nl_agg = p.tile_state;
     const int64_t first_tile = p.tile_begin + blockIdx.x, stride = gridDim.x;
-    if (tid == 0 && first_tile < p.tile_end) {
-        const int64_t start = first_tile * kTile;
-        load_slot(p.file, start, p.avail - start < kSlotBytes ? p.avail - start : kSlotBytes, sh.bytes[0],
-                  &sh.full[0]);
-    }
+    if (tid == 0 && first_tile < p.tile_end) start_tile(p, sh, first_tile, 0);
     int64_t k = 0;
     for (int64_t t = first_tile; t < p.tile_end; t += stride, ++k) {
         const int bs = static_cast<int>(k % kRing), ms = static_cast<int>(k & 1);
@@ -439,16 +468,16 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                 if (nuse > 0 && !mbar_wait_idle(&sh.bfree[nb], (nuse - 1) & 1))
                     atomicOr(p.status + 1, kErrCopyTimeout);
             }
-            const int64_t start = (t + stride) * kTile;
-            load_slot(p.file, start, p.avail - start < kSlotBytes ? p.avail - start : kSlotBytes, sh.bytes[nb],
-                      &sh.full[nb]);
+            start_tile(p, sh, t + stride, nb);
         }
         if (!mbar_wait_bounded(&sh.full[bs], buse & 1) && tid == 0) atomicOr(p.status + 1, kErrCopyTimeout);
         const uint8_t* buf = sh.bytes[bs];
+        const TileFile& F = sh.desc[bs];
+        const int64_t lt = t - F.tile_begin;  // the tile's index in its file
 
-        const int64_t tile_start = t * kTile;
-        const int64_t tile_end = p.n - tile_start < kTile ? p.n : tile_start + kTile;
-        const int64_t loaded_end = p.avail - tile_start < kSlotBytes ? p.avail : tile_start + kSlotBytes;
+        const int64_t tile_start = lt * kTile;
+        const int64_t tile_end = F.n - tile_start < kTile ? F.n : tile_start + kTile;
+        const int64_t loaded_end = F.avail - tile_start < kSlotBytes ? F.avail : tile_start + kSlotBytes;
         const int64_t ws = tile_start + 64 * tid;
 
         // ---- one round over the slot: the tile's words and the look-ahead after it
@@ -487,7 +516,7 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
         if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(cout);
         RSpan total;
         RSpan ex = index_scan_rspan(mine, sh.rscan[k & 1], &total);
-        if (t == 0) {  // the file's first line starts at byte 0
+        if (lt == 0) {  // the file's first line starts at byte 0
             const RSpan init{2, -1, 0, 0};
             ex = rspan_compose(init, ex);
             total = rspan_compose(init, total);
@@ -515,18 +544,18 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                     nm &= nm - 1;
                 }
             } else {
-                if (ws < tile_end) p.newline_bits[ws >> 6] = m.newline;
+                if (ws < tile_end) F.newline_bits[ws >> 6] = m.newline;
             }
             if (ex.rq & 2) {
                 // every byte of the word belongs to lines that start in this tile
                 if (ws < tile_end)
-                    finish_word<LV, kLines>(p, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, slot, valid, m.newline);
+                    finish_word<LV, kLines>(p, F, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, slot, valid, m.newline);
             } else if (has_nl) {
                 // the tile's first line starts at byte f of this word
                 sh.first_line = ws + f;
                 ClassMasks mm = m;
                 restrict_masks(mm, after);
-                finish_word<LV, kLines>(p, sh, ms, mm, pa, 0, -1, ws >> 6, f == 0, slot, valid, m.newline & after);
+                finish_word<LV, kLines>(p, F, sh, ms, mm, pa, 0, -1, ws >> 6, f == 0, slot, valid, m.newline & after);
             }
         } else if (lines_here && (ex.nl >> 16) == 0 && valid) {
             // No '\n' between the tile end and this word: the tile's last line
@@ -534,20 +563,20 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
             // one checked here); a word that starts with it belongs to the next tile.
             if (has_nl) sh.ext_b = ws + f;
             if (!(has_nl && f == 0))
-                finish_word<LV, kLines>(p, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, slot, valid,
+                finish_word<LV, kLines>(p, F, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, slot, valid,
                                 has_nl ? (1ull << f) : 0ull);
         }
         group_sync(kBarIndex, kIndexThreads);  // the tile's masks are complete in the slot
 
-        const int64_t a_t = t == 0 ? 0 : (lines_here ? sh.first_line : kNone);
+        const int64_t a_t = lt == 0 ? 0 : (lines_here ? sh.first_line : kNone);
         int64_t b_t = tile_end, hi = tile_end;
-        if (lines_here && tile_end < p.n) {
+        if (lines_here && tile_end < F.n) {
             if (ahead_nl > 0) {
                 b_t = sh.ext_b;
                 hi = b_t;
-            } else if (loaded_end == p.n) {
-                b_t = p.n;
-                hi = p.n;
+            } else if (loaded_end == F.n) {
+                b_t = F.n;
+                hi = F.n;
             } else {
                 // a line longer than the look-ahead: continue past the slot
                 // straight from device memory
@@ -555,7 +584,7 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                 const int64_t d_in = total.d0;
                 const int esc_in = sh.carry_esc;
                 if (tid < 32) {
-                    const int64_t e2 = find_line_end(p, loaded_end, tile_end);
+                    const int64_t e2 = find_line_end(F, loaded_end, tile_end);
                     if (tid == 0) sh.long_b = e2;
                 }
                 group_sync(kBarIndex, kIndexThreads);
@@ -564,12 +593,12 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                 const int64_t own_end = (b_t + 63) & ~static_cast<int64_t>(63);
                 int s = s_in, esc = esc_in;
                 int64_t d = d_in;
-                for (int64_t cs = loaded_end; cs < own_end && cs < p.n; cs += kRoundBytes) {
+                for (int64_t cs = loaded_end; cs < own_end && cs < F.n; cs += kRoundBytes) {
                     const int64_t cw = cs + 64 * tid;
-                    const uint64_t cvalid = cw < own_end ? bits_between(0, p.n - cw) : 0ull;
+                    const uint64_t cvalid = cw < own_end ? bits_between(0, F.n - cw) : 0ull;
                     ClassMasks c{0, 0, 0, 0, 0, 0, 0};
                     if (cvalid) {
-                        c = classify_global(p.file, p.n, cw);
+                        c = classify_global(F.file, F.n, cw);
                         restrict_masks(c, cvalid);
                     }
                     // escape carry: previous word's trailing run, else the bytes before
@@ -583,7 +612,7 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                     } else {
                         int run = 0;
                         int64_t j = cw - 1;
-                        while (j >= cs && __ldg(p.file + j) == '\\') {
+                        while (j >= cs && __ldg(F.file + j) == '\\') {
                             ++run;
                             --j;
                         }
@@ -600,7 +629,7 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                     const uint64_t ccheck =
                         (b_t >= cw && b_t < cw + 64) ? (c.newline & (1ull << (b_t - cw))) : 0ull;
                     if (cvalid)
-                        finish_word<LV, kLines>(p, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
+                        finish_word<LV, kLines>(p, F, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
                                         cw >> 6, true, -1, cvalid, ccheck);
                     if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(ccout);
                     group_sync(kBarIndex, kIndexThreads);

@@ -5,7 +5,9 @@
 //
 // offsets: block scans of the tile counts, 1024 tiles per CTA.  scatter: a
 // warp per tile adds the sums of the earlier blocks to the tile's offset and
-// writes its positions, each lane taking consecutive bitmap words.
+// writes its positions, each lane taking consecutive bitmap words.  A batch
+// of files shares one tile numbering; each file's newlines count from its
+// first tile.
 #include <cstdint>
 
 #include "index_kernel.h"
@@ -46,32 +48,52 @@ __global__ void __launch_bounds__(kScanThreads) newline_offsets_kernel(const int
     if (tid == 0) offsets[ntiles + blockIdx.x] = all;
 }
 
-// A warp per tile: the sum of the earlier blocks (lanes add them up), the
-// tile's offset in its block, then the positions, each lane taking
-// consecutive bitmap words.
-__global__ void __launch_bounds__(256) newline_scatter_kernel(const uint64_t* bits, int64_t words,
-                                                              const int32_t* counts, const int64_t* offsets,
-                                                              int64_t ntiles, int64_t* newlines, int64_t cap,
-                                                              unsigned long long* status) {
+// Sum of the tile counts before tile t of the whole batch (all lanes of a
+// warp call it; the block sums are added up by the lanes).
+__device__ __forceinline__ int64_t tiles_before(const int64_t* offsets, int64_t ntiles, int64_t t) {
+    const int lane = threadIdx.x & 31;
+    const int64_t* block_sums = offsets + ntiles;
+    const int64_t blk = t / kScanThreads;
+    int64_t base = 0;
+    for (int64_t b = lane; b < blk; b += 32) base += block_sums[b];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) base += __shfl_xor_sync(~0u, base, off);
+    return base + offsets[t];
+}
+
+// A warp per tile: the tile's newlines before it in its file (the batch
+// prefix at the tile minus the prefix at the file's first tile), then the
+// positions, each lane taking consecutive bitmap words.  `files` null: the
+// single file `one`.
+__global__ void __launch_bounds__(256) newline_scatter_kernel(const int32_t* counts, const int64_t* offsets,
+                                                              int64_t ntiles, LineFile one, const LineFile* files,
+                                                              int nfiles) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-    const int64_t* block_sums = offsets + ntiles;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && cap > 0) newlines[0] = 0;
     for (int64_t t = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); t < ntiles;
          t += warps) {
-        const int64_t blk = t / kScanThreads;
-        int64_t base = 0;
-        for (int64_t b = lane; b < blk; b += 32) base += block_sums[b];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) base += __shfl_xor_sync(~0u, base, off);
-        base += offsets[t];
-        if (t == ntiles - 1 && lane == 0) status[0] = static_cast<unsigned long long>(base + counts[t] + 1);
-        const int64_t w0 = t * kTileWordsL + lane * kWordsPerLane;
+        LineFile F = one;
+        if (files) {
+            int lo = 0, hi = nfiles - 1;  // last file with tile_begin <= t
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (files[mid].tile_begin <= t)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            F = files[lo];
+        }
+        const int64_t lt = t - F.tile_begin;
+        const int64_t base = tiles_before(offsets, ntiles, t) - tiles_before(offsets, ntiles, F.tile_begin);
+        if (lt == 0 && lane == 0 && F.cap > 0) F.newlines[0] = 0;
+        if (lt == F.ntiles - 1 && lane == 0) F.status[0] = static_cast<unsigned long long>(base + counts[t] + 1);
+        const int64_t w0 = lt * kTileWordsL + lane * kWordsPerLane;
         uint64_t m[kWordsPerLane];
         int cnt = 0;
 #pragma unroll
         for (int i = 0; i < kWordsPerLane; i++) {
-            m[i] = w0 + i < words ? bits[w0 + i] : 0ull;
+            m[i] = w0 + i < F.words ? F.newline_bits[w0 + i] : 0ull;
             cnt += popc64(m[i]);
         }
         int incl = cnt;
@@ -85,7 +107,7 @@ __global__ void __launch_bounds__(256) newline_scatter_kernel(const uint64_t* bi
         for (int i = 0; i < kWordsPerLane; i++) {
             uint64_t x = m[i];
             while (x) {
-                if (idx < cap) newlines[idx] = ((w0 + i) << 6) + ctz64(x);
+                if (idx < F.cap) F.newlines[idx] = ((w0 + i) << 6) + ctz64(x);
                 ++idx;
                 x &= x - 1;
             }
@@ -95,14 +117,25 @@ __global__ void __launch_bounds__(256) newline_scatter_kernel(const uint64_t* bi
 
 }  // namespace
 
+cudaError_t launch_newline_index_batch(const int32_t* tile_newlines, int64_t total_tiles, const LineFile* files,
+                                       int nfiles, int64_t* offsets, int grid, cudaStream_t stream) {
+    const int64_t blocks = (total_tiles + kScanThreads - 1) / kScanThreads;
+    newline_offsets_kernel<<<static_cast<unsigned>(blocks), kScanThreads, 0, stream>>>(tile_newlines, total_tiles,
+                                                                                       offsets);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    newline_scatter_kernel<<<grid, 256, 0, stream>>>(tile_newlines, offsets, total_tiles, LineFile{}, files, nfiles);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_newline_index(const IndexParams& p, int64_t* offsets, int grid, cudaStream_t stream) {
     const int64_t ntiles = (p.n + kLineTileBytes - 1) / kLineTileBytes;
     const int64_t blocks = (ntiles + kScanThreads - 1) / kScanThreads;
     newline_offsets_kernel<<<static_cast<unsigned>(blocks), kScanThreads, 0, stream>>>(p.tile_newlines, ntiles, offsets);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    newline_scatter_kernel<<<grid, 256, 0, stream>>>(p.newline_bits, p.level_size, p.tile_newlines, offsets, ntiles,
-                                                     p.newlines, p.newline_cap, p.status);
+    const LineFile one{p.newline_bits, p.level_size, p.newlines, p.newline_cap, p.status, 0, ntiles};
+    newline_scatter_kernel<<<grid, 256, 0, stream>>>(p.tile_newlines, offsets, ntiles, one, nullptr, 0);
     return cudaGetLastError();
 }
 

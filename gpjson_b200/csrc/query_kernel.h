@@ -26,4 +26,29 @@ struct QueryParams {
 cudaError_t launch_find_value(const QueryParams& p, int grid, cudaStream_t stream);
 int find_value_max_ctas_per_sm();
 
+// One file of a batched find_value launch: its index, its queries and where
+// their results go ([num_queries][out_lines][slots][2]); its lines are
+// [line_begin, line_begin + num_lines) of the batch's line numbering.
+struct QueryFile {
+    const uint8_t* file;
+    int64_t n;
+    const int64_t* newlines;
+    int64_t num_lines;
+    const uint64_t* string_index;
+    const uint64_t* leveled;
+    int64_t level_size;
+    const uint8_t* bytecode;
+    const int32_t* offsets;
+    int num_queries;
+    int slots;
+    int64_t* out;
+    int64_t out_lines;
+    int64_t line_begin;
+};
+
+// Every line of every file of the batch (`files`: device array, ascending
+// line_begin, total_lines lines in all) with its file's queries.
+cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_lines, int grid,
+                                    cudaStream_t stream);
+
 }  // namespace gpj

@@ -244,6 +244,32 @@ int gpj_result_slots(const gpj_result *r);
 const int64_t *gpj_result_offsets(const gpj_result *r);
 void gpj_result_release(gpj_result *r);
 
+/* ---- batches ---------------------------------------------------------------- */
+
+/* Many (file, paths) requests evaluated together, with no counterpart call in
+ * the reference (which handles one query() per call): gpj_batch_run indexes
+ * every file of the batch whose index is missing or too shallow in one
+ * kernel launch over all their tiles (plus one newline pass), evaluates every
+ * request's queries over every line of every file in one find_value launch,
+ * and copies all results back with one copy.  Files already indexed deeply
+ * enough keep their index (a resident corpus is indexed once).  Results of
+ * each request equal gpj_query_paths on its file alone.  Files must be of the
+ * batch's device and stay valid until gpj_batch_run returns. */
+typedef struct gpj_batch gpj_batch;
+int gpj_batch_create(gpj_ctx *ctx, gpj_batch **out);
+/* Adds a request; *item receives its number.  Paths are compiled here
+ * (GPJ_EPARSE / GPJ_EUNSUPPORTED as gpj_compile). */
+int gpj_batch_add(gpj_batch *batch, gpj_file *file, int nq, const char *const *paths, int *item);
+int gpj_batch_run(gpj_batch *batch);
+/* Results of request `item` of the last run (gpj_result layout, its queries
+ * in the order added; slots = the largest num_results among the queries of
+ * the request's file in this batch). */
+int gpj_batch_result(gpj_batch *batch, int item, gpj_result **out);
+int gpj_batch_size(const gpj_batch *batch);
+/* Removes all requests (the batch can be filled and run again). */
+void gpj_batch_clear(gpj_batch *batch);
+void gpj_batch_release(gpj_batch *batch);
+
 /* ---- diagnostics ---------------------------------------------------------- */
 
 /* Phase timings of the context as JSON (the role of Timings.export,
