@@ -52,6 +52,12 @@ def parse_args(argv=None):
                     help="default: gpj_index_query_device as shipped (index kernel, then one find_value "
                          "launch for all queries); fused: the queries evaluated inside the index kernel; "
                          "index: index only (diagnostic)")
+    ap.add_argument("--workload", choices=["tweets", "batched", "serving"], default="tweets",
+                    help="tweets: the 2 GiB single-file headline; batched: 512 files of 4 KiB-64 MiB, 1-8 "
+                         "queries each, one batch vs per-file calls; serving: 64 resident corpora, Poisson "
+                         "requests, continuous batching vs per-request")
+    ap.add_argument("--requests", type=int, default=20000, help="serving: number of requests")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serving: arrivals per second")
     return ap.parse_args(argv)
 
 
@@ -453,11 +459,164 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         print(json.dumps(result), flush=True)
 
 
+def batched_corpus(seed: int = 0x67706A73 + 3, files: int = 512):
+    """512 file sizes, lognormal clipped to 4 KiB-64 MiB (about 6 GiB in all),
+    three in four from the tweet-like generator, the rest adversarial; 1-8
+    queries per file from the 32-path pool."""
+    import numpy as np
+
+    from gpjson_b200 import serve
+
+    rng = np.random.default_rng(seed)
+    sizes = np.clip(rng.lognormal(mean=15.6, sigma=1.4, size=files), 4 << 10, 64 << 20).astype(np.int64)
+    kinds = rng.random(files) < 0.75
+    paths = [[serve.PATH_POOL[i] for i in rng.choice(32, size=int(rng.integers(1, 9)), replace=False)]
+             for _ in range(files)]
+    return sizes, kinds, paths
+
+
+def run_batched(args) -> None:
+    """Batched workload: every step indexes all 512 files and evaluates their
+    queries, once as one gpj_batch_run, once as 512 gpj_query_paths calls."""
+    import torch
+
+    import gpjson_b200 as gj
+    from gpjson_b200 import datagen
+
+    sizes, kinds, paths = batched_corpus()
+    total = int(sizes.sum())
+    dev = []
+    for i, (n, tweet) in enumerate(zip(sizes, kinds)):
+        seed = datagen.SEED_BASE + 1000 + i
+        host = datagen.tweets(int(n), seed=seed) if tweet else datagen.adversarial(int(n), seed=seed)
+        dev.append(torch.from_numpy(host).to("cuda"))
+    torch.cuda.synchronize()
+    g = gj.GPJSON(0)
+    nq = sum(len(p) for p in paths)
+
+    def fresh_files():  # unindexed views of the resident inputs
+        return [g.from_device(t.data_ptr(), t.numel(), keepalive=t) for t in dev]
+
+    def batched_step():
+        fs = fresh_files()
+        b = g.batch()
+        for f, p in zip(fs, paths):
+            b.add(f, p)
+        t0 = time.perf_counter()
+        b.run()
+        dt = time.perf_counter() - t0
+        b.release()
+        for f in fs:
+            f.release()
+        return dt
+
+    def per_file_step():
+        fs = fresh_files()
+        t0 = time.perf_counter()
+        for f, p in zip(fs, paths):
+            f.query_paths(p)
+        dt = time.perf_counter() - t0
+        for f in fs:
+            f.release()
+        return dt
+
+    for _ in range(args.warmup):
+        batched_step()
+        per_file_step()
+    tb = [batched_step() for _ in range(args.steps)]
+    tp = [per_file_step() for _ in range(max(1, min(args.steps, 3)))]
+    mb, mp = statistics.mean(tb), statistics.mean(tp)
+    line = {
+        "metric": "queries/s (batched index+query)",
+        "value": round(nq / mb, 1),
+        "unit": "queries/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(1000 * mb, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": {"workload": f"{len(sizes)} NDJSON files of 4 KiB-64 MiB ({total} B), 3/4 tweet-like, 1/4 "
+                               f"adversarial; {nq} queries, 1-8 per file from a 32-path pool; each step indexes "
+                               "every file and evaluates its queries, results copied to the host",
+                   "files": len(sizes), "bytes": total, "queries": nq},
+        "input_gbs": round(total / mb / 1e9, 2),
+        "per_file_calls": {"ms_per_step": round(1000 * mp, 3), "queries_per_s": round(nq / mp, 1),
+                           "input_gbs": round(total / mp / 1e9, 2)},
+        "batched_vs_per_file": round(mp / mb, 2),
+    }
+    g.close()
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args) -> None:
+    """Serving workload: 64 corpora of 1 MiB-1 GiB (log-uniform), requests
+    arriving Poisson with Zipf(1.1) corpus popularity, a 120 GiB budget;
+    continuous batching, then the per-request form on a saturated sample."""
+    import numpy as np
+
+    from gpjson_b200 import datagen, serve
+
+    rng = np.random.default_rng(0x67706A73 + 4)
+    sizes = np.exp(rng.uniform(np.log(1 << 20), np.log(1 << 30), size=64)).astype(np.int64)
+    corpora = {}
+    for i, n in enumerate(sizes):
+        seed = datagen.SEED_BASE + 2000 + i
+        corpora[f"c{i:02d}"] = datagen.tweets(int(n), seed=seed) if i % 4 else datagen.adversarial(int(n), seed=seed)
+    names = list(corpora)
+    total = int(sizes.sum())
+    srv = serve.Server(corpora, budget_bytes=120 << 30)
+    try:
+        reqs = serve.poisson_requests(names, args.requests, rate=args.rate)
+        live = srv.serve(reqs).summary()  # cold start included: corpora load on first request
+        sample = serve.poisson_requests(names, 2000, rate=1e9, seed=11)  # all at once: saturated
+        batched = srv.serve(sample).summary()
+        solo_sample = [serve.Request(0.0, r.corpus, list(r.paths)) for r in sample[:500]]
+        solo = srv.serve(solo_sample, per_request=True).summary()
+    finally:
+        srv.close()
+    line = {
+        "metric": "served queries/s (p50/p99 latency)",
+        "value": live["queries_per_s"],
+        "unit": "queries/s",
+        "n_gpus": 1,
+        "steps": 1,
+        "warmup": 0,
+        "ms_per_step": round(1000 * live["seconds"], 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "u8",
+        "data": "synthetic",
+        "config": {"workload": f"64 corpora of 1 MiB-1 GiB log-uniform ({total} B), {args.requests} requests "
+                               f"Poisson at {args.rate:.0f}/s, Zipf 1.1 popularity, 1 path each from a 32-path "
+                               "pool, 120 GiB resident budget, continuous batching",
+                   "corpora": 64, "bytes": total},
+        "latency_ms": {"p50": live["p50_ms"], "p99": live["p99_ms"], "mean": live["mean_ms"]},
+        "live": live,
+        "saturated_batched": batched,
+        "saturated_per_request": solo,
+        "batched_vs_per_request_qps": round(batched["queries_per_s"] / max(solo["queries_per_s"], 1e-9), 2),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main(argv=None) -> None:
     args = parse_args(argv)
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "batched":
+        if rank == 0:
+            run_batched(args)
+        return
+    if args.workload == "serving":
+        if rank == 0:
+            run_serving(args)
         return
     run_ours(args, rank, world, local)
 

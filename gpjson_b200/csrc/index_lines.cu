@@ -299,6 +299,9 @@ __device__ __forceinline__ RSpan index_scan_rspan(RSpan mine, RSpan* scratch, RS
 __device__ __forceinline__ void load_slot(const uint8_t* file, int64_t start, int64_t bytes, uint8_t* dst,
                                           uint64_t* bar) {
     const uint32_t bulk = static_cast<uint32_t>(bytes & ~static_cast<int64_t>(15));
+    // the last bytes of a file that do not fill 16 go by plain copies, before
+    // the arrive, so the threads waiting on `bar` see them too
+    for (int64_t i = bulk; i < bytes; i++) dst[i] = file[start + i];
     fence_proxy_async_smem();
     if (bulk > 0) {
         mbar_arrive_expect_tx(bar, bulk);
@@ -306,7 +309,6 @@ __device__ __forceinline__ void load_slot(const uint8_t* file, int64_t start, in
     } else {
         mbar_arrive(bar);
     }
-    for (int64_t i = bulk; i < bytes; i++) dst[i] = file[start + i];
 }
 
 // Loads and classifies the 64-byte word at global position `pos` straight
@@ -609,6 +611,8 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                     uint32_t ccin;
                     if ((tid & 31) > 0 && !prev_all) {
                         ccin = static_cast<uint32_t>(prev_par);
+                    } else if (!cvalid) {
+                        ccin = 0;  // a word past the line's end: never scan bytes past the file
                     } else {
                         int run = 0;
                         int64_t j = cw - 1;
