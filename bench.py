@@ -497,15 +497,17 @@ def run_batched(args) -> None:
     def fresh_files():  # unindexed views of the resident inputs
         return [g.from_device(t.data_ptr(), t.numel(), keepalive=t) for t in dev]
 
+    b = g.batch()  # reused: its page-locked result buffer is allocated once
+
     def batched_step():
         fs = fresh_files()
-        b = g.batch()
+        b.clear()
         for f, p in zip(fs, paths):
             b.add(f, p)
         t0 = time.perf_counter()
         b.run()
         dt = time.perf_counter() - t0
-        b.release()
+        b.clear()
         for f in fs:
             f.release()
         return dt
@@ -548,6 +550,7 @@ def run_batched(args) -> None:
                            "input_gbs": round(total / mp / 1e9, 2)},
         "batched_vs_per_file": round(mp / mb, 2),
     }
+    b.release()
     g.close()
     print(json.dumps(line), flush=True)
 
@@ -570,11 +573,18 @@ def run_serving(args) -> None:
     total = int(sizes.sum())
     srv = serve.Server(corpora, budget_bytes=120 << 30)
     try:
+        # cold: corpora load when first requested; then the same arrival
+        # process again with every corpus resident (steady state)
+        cold = srv.serve(serve.poisson_requests(names, args.requests, rate=args.rate, seed=21)).summary()
         reqs = serve.poisson_requests(names, args.requests, rate=args.rate)
-        live = srv.serve(reqs).summary()  # cold start included: corpora load on first request
-        sample = serve.poisson_requests(names, 2000, rate=1e9, seed=11)  # all at once: saturated
+        live = srv.serve(reqs).summary()
+        # saturated: every request available at once; each form runs once
+        # untimed first (result buffers grown, all corpora resident)
+        sample = serve.poisson_requests(names, 2000, rate=1e9, seed=11)
+        srv.serve([serve.Request(0.0, r.corpus, list(r.paths)) for r in sample])
         batched = srv.serve(sample).summary()
         solo_sample = [serve.Request(0.0, r.corpus, list(r.paths)) for r in sample[:500]]
+        srv.serve([serve.Request(0.0, r.corpus, list(r.paths)) for r in solo_sample], per_request=True)
         solo = srv.serve(solo_sample, per_request=True).summary()
     finally:
         srv.close()
@@ -593,10 +603,12 @@ def run_serving(args) -> None:
         "data": "synthetic",
         "config": {"workload": f"64 corpora of 1 MiB-1 GiB log-uniform ({total} B), {args.requests} requests "
                                f"Poisson at {args.rate:.0f}/s, Zipf 1.1 popularity, 1 path each from a 32-path "
-                               "pool, 120 GiB resident budget, continuous batching",
+                               "pool, 120 GiB resident budget, continuous batching (at most 512 requests per "
+                               "batch); value and latency with the corpora resident",
                    "corpora": 64, "bytes": total},
         "latency_ms": {"p50": live["p50_ms"], "p99": live["p99_ms"], "mean": live["mean_ms"]},
         "live": live,
+        "cold_start": cold,
         "saturated_batched": batched,
         "saturated_per_request": solo,
         "batched_vs_per_request_qps": round(batched["queries_per_s"] / max(solo["queries_per_s"], 1e-9), 2),

@@ -117,8 +117,14 @@ struct gpj_batch {
     };
     std::vector<Item> items;
     std::vector<FileRun> files;
-    std::vector<int64_t> results;
+    // results of the last run, page-locked (one copy from the device at full
+    // speed), kept and grown across runs
+    int64_t* results = nullptr;
+    size_t results_cap = 0;  // elements
     bool ran = false;
+    ~gpj_batch() {
+        if (results) cudaFreeHost(results);
+    }
 };
 
 namespace {
@@ -1382,7 +1388,6 @@ int gpj_batch_run(gpj_batch* b) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     b->files.clear();
-    b->results.clear();
     b->ran = false;
     for (auto& it : b->items) {
         int slot = -1;
@@ -1411,7 +1416,7 @@ int gpj_batch_run(gpj_batch* b) {
     std::vector<uint8_t> blob;  // per file: [int32 offsets (16-byte padded)][bytecode]
     std::vector<size_t> blob_at(b->files.size());
     size_t total_out = 0;
-    int64_t total_lines = 0;
+    int64_t total_items = 0;
     for (size_t i = 0; i < b->files.size(); i++) {
         auto& fr = b->files[i];
         const size_t nq = fr.queries.size();
@@ -1429,7 +1434,7 @@ int gpj_batch_run(gpj_batch* b) {
         fr.lines = fr.file->num_lines;
         fr.out_offset = total_out;
         total_out += nq * static_cast<size_t>(fr.lines) * fr.slots * 2;
-        total_lines += fr.lines;
+        total_items += static_cast<int64_t>(nq) * fr.lines;
     }
     uint8_t* d_blob = nullptr;
     int64_t* d_out = nullptr;
@@ -1439,7 +1444,7 @@ int gpj_batch_run(gpj_batch* b) {
     if (!rc) rc = device_alloc(ctx, &d_qf, b->files.size(), "cudaMalloc(batch query files)");
     if (!rc) {
         std::vector<gpj::QueryFile> qf;
-        int64_t line = 0;
+        int64_t item = 0;
         for (size_t i = 0; i < b->files.size(); i++) {
             auto& fr = b->files[i];
             gpj_file* f = fr.file;
@@ -1448,27 +1453,34 @@ int gpj_batch_run(gpj_batch* b) {
             qf.push_back(gpj::QueryFile{f->d_data, f->n, f->d_nl, fr.lines, f->d_str, f->d_lvl, f->words,
                                         d_blob + blob_at[i] + header,
                                         reinterpret_cast<const int32_t*>(d_blob + blob_at[i]),
-                                        static_cast<int>(nq), fr.slots, d_out + fr.out_offset, fr.lines, line});
-            line += fr.lines;
+                                        static_cast<int>(nq), fr.slots, d_out + fr.out_offset, fr.lines, item});
+            item += static_cast<int64_t>(nq) * fr.lines;
         }
         cudaError_t e = cudaMemcpyAsync(d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(d_qf, qf.data(), sizeof(gpj::QueryFile) * qf.size(), cudaMemcpyHostToDevice,
                                 ctx->stream);
-        if (e == cudaSuccess && total_lines > 0) {
+        if (e == cudaSuccess && total_items > 0) {
             const int64_t grid =
-                std::max<int64_t>(1, std::min<int64_t>((total_lines + 255) / 256, static_cast<int64_t>(ctx->sms) * 8));
-            e = gpj::launch_find_value_batch(d_qf, static_cast<int>(qf.size()), total_lines, static_cast<int>(grid),
+                std::max<int64_t>(1, std::min<int64_t>((total_items + 255) / 256, static_cast<int64_t>(ctx->sms) * 8));
+            e = gpj::launch_find_value_batch(d_qf, static_cast<int>(qf.size()), total_items, static_cast<int>(grid),
                                              ctx->stream);
             ctx->launches++;
         }
-        try {
-            b->results.resize(total_out);
-        } catch (const std::bad_alloc&) {
-            rc = fail(ctx, GPJ_ENOMEM, "out of host memory for results");
+        if (e == cudaSuccess && total_out > b->results_cap) {
+            // wait for the copy that may still read the old buffer, then grow (doubling)
+            const size_t cap = std::max(total_out, 2 * b->results_cap);
+            e = cudaStreamSynchronize(ctx->stream);
+            if (e == cudaSuccess && b->results) cudaFreeHost(b->results);
+            b->results = nullptr;
+            b->results_cap = 0;
+            if (e == cudaSuccess) {
+                e = cudaMallocHost(&b->results, cap * 8);
+                if (e == cudaSuccess) b->results_cap = cap;
+            }
         }
-        if (!rc && e == cudaSuccess && total_out > 0)
-            e = cudaMemcpyAsync(b->results.data(), d_out, total_out * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess && total_out > 0)
+            e = cudaMemcpyAsync(b->results, d_out, total_out * 8, cudaMemcpyDeviceToHost, ctx->stream);
         if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "batch query");
     }
@@ -1495,7 +1507,7 @@ int gpj_batch_result(gpj_batch* b, int item, gpj_result** out) {
     r->lines = fr.lines;
     r->slots = fr.slots;
     const size_t per_query = static_cast<size_t>(fr.lines) * fr.slots * 2;
-    const int64_t* src = b->results.data() + fr.out_offset + it.q0 * per_query;
+    const int64_t* src = b->results + fr.out_offset + it.q0 * per_query;
     try {
         r->offsets.assign(src, src + r->nq * per_query);
     } catch (const std::bad_alloc&) {
@@ -1512,7 +1524,6 @@ void gpj_batch_clear(gpj_batch* b) {
     if (!b) return;
     b->items.clear();
     b->files.clear();
-    b->results.clear();
     b->ran = false;
 }
 

@@ -44,20 +44,46 @@ enum LineStatus : int { kLineDone = 0, kLineDeferred = 1 };
 
 GPJ_HD bool is_ws(uint8_t c) { return c == '\n' || c == '\r' || c == '\t' || c == ' '; }
 
-// First set bit of `bm` at a position in [from, limit), or `limit`.
+// First set bit of `bm` at a position in [from, limit), or `limit`.  After
+// the first three words, four words are loaded per step (independent loads,
+// so a long jump waits for a quarter of the dependent memory round trips);
+// only words holding positions below `limit` are read.
+GPJ_HD int64_t first_of4(int64_t w, uint64_t a, uint64_t b, uint64_t c, uint64_t d, int64_t limit) {
+    int64_t base = w;
+    uint64_t x = a;
+    if (!a) {
+        base = b ? w + 1 : (c ? w + 2 : w + 3);
+        x = b ? b : (c ? c : d);
+    }
+    const int64_t p = (base << 6) + ctz64(x);
+    return p < limit ? p : limit;
+}
+
 GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit) {
     if (from >= limit) return limit;
     int64_t w = from >> 6;
-    uint64_t m = bm[w] & (~0ull << (from & 63));
-    for (;;) {
-        if (m) {
-            const int64_t p = (w << 6) + ctz64(m);
+    const int64_t wend = ((limit - 1) >> 6) + 1;
+    const uint64_t m = bm[w] & (~0ull << (from & 63));
+    if (m) {
+        const int64_t p = (w << 6) + ctz64(m);
+        return p < limit ? p : limit;
+    }
+    // the next two words one at a time (most jumps end there), then four per step
+    for (++w; w < wend && w < (from >> 6) + 3; ++w) {
+        const uint64_t x = bm[w];
+        if (x) {
+            const int64_t p = (w << 6) + ctz64(x);
             return p < limit ? p : limit;
         }
-        ++w;
-        if ((w << 6) >= limit) return limit;
-        m = bm[w];
     }
+    for (; w < wend; w += 4) {
+        const uint64_t a = bm[w];
+        const uint64_t b = w + 1 < wend ? bm[w + 1] : 0;
+        const uint64_t c = w + 2 < wend ? bm[w + 2] : 0;
+        const uint64_t d = w + 3 < wend ? bm[w + 3] : 0;
+        if (a | b | c | d) return first_of4(w, a, b, c, d, limit);
+    }
+    return limit;
 }
 
 // First position in [from, limit) set in bm and (in `filt`, or not in it
@@ -66,16 +92,28 @@ GPJ_HD int64_t next_bit_filtered(const uint64_t* bm, const uint64_t* filt, bool 
                                  int64_t limit) {
     if (from >= limit) return limit;
     int64_t w = from >> 6;
-    uint64_t m = bm[w] & (invert ? ~filt[w] : filt[w]) & (~0ull << (from & 63));
-    for (;;) {
-        if (m) {
-            const int64_t p = (w << 6) + ctz64(m);
+    const int64_t wend = ((limit - 1) >> 6) + 1;
+    const uint64_t flip = invert ? ~0ull : 0ull;
+    const uint64_t m = bm[w] & (filt[w] ^ flip) & (~0ull << (from & 63));
+    if (m) {
+        const int64_t p = (w << 6) + ctz64(m);
+        return p < limit ? p : limit;
+    }
+    for (++w; w < wend && w < (from >> 6) + 3; ++w) {
+        const uint64_t x = bm[w] & (filt[w] ^ flip);
+        if (x) {
+            const int64_t p = (w << 6) + ctz64(x);
             return p < limit ? p : limit;
         }
-        ++w;
-        if ((w << 6) >= limit) return limit;
-        m = bm[w] & (invert ? ~filt[w] : filt[w]);
     }
+    for (; w < wend; w += 4) {
+        const uint64_t a = bm[w] & (filt[w] ^ flip);
+        const uint64_t b = w + 1 < wend ? bm[w + 1] & (filt[w + 1] ^ flip) : 0;
+        const uint64_t c = w + 2 < wend ? bm[w + 2] & (filt[w + 2] ^ flip) : 0;
+        const uint64_t d = w + 3 < wend ? bm[w + 3] & (filt[w + 3] ^ flip) : 0;
+        if (a | b | c | d) return first_of4(w, a, b, c, d, limit);
+    }
+    return limit;
 }
 
 // Last set bit of `bm` at a position in (floor, from], or -1.

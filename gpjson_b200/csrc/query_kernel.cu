@@ -35,36 +35,36 @@ __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
 }
 
 __global__ void __launch_bounds__(256) find_value_batch_kernel(const QueryFile* files, int nfiles,
-                                                                int64_t total_lines) {
+                                                                int64_t total_items) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < total_lines; g += stride) {
-        int lo = 0, hi = nfiles - 1;  // last file with line_begin <= g
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < total_items; g += stride) {
+        int lo = 0, hi = nfiles - 1;  // last file with item_begin <= g
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (files[mid].line_begin <= g)
+            if (files[mid].item_begin <= g)
                 lo = mid;
             else
                 hi = mid - 1;
         }
         const QueryFile& F = files[lo];
-        const int64_t i = g - F.line_begin;
+        const int64_t k = g - F.item_begin;
+        const int64_t q = k / F.num_lines;
+        const int64_t i = k - q * F.num_lines;
         LineView view{F.file, F.n, F.string_index, F.leveled, F.level_size, F.n, nullptr};
         const int64_t start = F.newlines[i];
         const int64_t end = i + 1 < F.num_lines ? F.newlines[i + 1] : F.n;
         const int64_t per_line = 2 * static_cast<int64_t>(F.slots);
-        for (int q = 0; q < F.num_queries; q++) {
-            int64_t* res = F.out + (static_cast<int64_t>(q) * F.out_lines + i) * per_line;
-            for (int64_t k = 0; k < per_line; k++) res[k] = -1;
-            run_line(view, start, end, F.bytecode + F.offsets[q], res);
-        }
+        int64_t* res = F.out + (q * F.out_lines + i) * per_line;
+        for (int64_t r = 0; r < per_line; r++) res[r] = -1;
+        run_line(view, start, end, F.bytecode + F.offsets[q], res);
     }
 }
 
 }  // namespace
 
-cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_lines, int grid,
+cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_items, int grid,
                                     cudaStream_t stream) {
-    find_value_batch_kernel<<<grid, 256, 0, stream>>>(files, nfiles, total_lines);
+    find_value_batch_kernel<<<grid, 256, 0, stream>>>(files, nfiles, total_items);
     return cudaGetLastError();
 }
 

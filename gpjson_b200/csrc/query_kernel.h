@@ -43,12 +43,13 @@ struct QueryFile {
     int slots;
     int64_t* out;
     int64_t out_lines;
-    int64_t line_begin;
+    int64_t item_begin;  // first of the file's num_lines x num_queries (line, query) items in the batch
 };
 
-// Every line of every file of the batch (`files`: device array, ascending
-// line_begin, total_lines lines in all) with its file's queries.
-cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_lines, int grid,
+// Every (line, query) item of every file of the batch (`files`: device
+// array, ascending item_begin, total_items items in all), one per thread,
+// query-major within a file so a warp's lanes run the same query.
+cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_items, int grid,
                                     cudaStream_t stream);
 
 }  // namespace gpj
