@@ -338,15 +338,17 @@ __device__ __forceinline__ ClassMasks classify_global(const uint8_t* file, int64
 
 // Final masks of one word: checks the '\n' bits in `check`, keeps the word
 // in mask slot `ms` at `slot` (>= 0) and writes it to the global index when
-// `owned`.
+// `owned`; a word that is not `active` does nothing.  Called at one place
+// by every lane of a warp, so the level split's loop over bracket cuts runs
+// once per warp (its trip count is the largest of the lanes').
 template <int LV, bool kMasks, class Sh>
 __device__ __forceinline__ void finish_word(const IndexParams& p, const TileFile& F, Sh& sh, int ms,
                                             const ClassMasks& m,
                                             uint64_t p0, int s_w, int64_t d_w, int64_t word, bool owned, int slot,
-                                            uint64_t valid, uint64_t check) {
+                                            uint64_t valid, uint64_t check, bool active) {
     const uint64_t in_str = (p0 ^ (s_w ? ~0ull : 0ull)) & valid;
     const uint64_t open = m.open & ~in_str, close = m.close & ~in_str;
-    if (check) {
+    if (active && check) {
         // every checked '\n' must be outside strings at level -1
         if (check & in_str) atomicOr(F.status + 1, kErrIrregular);
         uint64_t c = check;
@@ -358,9 +360,11 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, const TileFile
             c &= c - 1;
         }
     }
-    if (!owned && slot < 0) return;
+    const bool split = active && (owned || slot >= 0);
+    const uint64_t keep = split ? ~0ull : 0ull;
     uint64_t lv[LV];
-    split_levels<LV>(open, close, m.structural & ~in_str, d_w, lv);
+    split_levels<LV>(open & keep, close & keep, m.structural & ~in_str & keep, d_w, lv);
+    if (!split) return;
     if constexpr (kMasks) {
         if (slot >= 0) {
             sh.str[ms][slot] = in_str;
@@ -534,6 +538,13 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
         } else {
             if (tid == 0) p.tile_newlines[t] = tile_nl;
         }
+        // What this CTA finishes of the word, from which state; the branches
+        // only choose it, so that finish_word runs converged below.
+        bool act = false, own = true;
+        ClassMasks wm = m;
+        uint64_t wp0 = p0, check = 0;
+        int ws_in = ex.rq & 1;
+        int64_t wd_in = ex.d0;
         if (!ahead) {
             if constexpr (kLines) {
                 const int excl = ex.nl & 0xFFFF;
@@ -550,24 +561,28 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
             }
             if (ex.rq & 2) {
                 // every byte of the word belongs to lines that start in this tile
-                if (ws < tile_end)
-                    finish_word<LV, kLines>(p, F, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, slot, valid, m.newline);
+                act = ws < tile_end;
+                check = m.newline;
             } else if (has_nl) {
                 // the tile's first line starts at byte f of this word
                 sh.first_line = ws + f;
-                ClassMasks mm = m;
-                restrict_masks(mm, after);
-                finish_word<LV, kLines>(p, F, sh, ms, mm, pa, 0, -1, ws >> 6, f == 0, slot, valid, m.newline & after);
+                restrict_masks(wm, after);
+                act = true;
+                own = f == 0;
+                wp0 = pa;
+                ws_in = 0;
+                wd_in = -1;
+                check = m.newline & after;
             }
         } else if (lines_here && (ex.nl >> 16) == 0 && valid) {
             // No '\n' between the tile end and this word: the tile's last line
             // runs into it.  The line ends at this word's first '\n' (the only
             // one checked here); a word that starts with it belongs to the next tile.
             if (has_nl) sh.ext_b = ws + f;
-            if (!(has_nl && f == 0))
-                finish_word<LV, kLines>(p, F, sh, ms, m, p0, ex.rq & 1, ex.d0, ws >> 6, true, slot, valid,
-                                has_nl ? (1ull << f) : 0ull);
+            act = !(has_nl && f == 0);
+            check = has_nl ? (1ull << f) : 0ull;
         }
+        finish_word<LV, kLines>(p, F, sh, ms, wm, wp0, ws_in, wd_in, ws >> 6, own, slot, valid, check, act);
         group_sync(kBarIndex, kIndexThreads);  // the tile's masks are complete in the slot
 
         const int64_t a_t = lt == 0 ? 0 : (lines_here ? sh.first_line : kNone);
@@ -632,9 +647,8 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                     const Span cex = index_scan_span(csp, sh.span_scratch, &ctotal);
                     const uint64_t ccheck =
                         (b_t >= cw && b_t < cw + 64) ? (c.newline & (1ull << (b_t - cw))) : 0ull;
-                    if (cvalid)
-                        finish_word<LV, kLines>(p, F, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
-                                        cw >> 6, true, -1, cvalid, ccheck);
+                    finish_word<LV, kLines>(p, F, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
+                                            cw >> 6, true, -1, cvalid, ccheck, cvalid != 0);
                     if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(ccout);
                     group_sync(kBarIndex, kIndexThreads);
                     esc = sh.carry_esc;

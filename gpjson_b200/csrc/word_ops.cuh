@@ -219,45 +219,40 @@ GPJ_HD Span span_compose(const Span& a, const Span& b) {
 // an opening bracket increments the counter and is marked at the new level,
 // a closing bracket is marked at the current level and then decrements it,
 // ':' and ',' are marked at the current level.  Levels outside
-// [0, num_levels) are not marked.  The word is cut into segments of constant
-// level at each bracket; levels are kept in LV registers.
+// [0, num_levels) are not marked.
+//
+// The word is cut into segments of constant level: an opening bracket at
+// byte x starts a segment at x, a closing bracket at byte x ends one after
+// x, so the cuts are `open | close << 1` and crossing the cut at x changes
+// the level by open[x] - close[x-1] (a '}' directly followed by '{' cuts
+// once with no change).  Every cut costs the same straight-line work, so
+// the lanes of a warp stay converged whatever brackets their words hold.
+// A word changes the level by at most 64, so the level is carried in 32
+// bits with `depth` clamped to +-128: a clamped start is out of range for
+// every byte exactly when the true one is.  Returns the level after the word.
 template <int LV>
 GPJ_HD int64_t split_levels(uint64_t open, uint64_t close, uint64_t structural, int64_t depth,
                             uint64_t (&lv)[LV]) {
 #pragma unroll
     for (int k = 0; k < LV; k++) lv[k] = 0;
-    uint64_t events = open | close;
+    const uint64_t close_after = close << 1;
+    uint64_t cuts = open | close_after;
     uint64_t rest = structural;
-    int64_t d = depth;
-    while (events) {
-        const int p = ctz64(events);
-        const uint64_t bit = 1ull << p;
-        uint64_t seg;
-        if (open & bit) {
-            seg = rest & (bit - 1);          // bytes before the bracket
-            rest &= ~(bit - 1);
-            if (d >= 0 && d < LV) {
+    int d = depth > 128 ? 128 : (depth < -128 ? -128 : static_cast<int>(depth));
+    while (cuts) {
+        const uint64_t cut = cuts & (~cuts + 1);  // lowest cut
+        const uint64_t seg = rest & (cut - 1);    // the bytes before it
+        rest ^= seg;
 #pragma unroll
-                for (int k = 0; k < LV; k++) lv[k] |= (d == k) ? seg : 0;
-            }
-            d++;
-        } else {
-            const uint64_t upto = (p == 63) ? ~0ull : ((bit << 1) - 1);
-            seg = rest & upto;               // bytes up to and including it
-            rest &= ~upto;
-            if (d >= 0 && d < LV) {
-#pragma unroll
-                for (int k = 0; k < LV; k++) lv[k] |= (d == k) ? seg : 0;
-            }
-            d--;
-        }
-        events &= events - 1;
+        for (int k = 0; k < LV; k++)
+            if (d == k) lv[k] |= seg;
+        d += ((open & cut) ? 1 : 0) - ((close_after & cut) ? 1 : 0);
+        cuts ^= cut;
     }
-    if (d >= 0 && d < LV) {
 #pragma unroll
-        for (int k = 0; k < LV; k++) lv[k] |= (d == k) ? rest : 0;
-    }
-    return d;
+    for (int k = 0; k < LV; k++)
+        if (d == k) lv[k] |= rest;
+    return depth + popc64(open) - popc64(close);
 }
 
 }  // namespace gpj
