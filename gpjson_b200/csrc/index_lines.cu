@@ -220,6 +220,7 @@ struct FShared {
     uint8_t ir[kIrBytes];
     int32_t ir_off[kIrQueries];
     SlotInfo info[kMaskSlots];
+    uint64_t lvacc[kTileWarps][LV][32];  // level split of each index warp (split_levels_warp)
     uint64_t full[kRing];   // TMA landed
     uint64_t bfree[kRing];  // line warps done with the bytes
     uint64_t mready[kMaskSlots];
@@ -234,9 +235,11 @@ struct FShared {
 };
 
 // Shared memory of the standalone index kernel (no line warps, no queries).
+template <int LV>
 struct TShared {
     uint8_t bytes[kRing][kSlotBytes];
     TileFile desc[kRing];
+    uint64_t lvacc[kTileWarps][LV][32];
     uint64_t full[kRing];
     Span span_scratch[kTileWarps];
     RSpan rscan[2][kTileWarps];
@@ -336,6 +339,89 @@ __device__ __forceinline__ ClassMasks classify_global(const uint8_t* file, int64
     return classify64(v);
 }
 
+// Bits 0..x of a word (x in 0..63).
+__device__ __forceinline__ uint64_t bits_upto(int x) { return x >= 63 ? ~0ull : ((2ull << x) - 1); }
+
+// Position of the i-th (from 0) set bit of k, which has more than i set bits.
+__device__ __forceinline__ int select_bit(uint64_t k, int i) {
+    uint32_t w = static_cast<uint32_t>(k);
+    int pos = 0;
+    const int c32 = __popc(w);
+    if (i >= c32) {
+        w = static_cast<uint32_t>(k >> 32);
+        pos = 32;
+        i -= c32;
+    }
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        const int c = __popc(w & ((1u << s) - 1));
+        if (i >= c) {
+            w >>= s;
+            pos += s;
+            i -= c;
+        }
+    }
+    return pos;
+}
+
+// split_levels (word_ops.cuh) for the 32 words of a warp at once.  A word
+// is cut into segments of constant level at its bracket cuts (`open |
+// close << 1`).  Each word keeps its first segment itself; the segments
+// that start at a cut are dealt out over the lanes, one per lane per pass
+// (ceil(cuts of the warp / 32) passes), and OR-ed into the owning word's
+// level slots in `acc` (this warp's [LV][32] words of shared memory).
+// Bracket counts differ a lot between words (most have none, some ten or
+// more), so a per-word loop would run as long as the warp's densest word;
+// here the warp makes about one pass.  Called by all 32 lanes.
+template <int LV>
+__device__ __forceinline__ void split_levels_warp(uint64_t open, uint64_t close, uint64_t structural, int64_t depth,
+                                                  uint64_t (*acc)[32], uint64_t (&lv)[LV]) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t close_after = close << 1;
+    const uint64_t cuts = open | close_after;
+    // a word moves the level by at most 64: clamping keeps "out of range"
+    const int d = depth > 128 ? 128 : (depth < -128 ? -128 : static_cast<int>(depth));
+    const uint64_t first = cuts & (~cuts + 1);
+    const uint64_t seg0 = structural & (first - 1);  // all of it when there is no cut
+#pragma unroll
+    for (int k = 0; k < LV; k++) acc[k][lane] = d == k ? seg0 : 0ull;
+    const int m = popc64(cuts);
+    int incl = m;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int o = __shfl_up_sync(~0u, incl, off);
+        if (lane >= off) incl += o;
+    }
+    const int base = incl - m;
+    const int total = __shfl_sync(~0u, incl, 31);
+    __syncwarp();
+    for (int r = 0; r < total; r += 32) {
+        const int g = r + lane;  // this lane's cut, numbered across the warp
+        int o = 0;               // its word: the last lane whose first cut number is <= g
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1)
+            if (__shfl_sync(~0u, base, o + s) <= g) o += s;
+        const int i = g - __shfl_sync(~0u, base, o);
+        const uint64_t k = __shfl_sync(~0u, cuts, o);
+        const uint64_t op = __shfl_sync(~0u, open, o);
+        const uint64_t ca = __shfl_sync(~0u, close_after, o);
+        const uint64_t st = __shfl_sync(~0u, structural, o);
+        const int dd = __shfl_sync(~0u, d, o);
+        if (g < total) {
+            const int x = select_bit(k, i);
+            const uint64_t upto = bits_upto(x);
+            const uint64_t later = k & ~upto;
+            // bytes from the cut up to the next one (or the word end)
+            const uint64_t seg = st & ~(upto >> 1) & ((later & (~later + 1)) - 1);
+            const int level = dd + popc64(op & upto) - popc64(ca & upto);
+            if (seg && level >= 0 && level < LV) atomicOr(reinterpret_cast<unsigned long long*>(&acc[level][o]), static_cast<unsigned long long>(seg));
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < LV; k++) lv[k] = acc[k][lane];
+}
+
 // Final masks of one word: checks the '\n' bits in `check`, keeps the word
 // in mask slot `ms` at `slot` (>= 0) and writes it to the global index when
 // `owned`; a word that is not `active` does nothing.  Called at one place
@@ -363,7 +449,8 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, const TileFile
     const bool split = active && (owned || slot >= 0);
     const uint64_t keep = split ? ~0ull : 0ull;
     uint64_t lv[LV];
-    split_levels<LV>(open & keep, close & keep, m.structural & ~in_str & keep, d_w, lv);
+    split_levels_warp<LV>(open & keep, close & keep, m.structural & ~in_str & keep, d_w, sh.lvacc[threadIdx.x >> 5],
+                          lv);
     if (!split) return;
     if constexpr (kMasks) {
         if (slot >= 0) {
@@ -796,7 +883,7 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
 template <int LV>
 __global__ void __launch_bounds__(kIndexThreads, 3) tile_index_kernel(IndexParams p) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
-    TShared& sh = *reinterpret_cast<TShared*>(smem_raw);
+    TShared<LV>& sh = *reinterpret_cast<TShared<LV>*>(smem_raw);
     if (threadIdx.x == 0) {
         for (int i = 0; i < kRing; i++) mbar_init(&sh.full[i], 1);
         fence_mbar_init();
@@ -824,7 +911,7 @@ struct KernelOf {
     static void* fn() {
         return kLines ? reinterpret_cast<void*>(line_index_kernel<LV>) : reinterpret_cast<void*>(tile_index_kernel<LV>);
     }
-    static size_t smem() { return kLines ? sizeof(FShared<LV>) : sizeof(TShared); }
+    static size_t smem() { return kLines ? sizeof(FShared<LV>) : sizeof(TShared<LV>); }
     static int threads() { return kLines ? kThreads : kIndexThreads; }
     static std::atomic<unsigned long long>& done() {
         static std::atomic<unsigned long long> d{0};
@@ -850,7 +937,7 @@ cudaError_t launch(const IndexParams& p, int grid, cudaStream_t stream) {
     if (kLines)
         line_index_kernel<LV><<<grid, kThreads, sizeof(FShared<LV>), stream>>>(p);
     else
-        tile_index_kernel<LV><<<grid, kIndexThreads, sizeof(TShared), stream>>>(p);
+        tile_index_kernel<LV><<<grid, kIndexThreads, sizeof(TShared<LV>), stream>>>(p);
     return cudaGetLastError();
 }
 
