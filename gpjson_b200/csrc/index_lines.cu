@@ -288,13 +288,19 @@ __device__ __forceinline__ RSpan index_scan_rspan(RSpan mine, RSpan* scratch, RS
     RSpan excl = shfl_rspan_up(incl, 1);
     if (lane == 0) excl = RSpan{0, 0, 0, 0};
     group_sync(kBarIndex, kIndexThreads);
-    RSpan prefix{0, 0, 0, 0}, all{0, 0, 0, 0};
+    // every warp scans the eight warp totals in its first eight lanes
+    RSpan wv = lane < kTileWarps ? scratch[lane] : RSpan{0, 0, 0, 0};
 #pragma unroll
-    for (int w = 0; w < kTileWarps; w++) {
-        if (w == warp) prefix = all;
-        all = rspan_compose(all, scratch[w]);
+    for (int off = 1; off < kTileWarps; off <<= 1) {
+        const RSpan o = shfl_rspan_up(wv, off);
+        if (lane >= off) wv = rspan_compose(o, wv);
     }
-    *total = all;
+    *total = RSpan{__shfl_sync(~0u, wv.rq, kTileWarps - 1), __shfl_sync(~0u, wv.d0, kTileWarps - 1),
+                   __shfl_sync(~0u, wv.dt, kTileWarps - 1), __shfl_sync(~0u, wv.nl, kTileWarps - 1)};
+    const int src = warp > 0 ? warp - 1 : 0;
+    RSpan prefix{__shfl_sync(~0u, wv.rq, src), __shfl_sync(~0u, wv.d0, src), __shfl_sync(~0u, wv.dt, src),
+                 __shfl_sync(~0u, wv.nl, src)};
+    if (warp == 0) prefix = RSpan{0, 0, 0, 0};
     return rspan_compose(prefix, excl);
 }
 
