@@ -445,7 +445,7 @@ int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, i
     p.slots = slots;
     p.out = d_out;
     p.out_lines = out_lines;
-    const int64_t want = (f->num_lines + 255) / 256;
+    const int64_t want = (gpj::query_items(f->num_lines, nq) + 255) / 256;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * ctx->query_occupancy));
     GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->stream));
     ctx->launches++;
@@ -1434,7 +1434,7 @@ int gpj_batch_run(gpj_batch* b) {
         fr.lines = fr.file->num_lines;
         fr.out_offset = total_out;
         total_out += nq * static_cast<size_t>(fr.lines) * fr.slots * 2;
-        total_items += static_cast<int64_t>(nq) * fr.lines;
+        total_items += gpj::query_items(fr.lines, static_cast<int>(nq));
     }
     uint8_t* d_blob = nullptr;
     int64_t* d_out = nullptr;
@@ -1454,7 +1454,7 @@ int gpj_batch_run(gpj_batch* b) {
                                         d_blob + blob_at[i] + header,
                                         reinterpret_cast<const int32_t*>(d_blob + blob_at[i]),
                                         static_cast<int>(nq), fr.slots, d_out + fr.out_offset, fr.lines, item});
-            item += static_cast<int64_t>(nq) * fr.lines;
+            item += gpj::query_items(fr.lines, static_cast<int>(nq));
         }
         cudaError_t e = cudaMemcpyAsync(d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->stream);
         if (e == cudaSuccess)

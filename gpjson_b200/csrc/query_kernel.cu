@@ -3,14 +3,19 @@
 // The reference launches find_value once per query with 512x1024 threads
 // and a contiguous range of lines per thread
 // (functions/QueryFunction.java:201-241, kernels/find_value.cu:12-23).
-// Here one launch evaluates every query of the call: threads stride over
-// lines (grid sized to the SMs), and a thread runs all queries on its line
-// back to back, so the line's bitmap words and key bytes are fetched from
-// DRAM once and re-read from L1/L2 by the following queries.  Each query
-// writes its own -1-initialised slots, so its results equal a solo run.
+// Here one launch evaluates every query of the call.  Lines are taken in
+// blocks of 32; a block's (line, query) items are nq warps, one query per
+// warp and one line per lane, so a warp's lanes follow the same opcode
+// sequence and the block's queries run side by side on one SM: the lines'
+// bitmap words and key bytes come from DRAM once and are re-read from L1/L2
+// by the other queries' warps while still there.  Warps stride over the
+// blocks (grid sized to the SMs) and rotate through the queries from one
+// block to the next, so a cheap query does not leave its warp idle.  Each
+// query writes its own -1-initialised slots, so its results equal a solo run.
 #include <cstdint>
 
 #include "interp.cuh"
+#include "query_items.cuh"
 #include "query_kernel.h"
 
 namespace gpj {
@@ -22,15 +27,16 @@ __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
     LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size, p.n, nullptr};
     const int64_t lines = p.num_lines;
     const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
-    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < lines;
-         i += stride) {
+    const int64_t items = query_items(lines, p.num_queries);
+    for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < items; g += stride) {
+        int64_t i;
+        int q;
+        if (!query_item(g, 0, lines, p.num_queries, stride, &i, &q)) continue;
         const int64_t start = p.newlines[i];
         const int64_t end = i + 1 < lines ? p.newlines[i + 1] : p.n;
-        for (int q = 0; q < p.num_queries; q++) {
-            int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + i) * per_line;
-            for (int64_t k = 0; k < per_line; k++) res[k] = -1;
-            run_line(view, start, end, p.bytecode + p.offsets[q], res);
-        }
+        int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + i) * per_line;
+        for (int64_t k = 0; k < per_line; k++) res[k] = -1;
+        run_line(view, start, end, p.bytecode + p.offsets[q], res);
     }
 }
 
@@ -47,9 +53,9 @@ __global__ void __launch_bounds__(256) find_value_batch_kernel(const QueryFile* 
                 hi = mid - 1;
         }
         const QueryFile& F = files[lo];
-        const int64_t k = g - F.item_begin;
-        const int64_t q = k / F.num_lines;
-        const int64_t i = k - q * F.num_lines;
+        int64_t i;
+        int q;
+        if (!query_item(g - F.item_begin, F.item_begin, F.num_lines, F.num_queries, stride, &i, &q)) continue;
         LineView view{F.file, F.n, F.string_index, F.leveled, F.level_size, F.n, nullptr};
         const int64_t start = F.newlines[i];
         const int64_t end = i + 1 < F.num_lines ? F.newlines[i + 1] : F.n;

@@ -5,6 +5,8 @@
 
 #include <cstdint>
 
+#include "query_items.cuh"
+
 namespace gpj {
 
 struct QueryParams {
@@ -43,12 +45,15 @@ struct QueryFile {
     int slots;
     int64_t* out;
     int64_t out_lines;
-    int64_t item_begin;  // first of the file's num_lines x num_queries (line, query) items in the batch
+    // first of the file's items in the batch: ceil(num_lines / 32) blocks of
+    // 32 lines x num_queries (a multiple of 32, so no warp spans two files)
+    int64_t item_begin;
 };
 
 // Every (line, query) item of every file of the batch (`files`: device
-// array, ascending item_begin, total_items items in all), one per thread,
-// query-major within a file so a warp's lanes run the same query.
+// array, ascending item_begin, total_items items in all), one per thread:
+// a warp's lanes run one query on 32 lines of one file, and the warps of a
+// block of lines run its queries side by side.
 cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_items, int grid,
                                     cudaStream_t stream);
 

@@ -42,6 +42,8 @@ def hostsim():
     L.hs_find_values.restype = None
     L.hs_find_values.argtypes = [P, ctypes.c_int64, P, ctypes.c_int64, P, P, ctypes.c_int, P, ctypes.c_int, P, P,
                                  ctypes.c_int]
+    L.hs_query_items.restype = ctypes.c_int64
+    L.hs_query_items.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int64, P]
     L.hs_escaped_mask.restype = ctypes.c_uint64
     L.hs_escaped_mask.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
     return L

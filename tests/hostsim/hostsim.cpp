@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../gpjson_b200/csrc/interp.cuh"
+#include "../../gpjson_b200/csrc/query_items.cuh"
 #include "../../gpjson_b200/csrc/word_ops.cuh"
 
 using namespace gpj;
@@ -213,6 +214,24 @@ void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t line
 // Escape-mask check on one word against a byte loop.
 uint64_t hs_escaped_mask(uint64_t bs, uint32_t cin, uint32_t* cout) {
     return escaped_mask(bs, cin, cout);
+}
+
+// The find_value kernels' item numbering: for items [0, query_items) of a
+// file, writes (line, query) of each real item to pairs[] (in item order)
+// and returns how many there were.
+int64_t hs_query_items(int64_t item_begin, int64_t num_lines, int num_queries, int64_t stride, int64_t* pairs) {
+    const int64_t items = query_items(num_lines, num_queries);
+    int64_t count = 0;
+    for (int64_t k = 0; k < items; k++) {
+        int64_t line;
+        int q;
+        if (query_item(k, item_begin, num_lines, num_queries, stride, &line, &q)) {
+            pairs[2 * count] = line;
+            pairs[2 * count + 1] = q;
+            ++count;
+        }
+    }
+    return count;
 }
 
 }  // extern "C"

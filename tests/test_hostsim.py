@@ -157,3 +157,33 @@ def test_interpreter_matches_oracle(hostsim):
                                        idx.strings.ctypes.data, idx.levels.ctypes.data, 1, ptrs, slots,
                                        got.ctypes.data, colon_ptr, packed)
                 assert np.array_equal(got, want), (path, data[:120], colon_ptr is not None, packed)
+
+
+@pytest.mark.parametrize("lines", [0, 1, 31, 32, 33, 1000])
+@pytest.mark.parametrize("nq", [1, 3, 4, 17])
+@pytest.mark.parametrize("stride", [256, 768, 1792, 227328])
+def test_query_item_numbering(hostsim, lines, nq, stride):
+    """Every (line, query) pair of a file is one item of the find_value
+    kernels, whatever the grid stride and the file's offset in a batch; the
+    32 lanes of a warp share one query on 32 consecutive lines."""
+    for item_begin in (0, 96, 4128):
+        pairs = np.full((max(1, lines * nq), 2), -7, dtype=np.int64)
+        count = hostsim.hs_query_items(item_begin, lines, nq, stride, pairs.ctypes.data)
+        assert count == lines * nq
+        got = pairs[:count]
+        want = {(i, q) for i in range(lines) for q in range(nq)}
+        assert set(map(tuple, got.tolist())) == want
+        # items in numbering order: warps of 32 share the query, lines consecutive
+        full = np.full(((lines + 31) // 32 * 32 * nq, 2), -1, dtype=np.int64)
+        k = 0
+        for blk in range((lines + 31) // 32):
+            for w in range(nq):
+                n_real = min(32, lines - 32 * blk)
+                full[k:k + n_real] = got[:n_real]
+                got = got[n_real:]
+                k += 32
+        for w0 in range(0, len(full), 32):
+            warp = full[w0:w0 + 32]
+            real = warp[warp[:, 0] >= 0]
+            assert len(set(real[:, 1].tolist())) <= 1
+            assert (np.diff(real[:, 0]) == 1).all()
