@@ -59,12 +59,18 @@ GPJ_HD int64_t first_of4(int64_t w, uint64_t a, uint64_t b, uint64_t c, uint64_t
     return p < limit ? p : limit;
 }
 
-GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit) {
+// `cw`/`cv`: a word of bm the caller already holds (index, value; cw = -1
+// for none), used instead of reloading it; on return they hold the word the
+// result was found in.
+GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit, int64_t& cw, uint64_t& cv) {
     if (from >= limit) return limit;
     int64_t w = from >> 6;
     const int64_t wend = ((limit - 1) >> 6) + 1;
-    const uint64_t m = bm[w] & (~0ull << (from & 63));
+    const uint64_t first = w == cw ? cv : bm[w];
+    const uint64_t m = first & (~0ull << (from & 63));
     if (m) {
+        cw = w;
+        cv = first;
         const int64_t p = (w << 6) + ctz64(m);
         return p < limit ? p : limit;
     }
@@ -72,6 +78,8 @@ GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit) {
     for (++w; w < wend && w < (from >> 6) + 3; ++w) {
         const uint64_t x = bm[w];
         if (x) {
+            cw = w;
+            cv = x;
             const int64_t p = (w << 6) + ctz64(x);
             return p < limit ? p : limit;
         }
@@ -81,9 +89,20 @@ GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit) {
         const uint64_t b = w + 1 < wend ? bm[w + 1] : 0;
         const uint64_t c = w + 2 < wend ? bm[w + 2] : 0;
         const uint64_t d = w + 3 < wend ? bm[w + 3] : 0;
-        if (a | b | c | d) return first_of4(w, a, b, c, d, limit);
+        if (a | b | c | d) {
+            const int64_t p = first_of4(w, a, b, c, d, limit);
+            cw = w + (a ? 0 : (b ? 1 : (c ? 2 : 3)));
+            cv = a ? a : (b ? b : (c ? c : d));
+            return p;
+        }
     }
     return limit;
+}
+
+GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit) {
+    int64_t cw = -1;
+    uint64_t cv = 0;
+    return next_bit(bm, from, limit, cw, cv);
 }
 
 // First position in [from, limit) set in bm and (in `filt`, or not in it
@@ -116,11 +135,12 @@ GPJ_HD int64_t next_bit_filtered(const uint64_t* bm, const uint64_t* filt, bool 
     return limit;
 }
 
-// Last set bit of `bm` at a position in (floor, from], or -1.
-GPJ_HD int64_t prev_bit(const uint64_t* bm, int64_t from, int64_t floor) {
+// Last set bit of `bm` at a position in (floor, from], or -1; `first` is
+// bm[from >> 6] (read only when from > floor).
+GPJ_HD int64_t prev_bit(const uint64_t* bm, uint64_t first, int64_t from, int64_t floor) {
     if (from <= floor) return -1;
     int64_t w = from >> 6;
-    uint64_t m = bm[w] & (~0ull >> (63 - (from & 63)));
+    uint64_t m = first & (~0ull >> (63 - (from & 63)));
     for (;;) {
         if (m) {
             const int64_t k = (w << 6) + 63 - clz64(m);
@@ -130,6 +150,10 @@ GPJ_HD int64_t prev_bit(const uint64_t* bm, int64_t from, int64_t floor) {
         --w;
         m = bm[w];
     }
+}
+
+GPJ_HD int64_t prev_bit(const uint64_t* bm, int64_t from, int64_t floor) {
+    return from <= floor ? -1 : prev_bit(bm, bm[from >> 6], from, floor);
 }
 
 GPJ_HD uint32_t read_varint(const uint8_t* ir, int& pc) {
@@ -208,6 +232,11 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
     bool execute = true;
 
     int64_t j = line_start;
+    // the search state: j came from next_bit (so it is a structural bit of
+    // level cur), and the bitmap word next_bit found it in
+    bool found = false;
+    int64_t cw = -1;
+    uint64_t cv = 0;
     while (j < lv.end(cur) && j < n) {
         while (execute) {
             type = ir[pc++];
@@ -280,12 +309,21 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
         // Searching: j is a candidate position ([bounded] only inside the file).
         if (j < hi) {
             const uint64_t* bits = v.levels + v.level_size * cur;
-            const bool structural = (bits[j >> 6] >> (j & 63)) & 1u;
+            const bool structural = found || ((bits[j >> 6] >> (j & 63)) & 1u);
+            const uint8_t at = file[j];
             if (type == 4) {  // key match at a structural ':' (:225-251)
-                if (structural && file[j] == ':') {
-                    const int64_t string_end = prev_bit(v.string_index, j - 1, line_start);
+                // Loads that do not depend on each other are issued together:
+                // the string-index word before j, and the byte where the key's
+                // opening quote is when the key ends right before the ':'
+                // (the usual layout), checked against the real position below.
+                const uint64_t sw = j > line_start ? v.string_index[(j - 1) >> 6] : 0;
+                const int64_t guess = j - 2 - want_len;
+                const uint8_t at_guess = guess >= line_start ? file[guess] : 0;
+                if (structural && at == ':') {
+                    const int64_t string_end = prev_bit(v.string_index, sw, j - 1, line_start);
                     const int64_t string_start = string_end - want_len;
-                    if (string_start >= line_start && file[string_start] == '"') {
+                    if (string_start >= line_start &&
+                        (string_start == guess ? at_guess : file[string_start]) == '"') {
                         bool same = true;
                         for (int64_t k = 0; k < want_len; k++) {
                             if (want[k] != file[string_start + k + 1]) {
@@ -297,7 +335,7 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
                     }
                 }
             } else if (type == 5) {  // index match at a structural ',' (:252-259)
-                if (structural && file[j] == ',') {
+                if (structural && at == ',') {
                     const int64_t count = lv.idx(cur) + 1;
                     lv.set_idx(cur, count);
                     if (want_index == count) execute = true;
@@ -305,6 +343,7 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
             }
         }
         ++j;
+        found = false;
         if (!execute) {
             // Nothing happens until the next structural bit of this level.
             const int64_t end = lv.end(cur);
@@ -313,8 +352,11 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
                 if (v.colon)
                     j = next_bit_filtered(v.levels + v.level_size * cur, v.colon, type != 4, j, lim);
                 else
-                    j = next_bit(v.levels + v.level_size * cur, j, lim);
+                    j = next_bit(v.levels + v.level_size * cur, j, lim, cw, cv);
+                found = j < lim;
             }
+        } else {
+            cw = -1;  // opcodes run next and may change the level
         }
     }
     return kLineDone;
