@@ -237,7 +237,9 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
     bool found = false;
     int64_t cw = -1;
     uint64_t cv = 0;
-    while (j < lv.end(cur) && j < n) {
+    int64_t cend = lv.end(cur);  // lv.end(cur), kept while searching (only opcodes change it)
+    while (j < cend && j < n) {
+        const bool ran = execute;
         while (execute) {
             type = ir[pc++];
             switch (type) {
@@ -305,6 +307,7 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
                     return kLineDone;
             }
         }
+        if (ran) cend = lv.end(cur);
 
         // Searching: j is a candidate position ([bounded] only inside the file).
         if (j < hi) {
@@ -346,8 +349,7 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
         found = false;
         if (!execute) {
             // Nothing happens until the next structural bit of this level.
-            const int64_t end = lv.end(cur);
-            const int64_t lim = end < n ? end : n;
+            const int64_t lim = cend < n ? cend : n;
             if (j < lim) {
                 if (v.colon)
                     j = next_bit_filtered(v.levels + v.level_size * cur, v.colon, type != 4, j, lim);
