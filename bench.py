@@ -344,20 +344,30 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
 
     # ---- end to end through the C ABI with host buffers ----------------------
     res_host = torch.empty((len(QUERIES), lines, slots, 2), dtype=torch.int64, pin_memory=True)
-    e2e_times = []
+    # one call: copy, index and queries pipelined (gpj_file_from_host_query);
+    # beside it the two-call form (gpj_file_from_host_indexed, then gpj_query)
+    e2e_times, e2e_two_call = [], []
+    e2e_lines = ctypes.c_int64()
     for k in range(1 + args.e2e_steps):
-        barrier(world, device)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        h = ctypes.c_void_p()
-        g._native.check(lib.gpj_file_from_host_indexed(ctx, host.data_ptr(), n, LEVELS, ctypes.byref(h)))
-        g._native.check(lib.gpj_query(ctx, h, len(compiled), ptrs, lens, slots, res_host.data_ptr(),
-                                      res_host.numel()))
-        lib.gpj_file_release(h)
-        dt = time.perf_counter() - t0
-        if k > 0:
-            e2e_times.append(dt)
+        for form in ("two", "one"):  # the one-call form last: its results are checked below
+            barrier(world, device)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            h = ctypes.c_void_p()
+            if form == "one":
+                g._native.check(lib.gpj_file_from_host_query(ctx, host.data_ptr(), n, LEVELS, len(compiled), ptrs,
+                                                             lens, slots, res_host.data_ptr(), res_host.numel(),
+                                                             ctypes.byref(e2e_lines), ctypes.byref(h)))
+            else:
+                g._native.check(lib.gpj_file_from_host_indexed(ctx, host.data_ptr(), n, LEVELS, ctypes.byref(h)))
+                g._native.check(lib.gpj_query(ctx, h, len(compiled), ptrs, lens, slots, res_host.data_ptr(),
+                                              res_host.numel()))
+            lib.gpj_file_release(h)
+            dt = time.perf_counter() - t0
+            if k > 0:
+                (e2e_times if form == "one" else e2e_two_call).append(dt)
     e2e_s = max_over_ranks(statistics.mean(e2e_times), world, device)
+    e2e_two_s = max_over_ranks(statistics.mean(e2e_two_call), world, device)
     # the e2e ceiling: a plain pinned host-to-device copy of the same bytes
     scratch = torch.empty(n, dtype=torch.uint8, device=device)
     scratch.copy_(host, non_blocking=True)
@@ -434,7 +444,10 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
             "unit": "GB/s",
             "h2d_bytes_per_step": n,
             "d2h_bytes_per_step": int(res_host.numel() * 8),
-            "path": "gpj_file_from_host_indexed (copy overlapped with indexing) + gpj_query to pinned host",
+            "path": "gpj_file_from_host_query: copy overlapped with indexing and with each chunk's queries, "
+                    "results to pinned host",
+            "two_call_gbs": round(world * n / e2e_two_s / 1e9, 3),
+            "two_call_path": "gpj_file_from_host_indexed (copy overlapped with indexing) + gpj_query",
             "pinned_h2d_copy_gbs": round(h2d_gbs, 2),
         },
         "gpu_launches": int(launches),

@@ -434,6 +434,31 @@ class GPJSON:
             self._native.h, arr.ctypes.data, arr.size, num_levels, byref(h)))
         return File(self._native, h, host_bytes=bytes(arr.tobytes()) if arr.size < (1 << 26) else arr)
 
+    def load_bytes_query(self, data: bytes | bytearray | memoryview | np.ndarray, num_levels: int,
+                         queries: list[CompiledQuery], slots: int | None = None,
+                         out: np.ndarray | None = None) -> tuple[File, np.ndarray]:
+        """gpj_file_from_host_query: copy, index and query in one pipelined
+        call; returns the indexed File and int64 [nq][lines][slots][2].
+        `out` (optional, e.g. page-locked) receives the results when it is
+        large enough; otherwise a new array is returned."""
+        arr = np.frombuffer(data, dtype=np.uint8) if not isinstance(data, np.ndarray) else data
+        nq = len(queries)
+        slots = slots or max(q.num_results for q in queries)
+        bufs = [ctypes.create_string_buffer(q.bytecode, len(q.bytecode)) for q in queries]
+        ptrs = (c_void_p * nq)(*[ctypes.addressof(b) for b in bufs])
+        lens = (c_size_t * nq)(*[len(q.bytecode) for q in queries])
+        h, lines = c_void_p(), c_int64()
+        dst = out if out is not None else np.empty(0, dtype=np.int64)
+        rc = self._native.lib.gpj_file_from_host_query(
+            self._native.h, arr.ctypes.data, arr.size, num_levels, nq, ptrs, lens, slots,
+            dst.ctypes.data if dst.size else None, dst.size, byref(lines), byref(h))
+        if rc == _lib.GPJ_ELIMIT and h.value:
+            f = File(self._native, h, host_bytes=bytes(arr.tobytes()) if arr.size < (1 << 26) else arr)
+            return f, f.run(queries, slots)
+        self._native.check(rc)
+        f = File(self._native, h, host_bytes=bytes(arr.tobytes()) if arr.size < (1 << 26) else arr)
+        return f, dst.reshape(-1)[: nq * lines.value * slots * 2].reshape(nq, lines.value, slots, 2)
+
     def from_device(self, ptr: int, n: int, keepalive=None) -> File:
         """Wraps n bytes already in device memory (e.g. a torch uint8 tensor's
         data_ptr()); `keepalive` is held for the File's lifetime."""

@@ -60,6 +60,11 @@ SIGNATURES: dict[str, tuple] = {
     ),
     "gpj_set_query_fusion": (c_int, [c_void_p, c_int]),
     "gpj_file_from_host_indexed": (c_int, [c_void_p, c_void_p, c_int64, c_int, POINTER(c_void_p)]),
+    "gpj_file_from_host_query": (
+        c_int,
+        [c_void_p, c_void_p, c_int64, c_int, c_int, POINTER(c_void_p), POINTER(c_size_t), c_int, c_void_p, c_int64,
+         POINTER(c_int64), POINTER(c_void_p)],
+    ),
     "gpj_batch_create": (c_int, [c_void_p, POINTER(c_void_p)]),
     "gpj_batch_add": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_char_p), POINTER(c_int)]),
     "gpj_batch_run": (c_int, [c_void_p]),

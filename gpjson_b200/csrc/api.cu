@@ -429,9 +429,13 @@ int upload_queries(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, 
     return GPJ_OK;
 }
 
-int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, int64_t out_lines) {
+// find_value over the file's lines, or (d_range given) over lines
+// [d_range[0], d_range[1]) of a file whose index is still being built
+// (`last`: they include the file's last line).
+int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, int64_t out_lines,
+                 const int64_t* d_range = nullptr, bool last = false) {
     const size_t header = ((static_cast<size_t>(nq) * 4 + 15) / 16) * 16;
-    gpj::QueryParams p;
+    gpj::QueryParams p{};
     p.file = f->d_data;
     p.n = f->n;
     p.newlines = f->d_nl;
@@ -445,7 +449,10 @@ int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, i
     p.slots = slots;
     p.out = d_out;
     p.out_lines = out_lines;
-    const int64_t want = (gpj::query_items(f->num_lines, nq) + 255) / 256;
+    p.range = d_range;
+    p.last = last ? 1 : 0;
+    p.newline_cap = f->nl_cap;
+    const int64_t want = d_range ? INT64_MAX : (gpj::query_items(f->num_lines, nq) + 255) / 256;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * ctx->query_occupancy));
     GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->stream));
     ctx->launches++;
@@ -510,17 +517,33 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
     return GPJ_OK;
 }
 
-// Bytes copied per step of load_and_index: 4681 line-kernel tiles (~64 MiB).
-constexpr int64_t kLoadChunk = gpj::kLineTileBytes * 4681;
+// Bytes copied per step of load_and_index: 4096 line-kernel tiles (56 MiB),
+// a whole number of the newline scan's 1024-tile blocks.
+constexpr int64_t kLoadTiles = 4096;
+constexpr int64_t kLoadChunk = gpj::kLineTileBytes * kLoadTiles;
+
+// Queries load_and_index evaluates on each chunk's lines as soon as their
+// index is complete (bytecode uploaded; results strided by out_lines).
+struct ChunkQueries {
+    int nq = 0;
+    int slots = 0;
+    int64_t* d_out = nullptr;
+    int64_t out_lines = 0;
+};
 
 // Copies n host bytes into f->d_owned in chunks on the copy stream and
 // indexes chunk k with the line-parallel kernel as soon as chunk k + 1 has
 // landed (a line starting in chunk k ends in chunk k + 1 unless it is longer
-// than a chunk), so the copy and the index build overlap.  Inputs the line
-// kernel cannot index this way (not NDJSON, or a line longer than a chunk)
-// are indexed again from the complete copy by run_index.
-int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_levels) {
+// than a chunk), so the copy and the index build overlap.  With `cq`, the
+// newline index of chunk k follows at once, and then find_value on the
+// lines it completes, so the queries overlap the copy too (*queries_done
+// tells whether they all ran that way).  Inputs the line kernel cannot
+// index this way (not NDJSON, or a line longer than a chunk) are indexed
+// again from the complete copy by run_index.
+int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_levels, const ChunkQueries* cq = nullptr,
+                   bool* queries_done = nullptr) {
     const int64_t n = f->n;
+    if (queries_done) *queries_done = false;
     int rc = ensure_index_buffers(ctx, f, num_levels);
     if (rc) return rc;
     f->indexed = false;
@@ -553,10 +576,14 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         p.materialize = 1;
         TileScratch ts;
         rc = alloc_tile_scratch(ctx, n, &ts);
+        int64_t* d_lines = nullptr;  // [k + 1]: lines complete after chunk k
+        if (!rc && cq) rc = device_alloc(ctx, &d_lines, static_cast<size_t>(nchunks + 1), "cudaMalloc(chunk lines)");
         if (rc) {
             free_tile_scratch(ctx, &ts);
+            device_free(ctx, d_lines);
             return rc;
         }
+        if (cq) GPJ_CUDA(ctx, cudaMemsetAsync(d_lines, 0, sizeof(int64_t), ctx->stream));
         GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
         p.status = ctx->d_status;
         p.newline_bits = ts.bits;
@@ -564,12 +591,18 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         // the copies start once the buffers exist (pool allocations are ordered on ctx->stream)
         GPJ_CUDA(ctx, cudaEventRecord(ctx->ev_ready, ctx->stream));
         GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0));
-        const int64_t tiles_per_chunk = kLoadChunk / gpj::kLineTileBytes;
         auto launch_chunk = [&](int64_t k) -> int {
-            set_tile_range(&p, k * tiles_per_chunk, std::min(p.ntiles, (k + 1) * tiles_per_chunk),
-                           std::min(n, (k + 2) * kLoadChunk));
+            const int64_t t0 = k * kLoadTiles, t1 = std::min(p.ntiles, (k + 1) * kLoadTiles);
+            set_tile_range(&p, t0, t1, std::min(n, (k + 2) * kLoadChunk));
             GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->chunk_events[std::min(k + 1, nchunks - 1)], 0));
-            return launch_tiles(ctx, p);
+            int r = launch_tiles(ctx, p);
+            if (r || !cq) return r;
+            // the chunk's newline index, then the queries on the lines it completes
+            const int64_t grid = std::min<int64_t>((t1 - t0 + 7) / 8, static_cast<int64_t>(ctx->sms) * 8);
+            GPJ_CUDA(ctx, gpj::launch_newline_index_range(p, ts.offsets, t0, t1, d_lines + k + 1, static_cast<int>(grid),
+                                                          ctx->stream));
+            ctx->launches += 2;
+            return launch_query(ctx, f, cq->nq, cq->slots, cq->d_out, cq->out_lines, d_lines + k, k == nchunks - 1);
         };
         for (int64_t k = 0; k < nchunks && !rc; k++) {
             const int64_t pos = k * kLoadChunk;
@@ -580,8 +613,18 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
             if (!rc && k >= 1) rc = launch_chunk(k - 1);
         }
         if (!rc) rc = launch_chunk(nchunks - 1);
-        if (!rc) rc = finish_tiles(ctx, p, ts);
+        if (!rc) {
+            if (cq) {  // the newline index is complete: read the status words
+                cudaError_t e = cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(unsigned long long),
+                                                cudaMemcpyDeviceToHost, ctx->stream);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+                if (e != cudaSuccess) rc = cuda_fail(ctx, e, "chunked index status");
+            } else {
+                rc = finish_tiles(ctx, p, ts);
+            }
+        }
         free_tile_scratch(ctx, &ts);
+        device_free(ctx, d_lines);
         if (rc) {
             cudaStreamSynchronize(ctx->copy_stream);
             return rc;
@@ -594,6 +637,8 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
             if (rc) return rc;
         } else if ((rc = status_error(ctx, errs))) {
             return rc;
+        } else if (cq && lines <= f->nl_cap && lines <= cq->out_lines && queries_done) {
+            *queries_done = true;
         }
     }
     if (lines > f->nl_cap) {  // more lines than the first guess: size exactly and rebuild
@@ -911,6 +956,81 @@ int gpj_file_from_host_indexed(gpj_ctx* ctx, const void* data, int64_t n, int nu
     }
     *out = f;
     return GPJ_OK;
+}
+
+int gpj_file_from_host_query(gpj_ctx* ctx, const void* data, int64_t n, int num_levels, int nq,
+                             const uint8_t* const* bytecode, const size_t* bytecode_len, int result_slots,
+                             int64_t* host_out, int64_t out_count, int64_t* num_lines, gpj_file** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out || !num_lines || !bytecode || !bytecode_len || n < 0 || (n > 0 && !data) || out_count < 0 ||
+        (out_count > 0 && !host_out))
+        return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (num_levels < 1 || num_levels > GPJ_MAX_LEVELS)
+        return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(num_levels));
+    rc = check_query_args(ctx, nq, result_slots);
+    if (rc) return rc;
+    gpj_file* f = nullptr;
+    rc = make_file(ctx, n, &f);
+    if (rc) return rc;
+    rc = device_alloc(ctx, &f->d_owned, static_cast<size_t>(n), "cudaMalloc(file)");
+    if (rc) {
+        delete f;
+        return rc;
+    }
+    f->d_data = f->d_owned;
+    auto done = [&](int r) {
+        if (r) {
+            gpj_file_release(f);
+            return r;
+        }
+        *out = f;
+        return GPJ_OK;
+    };
+    int depth = 0;
+    rc = upload_queries(ctx, f, nq, bytecode, bytecode_len, result_slots, &depth);
+    if (!rc && depth > num_levels)
+        rc = fail(ctx, GPJ_ELIMIT, "queries need " + std::to_string(depth) + " levels, the index is built with " +
+                                       std::to_string(num_levels));
+    if (!rc) rc = ensure_index_buffers(ctx, f, num_levels);
+    // results strided by the newline index's line capacity until the count is known
+    int64_t stride = f->nl_cap;
+    if (!rc) rc = ensure_out(ctx, f, static_cast<size_t>(nq) * stride * result_slots * 2);
+    if (rc) return done(rc);
+    const double t0 = now_ms();
+    ChunkQueries cq;
+    cq.nq = nq;
+    cq.slots = result_slots;
+    cq.d_out = f->d_out;
+    cq.out_lines = stride;
+    bool queried = false;
+    rc = load_and_index(ctx, f, static_cast<const uint8_t*>(data), num_levels, &cq, &queried);
+    if (rc) return done(rc);
+    if (!queried) {
+        // the input was indexed again from the complete copy: query it whole
+        stride = f->num_lines;
+        rc = ensure_out(ctx, f, static_cast<size_t>(nq) * stride * result_slots * 2);
+        if (!rc) rc = launch_query(ctx, f, nq, result_slots, f->d_out, stride);
+        if (rc) return done(rc);
+    }
+    *num_lines = f->num_lines;
+    const size_t per_query = static_cast<size_t>(f->num_lines) * result_slots * 2;
+    if (out_count < static_cast<int64_t>(per_query * nq)) {
+        *out = f;  // indexed and kept: gpj_query gives the results
+        return fail(ctx, GPJ_ELIMIT, "output holds " + std::to_string(out_count) + " elements, " +
+                                         std::to_string(per_query * nq) + " needed (the file is indexed)");
+    }
+    for (int q = 0; q < nq && !rc; q++) {
+        cudaError_t e = cudaMemcpyAsync(host_out + q * per_query, f->d_out + static_cast<size_t>(q) * stride * result_slots * 2,
+                                        per_query * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemcpyAsync(results)");
+    }
+    if (!rc) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaStreamSynchronize(results)");
+    }
+    if (!rc) rc = end_phase(ctx, "load_index_query", t0);
+    return done(rc);
 }
 
 int gpj_file_open(gpj_ctx* ctx, const char* filename, gpj_file** out) {

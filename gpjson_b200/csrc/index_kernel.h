@@ -102,6 +102,13 @@ int tile_index_max_ctas_per_sm(int num_levels);
 // entries), then every tile's '\n' positions; writes status[0] =
 // newlines + 1 and at most newline_cap entries.  Two launches, one stream.
 cudaError_t launch_newline_index(const IndexParams& p, int64_t* offsets, int grid, cudaStream_t stream);
+// The same for tiles [t0, t1) only, once every earlier tile's newline index
+// is written (t0 and, unless t1 = ntiles, t1 multiples of 1024); the number
+// of lines whose both ends are then known goes to device memory
+// `lines_done` (the newlines up to tile t1 - 1, + 1 for the last line when
+// t1 = ntiles).
+cudaError_t launch_newline_index_range(const IndexParams& p, int64_t* offsets, int64_t t0, int64_t t1,
+                                       int64_t* lines_done, int grid, cudaStream_t stream);
 inline int64_t newline_offsets_words(int64_t ntiles) { return ntiles + (ntiles + 1023) / 1024; }
 
 // Where the newline index of one file of a batch goes.

@@ -23,12 +23,14 @@ constexpr int kWordsPerLane = kTileWordsL / 32;                      // 7
 static_assert(kWordsPerLane * 32 == kTileWordsL, "a tile's words split evenly over a warp");
 
 // Offsets of the tile counts within blocks of 1024 tiles (coalesced, one
-// CTA per block); the block sums go after the ntiles entries.
+// CTA per block, blocks blk0, blk0 + 1, ...); the block sums go after the
+// ntiles entries.
 __global__ void __launch_bounds__(kScanThreads) newline_offsets_kernel(const int32_t* counts, int64_t ntiles,
-                                                                       int64_t* offsets) {
+                                                                       int64_t* offsets, int64_t blk0) {
     __shared__ int64_t warp_total[kScanThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int64_t i = static_cast<int64_t>(blockIdx.x) * kScanThreads + tid;
+    const int64_t blk = blk0 + blockIdx.x;
+    const int64_t i = blk * kScanThreads + tid;
     const int64_t c = i < ntiles ? counts[i] : 0;
     int64_t incl = c;
 #pragma unroll
@@ -45,7 +47,7 @@ __global__ void __launch_bounds__(kScanThreads) newline_offsets_kernel(const int
         all += warp_total[w];
     }
     if (i < ntiles) offsets[i] = before + incl - c;
-    if (tid == 0) offsets[ntiles + blockIdx.x] = all;
+    if (tid == 0) offsets[ntiles + blk] = all;
 }
 
 // Sum of the tile counts before tile t of the whole batch (all lanes of a
@@ -61,16 +63,20 @@ __device__ __forceinline__ int64_t tiles_before(const int64_t* offsets, int64_t 
     return base + offsets[t];
 }
 
-// A warp per tile: the tile's newlines before it in its file (the batch
-// prefix at the tile minus the prefix at the file's first tile), then the
-// positions, each lane taking consecutive bitmap words.  `files` null: the
-// single file `one`.
+// A warp per tile of [t0, t1): the tile's newlines before it in its file
+// (the batch prefix at the tile minus the prefix at the file's first tile),
+// then the positions, each lane taking consecutive bitmap words.  `files`
+// null: the single file `one`.  `lines_done` (optional, single file): the
+// warp of tile t1 - 1 writes there how many lines have both ends in the
+// newline index written so far (the newlines up to t1 - 1, plus the last
+// line when t1 - 1 is the file's last tile).
 __global__ void __launch_bounds__(256) newline_scatter_kernel(const int32_t* counts, const int64_t* offsets,
-                                                              int64_t ntiles, LineFile one, const LineFile* files,
-                                                              int nfiles) {
+                                                              int64_t ntiles, int64_t t0, int64_t t1, LineFile one,
+                                                              const LineFile* files, int nfiles,
+                                                              int64_t* lines_done) {
     const int lane = threadIdx.x & 31;
     const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
-    for (int64_t t = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); t < ntiles;
+    for (int64_t t = t0 + static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); t < t1;
          t += warps) {
         LineFile F = one;
         if (files) {
@@ -88,6 +94,7 @@ __global__ void __launch_bounds__(256) newline_scatter_kernel(const int32_t* cou
         const int64_t base = tiles_before(offsets, ntiles, t) - tiles_before(offsets, ntiles, F.tile_begin);
         if (lt == 0 && lane == 0 && F.cap > 0) F.newlines[0] = 0;
         if (lt == F.ntiles - 1 && lane == 0) F.status[0] = static_cast<unsigned long long>(base + counts[t] + 1);
+        if (lines_done && t == t1 - 1 && lane == 0) *lines_done = base + counts[t] + (lt == F.ntiles - 1 ? 1 : 0);
         const int64_t w0 = lt * kTileWordsL + lane * kWordsPerLane;
         uint64_t m[kWordsPerLane];
         int cnt = 0;
@@ -121,22 +128,34 @@ cudaError_t launch_newline_index_batch(const int32_t* tile_newlines, int64_t tot
                                        int nfiles, int64_t* offsets, int grid, cudaStream_t stream) {
     const int64_t blocks = (total_tiles + kScanThreads - 1) / kScanThreads;
     newline_offsets_kernel<<<static_cast<unsigned>(blocks), kScanThreads, 0, stream>>>(tile_newlines, total_tiles,
-                                                                                       offsets);
+                                                                                       offsets, 0);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    newline_scatter_kernel<<<grid, 256, 0, stream>>>(tile_newlines, offsets, total_tiles, LineFile{}, files, nfiles);
+    newline_scatter_kernel<<<grid, 256, 0, stream>>>(tile_newlines, offsets, total_tiles, 0, total_tiles, LineFile{},
+                                                     files, nfiles, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_newline_index_range(const IndexParams& p, int64_t* offsets, int64_t t0, int64_t t1,
+                                       int64_t* lines_done, int grid, cudaStream_t stream) {
+    const int64_t ntiles = (p.n + kLineTileBytes - 1) / kLineTileBytes;
+    if (t0 % kScanThreads != 0 || t1 <= t0 || t1 > ntiles || (t1 != ntiles && t1 % kScanThreads != 0))
+        return cudaErrorInvalidValue;
+    const int64_t blk0 = t0 / kScanThreads;
+    const int64_t blocks = (t1 - t0 + kScanThreads - 1) / kScanThreads;
+    newline_offsets_kernel<<<static_cast<unsigned>(blocks), kScanThreads, 0, stream>>>(p.tile_newlines, ntiles, offsets,
+                                                                                       blk0);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const LineFile one{p.newline_bits, p.level_size, p.newlines, p.newline_cap, p.status, 0, ntiles};
+    newline_scatter_kernel<<<grid, 256, 0, stream>>>(p.tile_newlines, offsets, ntiles, t0, t1, one, nullptr, 0,
+                                                     lines_done);
     return cudaGetLastError();
 }
 
 cudaError_t launch_newline_index(const IndexParams& p, int64_t* offsets, int grid, cudaStream_t stream) {
     const int64_t ntiles = (p.n + kLineTileBytes - 1) / kLineTileBytes;
-    const int64_t blocks = (ntiles + kScanThreads - 1) / kScanThreads;
-    newline_offsets_kernel<<<static_cast<unsigned>(blocks), kScanThreads, 0, stream>>>(p.tile_newlines, ntiles, offsets);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    const LineFile one{p.newline_bits, p.level_size, p.newlines, p.newline_cap, p.status, 0, ntiles};
-    newline_scatter_kernel<<<grid, 256, 0, stream>>>(p.tile_newlines, offsets, ntiles, one, nullptr, 0);
-    return cudaGetLastError();
+    return launch_newline_index_range(p, offsets, 0, ntiles, nullptr, grid, stream);
 }
 
 }  // namespace gpj

@@ -25,15 +25,24 @@ namespace {
 __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size, p.n, nullptr};
-    const int64_t lines = p.num_lines;
     const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
+    // lines [first, first + lines); the file's last line ends at p.n
+    int64_t first = 0, lines = p.num_lines, file_lines = p.num_lines;
+    if (p.range) {
+        first = p.range[0];
+        lines = p.range[1] - first;
+        file_lines = p.last ? p.range[1] : INT64_MAX;
+    }
     const int64_t items = query_items(lines, p.num_queries);
     for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < items; g += stride) {
-        int64_t i;
+        int64_t li;
         int q;
-        if (!query_item(g, 0, lines, p.num_queries, stride, &i, &q)) continue;
+        if (!query_item(g, 0, lines, p.num_queries, stride, &li, &q)) continue;
+        const int64_t i = first + li;
+        const bool to_eof = i + 1 >= file_lines;
+        if (p.range && (i >= p.out_lines || i + (to_eof ? 0 : 1) >= p.newline_cap)) continue;
         const int64_t start = p.newlines[i];
-        const int64_t end = i + 1 < lines ? p.newlines[i + 1] : p.n;
+        const int64_t end = to_eof ? p.n : p.newlines[i + 1];
         int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + i) * per_line;
         for (int64_t k = 0; k < per_line; k++) res[k] = -1;
         run_line(view, start, end, p.bytecode + p.offsets[q], res);

@@ -23,6 +23,15 @@ struct QueryParams {
     int slots;     // result slots per line (max num_results)
     int64_t* out;       // [num_queries][out_lines][slots][2]
     int64_t out_lines;  // query stride of `out` (>= num_lines)
+    // Optional, for a file still being indexed: only lines [range[0],
+    // range[1]) (device memory, read by the kernel), whose newline-index
+    // entries up to range[1] are written; the last of them ends at the file
+    // end when `last`, else at newlines[range[1]].  Lines whose results or
+    // end do not fit out_lines / newline_cap are skipped (the caller sees the
+    // line count and evaluates again).
+    const int64_t* range;
+    int last;
+    int64_t newline_cap;
 };
 
 cudaError_t launch_find_value(const QueryParams& p, int grid, cudaStream_t stream);

@@ -120,6 +120,22 @@ int gpj_file_from_host(gpj_ctx *ctx, const void *data, int64_t n, gpj_file **out
 int gpj_file_from_host_indexed(gpj_ctx *ctx, const void *data, int64_t n, int num_levels,
                                gpj_file **out);
 
+/* gpj_file_from_host_indexed and gpj_query in one pipelined call: while
+ * the input is still being copied, each chunk's newline index is built right
+ * after its index kernel and find_value runs on the lines it completes, so
+ * the queries overlap the copy as well (the reference's query() reads the
+ * file, then indexes it, then runs one find_value launch per query,
+ * QueryFunction.java:165-241, one after the other).  Results as gpj_query:
+ * int64[nq][lines][result_slots][2] into host_out (`out_count` elements;
+ * page-locked memory copies fastest).  *num_lines receives the line count;
+ * when host_out is too small the call returns GPJ_ELIMIT after indexing, with
+ * *num_lines and *out set, and gpj_query on *out gives the results.  *out is
+ * the indexed file (num_levels levels), to release with gpj_file_release. */
+int gpj_file_from_host_query(gpj_ctx *ctx, const void *data, int64_t n, int num_levels, int nq,
+                             const uint8_t *const *bytecode, const size_t *bytecode_len,
+                             int result_slots, int64_t *host_out, int64_t out_count,
+                             int64_t *num_lines, gpj_file **out);
+
 /* Wraps `n` bytes that are already in device memory (not copied, not freed).
  * `d_data` must be 16-byte aligned and stay valid until gpj_file_release. */
 int gpj_file_from_device(gpj_ctx *ctx, const void *d_data, int64_t n, gpj_file **out);

@@ -196,3 +196,56 @@ def test_errors(gpjson):
         gpjson.query(path, "$" + ".a" * 17)
     with pytest.raises(gj.GPJSONException):
         gpjson.query(str(FIXTURES / "does-not-exist.ldjson"), "$.a")
+
+
+def _pipelined_case(case: str) -> tuple[np.ndarray, list[str]]:
+    if case == "small":
+        return datagen.tweets(1 << 20, seed=datagen.SEED_BASE + 61), TWEET_PATHS
+    if case == "empty":
+        return np.zeros(0, dtype=np.uint8), ["$.a"]
+    if case == "many_lines":  # more lines than the newline index's first estimate
+        return np.frombuffer(b'{"a":1}\n' * (15 << 20), dtype=np.uint8), ["$.a", "$.b"]
+    base = datagen.tweets(150 << 20, seed=datagen.SEED_BASE + 62)
+    if case == "ndjson":
+        return base, TWEET_PATHS
+    cut = int(np.flatnonzero(base[100 << 20:] == 10)[0]) + (100 << 20)
+    extra = b'{"k":"' + b"x" * (70 << 20) + b'"}' if case == "long_line" else b'{"k": "a' + bytes([10]) + b'b"}'
+    data = np.concatenate([base[: cut + 1], np.frombuffer(extra + b"\n", dtype=np.uint8), base[cut + 1:]])
+    return data, TWEET_PATHS + ["$.k"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ndjson", "long_line", "raw_newline", "small", "empty", "many_lines"])
+def test_pipelined_query_equals_load_then_query(gpjson, case):
+    """gpj_file_from_host_query (each chunk's newline index and queries run
+    while later chunks are still copied) equals the plain copy + index build
+    + find_value call, including inputs that are indexed again after the
+    copy (a line longer than a chunk, a raw newline in a string, more lines
+    than the first estimate) and a result buffer that is too small."""
+    data, paths = _pipelined_case(case)
+    compiled = [gj.compile_path(p) for p in paths]
+    levels = max(c.max_depth for c in compiled)
+    f = gpjson.load_bytes(data)
+    try:
+        f.build_index(levels)
+        want = f.run(compiled)
+        lines = f.num_lines
+    finally:
+        f.release()
+    out = np.full(want.size + 10, -5, dtype=np.int64)
+    g, got = gpjson.load_bytes_query(data, levels, compiled, out=out)
+    try:
+        assert g.num_lines == lines
+        assert np.array_equal(got, want)
+        assert (out[want.size:] == -5).all()
+    finally:
+        g.release()
+    if case in ("ndjson", "small"):
+        g, got = gpjson.load_bytes_query(data, levels, compiled)  # no buffer: GPJ_ELIMIT, then gpj_query
+        try:
+            assert np.array_equal(got, want)
+        finally:
+            g.release()
+    if case == "small":
+        ref = oracle.query(data.tobytes(), paths)
+        assert np.array_equal(want, ref)
