@@ -44,34 +44,40 @@ enum LineStatus : int { kLineDone = 0, kLineDeferred = 1 };
 
 GPJ_HD bool is_ws(uint8_t c) { return c == '\n' || c == '\r' || c == '\t' || c == ' '; }
 
+// The bit helpers and the interpreter below are templates on the position
+// type P: int64_t for positions in the file, int32_t for positions relative
+// to a line's first word (run_line; half the integer work per step).
+
 // First set bit of `bm` at a position in [from, limit), or `limit`.  After
 // the first three words, four words are loaded per step (independent loads,
 // so a long jump waits for a quarter of the dependent memory round trips);
 // only words holding positions below `limit` are read.
-GPJ_HD int64_t first_of4(int64_t w, uint64_t a, uint64_t b, uint64_t c, uint64_t d, int64_t limit) {
-    int64_t base = w;
+template <typename P>
+GPJ_HD P first_of4(P w, uint64_t a, uint64_t b, uint64_t c, uint64_t d, P limit) {
+    P base = w;
     uint64_t x = a;
     if (!a) {
         base = b ? w + 1 : (c ? w + 2 : w + 3);
         x = b ? b : (c ? c : d);
     }
-    const int64_t p = (base << 6) + ctz64(x);
+    const P p = (base << 6) + ctz64(x);
     return p < limit ? p : limit;
 }
 
 // `cw`/`cv`: a word of bm the caller already holds (index, value; cw = -1
 // for none), used instead of reloading it; on return they hold the word the
 // result was found in.
-GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit, int64_t& cw, uint64_t& cv) {
+template <typename P>
+GPJ_HD P next_bit(const uint64_t* bm, P from, P limit, P& cw, uint64_t& cv) {
     if (from >= limit) return limit;
-    int64_t w = from >> 6;
-    const int64_t wend = ((limit - 1) >> 6) + 1;
+    P w = from >> 6;
+    const P wend = ((limit - 1) >> 6) + 1;
     const uint64_t first = w == cw ? cv : bm[w];
     const uint64_t m = first & (~0ull << (from & 63));
     if (m) {
         cw = w;
         cv = first;
-        const int64_t p = (w << 6) + ctz64(m);
+        const P p = (w << 6) + ctz64(m);
         return p < limit ? p : limit;
     }
     // the next two words one at a time (most jumps end there), then four per step
@@ -80,7 +86,7 @@ GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit, int64_t
         if (x) {
             cw = w;
             cv = x;
-            const int64_t p = (w << 6) + ctz64(x);
+            const P p = (w << 6) + ctz64(x);
             return p < limit ? p : limit;
         }
     }
@@ -90,7 +96,7 @@ GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit, int64_t
         const uint64_t c = w + 2 < wend ? bm[w + 2] : 0;
         const uint64_t d = w + 3 < wend ? bm[w + 3] : 0;
         if (a | b | c | d) {
-            const int64_t p = first_of4(w, a, b, c, d, limit);
+            const P p = first_of4<P>(w, a, b, c, d, limit);
             cw = w + (a ? 0 : (b ? 1 : (c ? 2 : 3)));
             cv = a ? a : (b ? b : (c ? c : d));
             return p;
@@ -99,29 +105,30 @@ GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit, int64_t
     return limit;
 }
 
-GPJ_HD int64_t next_bit(const uint64_t* bm, int64_t from, int64_t limit) {
-    int64_t cw = -1;
+template <typename P>
+GPJ_HD P next_bit(const uint64_t* bm, P from, P limit) {
+    P cw = -1;
     uint64_t cv = 0;
-    return next_bit(bm, from, limit, cw, cv);
+    return next_bit<P>(bm, from, limit, cw, cv);
 }
 
 // First position in [from, limit) set in bm and (in `filt`, or not in it
 // when `invert`), or `limit`.
-GPJ_HD int64_t next_bit_filtered(const uint64_t* bm, const uint64_t* filt, bool invert, int64_t from,
-                                 int64_t limit) {
+template <typename P>
+GPJ_HD P next_bit_filtered(const uint64_t* bm, const uint64_t* filt, bool invert, P from, P limit) {
     if (from >= limit) return limit;
-    int64_t w = from >> 6;
-    const int64_t wend = ((limit - 1) >> 6) + 1;
+    P w = from >> 6;
+    const P wend = ((limit - 1) >> 6) + 1;
     const uint64_t flip = invert ? ~0ull : 0ull;
     const uint64_t m = bm[w] & (filt[w] ^ flip) & (~0ull << (from & 63));
     if (m) {
-        const int64_t p = (w << 6) + ctz64(m);
+        const P p = (w << 6) + ctz64(m);
         return p < limit ? p : limit;
     }
     for (++w; w < wend && w < (from >> 6) + 3; ++w) {
         const uint64_t x = bm[w] & (filt[w] ^ flip);
         if (x) {
-            const int64_t p = (w << 6) + ctz64(x);
+            const P p = (w << 6) + ctz64(x);
             return p < limit ? p : limit;
         }
     }
@@ -130,20 +137,21 @@ GPJ_HD int64_t next_bit_filtered(const uint64_t* bm, const uint64_t* filt, bool 
         const uint64_t b = w + 1 < wend ? bm[w + 1] & (filt[w + 1] ^ flip) : 0;
         const uint64_t c = w + 2 < wend ? bm[w + 2] & (filt[w + 2] ^ flip) : 0;
         const uint64_t d = w + 3 < wend ? bm[w + 3] & (filt[w + 3] ^ flip) : 0;
-        if (a | b | c | d) return first_of4(w, a, b, c, d, limit);
+        if (a | b | c | d) return first_of4<P>(w, a, b, c, d, limit);
     }
     return limit;
 }
 
 // Last set bit of `bm` at a position in (floor, from], or -1; `first` is
 // bm[from >> 6] (read only when from > floor).
-GPJ_HD int64_t prev_bit(const uint64_t* bm, uint64_t first, int64_t from, int64_t floor) {
+template <typename P>
+GPJ_HD P prev_bit(const uint64_t* bm, uint64_t first, P from, P floor) {
     if (from <= floor) return -1;
-    int64_t w = from >> 6;
+    P w = from >> 6;
     uint64_t m = first & (~0ull >> (63 - (from & 63)));
     for (;;) {
         if (m) {
-            const int64_t k = (w << 6) + 63 - clz64(m);
+            const P k = (w << 6) + 63 - clz64(m);
             return k > floor ? k : -1;
         }
         if ((w << 6) <= floor + 1) return -1;
@@ -152,8 +160,9 @@ GPJ_HD int64_t prev_bit(const uint64_t* bm, uint64_t first, int64_t from, int64_
     }
 }
 
-GPJ_HD int64_t prev_bit(const uint64_t* bm, int64_t from, int64_t floor) {
-    return from <= floor ? -1 : prev_bit(bm, bm[from >> 6], from, floor);
+template <typename P>
+GPJ_HD P prev_bit(const uint64_t* bm, P from, P floor) {
+    return from <= floor ? -1 : prev_bit<P>(bm, bm[from >> 6], from, floor);
 }
 
 GPJ_HD uint32_t read_varint(const uint8_t* ir, int& pc) {
@@ -171,22 +180,25 @@ GPJ_HD uint32_t read_varint(const uint8_t* ir, int& pc) {
 // entered at level k, -1 unknown) and current_index[k] (the array element
 // counter, -1 before the array's '[' is reached).
 //
-// In registers/local memory, for every level a query may reach.
-struct LocalLevels {
-    int64_t ends[kLevelSlots];
-    int64_t index[kLevelSlots];
-    GPJ_HD void reset(int64_t line_end) {
+// In registers/local memory, for every level a query may reach, in the
+// interpreter's position type P.
+template <typename P>
+struct LocalLevelsT {
+    P ends[kLevelSlots];
+    P index[kLevelSlots];
+    GPJ_HD void reset(P line_end) {
         ends[0] = line_end;
 #pragma unroll
         for (int k = 1; k < kLevelSlots; k++) ends[k] = -1;
 #pragma unroll
         for (int k = 0; k < kLevelSlots; k++) index[k] = -1;
     }
-    GPJ_HD int64_t end(int k) const { return ends[k]; }
-    GPJ_HD void set_end(int k, int64_t v) { ends[k] = v; }
-    GPJ_HD int64_t idx(int k) const { return index[k]; }
-    GPJ_HD void set_idx(int k, int64_t v) { index[k] = v; }
+    GPJ_HD P end(int k) const { return ends[k]; }
+    GPJ_HD void set_end(int k, P v) { ends[k] = v; }
+    GPJ_HD P idx(int k) const { return index[k]; }
+    GPJ_HD void set_idx(int k, P v) { index[k] = v; }
 };
+using LocalLevels = LocalLevelsT<int64_t>;
 
 // In caller-provided storage (e.g. shared memory, entries `stride` apart),
 // as 32-bit offsets from the line start: for lines shorter than 2 GiB and
@@ -215,29 +227,30 @@ struct PackedLevels {
 // Runs validated bytecode `ir` on the line [line_start, line_end) and writes
 // (start, end) pairs to res[2*k], res[2*k+1] for the k-th STORE_RESULT.
 // res must hold -1 on entry.  Returns kLineDeferred when the view ends
-// before the line's evaluation does.  `lv` holds the per-level state.
-template <typename Levels>
-GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
-                         int64_t* res, Levels& lv) {
+// before the line's evaluation does (`skip_end`: what a whitespace skip that
+// reaches `hi` returns).  Positions are of type P and relative to `base`
+// (added to the stored results); `file`, `string_index`, `levels` and
+// `colon` are rebased to match.  `lv` holds the per-level state.
+template <typename P, typename Levels>
+GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uint64_t* string_index,
+                         const uint64_t* levels, int64_t level_size, const uint64_t* colon, P line_start,
+                         P line_end, const uint8_t* ir, int64_t* res, int64_t base, Levels& lv) {
     lv.reset(line_end);
 
-    const uint8_t* file = v.file;
-    const int64_t n = v.n;
-    const int64_t hi = v.hi;
-    const int skip_end = hi < n ? kLineDeferred : kLineDone;
     int pc = 0, cur = 0, result_index = 0;
     uint8_t type = 0xFF;
-    int64_t want_len = 0, want_index = -1;
+    P want_len = 0;
+    int64_t want_index = -1;
     const uint8_t* want = nullptr;
     bool execute = true;
 
-    int64_t j = line_start;
+    P j = line_start;
     // the search state: j came from next_bit (so it is a structural bit of
     // level cur), and the bitmap word next_bit found it in
     bool found = false;
-    int64_t cw = -1;
+    P cw = -1;
     uint64_t cv = 0;
-    int64_t cend = lv.end(cur);  // lv.end(cur), kept while searching (only opcodes change it)
+    P cend = lv.end(cur);  // lv.end(cur), kept while searching (only opcodes change it)
     while (j < cend && j < n) {
         const bool ran = execute;
         while (execute) {
@@ -245,13 +258,15 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
             switch (type) {
                 case 0:  // END
                     return kLineDone;
-                case 1:  // STORE_RESULT (find_value.cu:59-82)
+                case 1: {  // STORE_RESULT (find_value.cu:59-82)
                     while (j < hi && is_ws(file[j])) ++j;  // [bounded] stops at end of file
                     if (j >= hi && skip_end) return kLineDeferred;
-                    res[2 * result_index] = j;
-                    res[2 * result_index + 1] = lv.end(cur);
+                    const P e = lv.end(cur);
+                    res[2 * result_index] = base + j;
+                    res[2 * result_index + 1] = e < 0 ? -1 : base + e;
                     ++result_index;
                     break;
+                }
                 case 2:  // MOVE_UP (:83-90)
                     if (lv.end(cur) < 0) return kLineDone;  // [bounded] would continue at j=-1
                     j = lv.end(cur);
@@ -261,14 +276,14 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
                 case 3: {  // MOVE_DOWN (:91-111): end of the value = next structural one level up
                     ++cur;
                     if (lv.end(cur) == -1) {
-                        const int64_t lim = lv.end(cur - 1);
-                        const int64_t m = next_bit(v.levels + v.level_size * (cur - 1), j + 1, lim);
+                        const P lim = lv.end(cur - 1);
+                        const P m = next_bit<P>(levels + level_size * (cur - 1), j + 1, lim);
                         if (m < lim) lv.set_end(cur, m);
                     }
                     break;
                 }
                 case 4:  // MOVE_TO_KEY (:112-130)
-                    want_len = read_varint(ir, pc);
+                    want_len = static_cast<P>(read_varint(ir, pc));
                     want = ir + pc;
                     pc += static_cast<int>(want_len);
                     execute = false;
@@ -293,13 +308,13 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
                     }
                     break;
                 case 6: {  // EXPRESSION_STRING_EQUALS (:170-210)
-                    want_len = read_varint(ir, pc);
+                    want_len = static_cast<P>(read_varint(ir, pc));
                     want = ir + pc;
                     pc += static_cast<int>(want_len);
                     while (j < hi && is_ws(file[j])) ++j;  // [bounded]
                     if (j >= hi && skip_end) return kLineDeferred;
                     if (lv.end(cur) - j != want_len) return kLineDone;
-                    for (int64_t k = 0; k < want_len; k++)
+                    for (P k = 0; k < want_len; k++)
                         if (want[k] != file[j + k]) return kLineDone;
                     break;
                 }
@@ -311,7 +326,7 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
 
         // Searching: j is a candidate position ([bounded] only inside the file).
         if (j < hi) {
-            const uint64_t* bits = v.levels + v.level_size * cur;
+            const uint64_t* bits = levels + level_size * cur;
             const bool structural = found || ((bits[j >> 6] >> (j & 63)) & 1u);
             const uint8_t at = file[j];
             if (type == 4) {  // key match at a structural ':' (:225-251)
@@ -319,16 +334,16 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
                 // the string-index word before j, and the byte where the key's
                 // opening quote is when the key ends right before the ':'
                 // (the usual layout), checked against the real position below.
-                const uint64_t sw = j > line_start ? v.string_index[(j - 1) >> 6] : 0;
-                const int64_t guess = j - 2 - want_len;
+                const uint64_t sw = j > line_start ? string_index[(j - 1) >> 6] : 0;
+                const int64_t guess = static_cast<int64_t>(j) - 2 - want_len;
                 const uint8_t at_guess = guess >= line_start ? file[guess] : 0;
                 if (structural && at == ':') {
-                    const int64_t string_end = prev_bit(v.string_index, sw, j - 1, line_start);
-                    const int64_t string_start = string_end - want_len;
+                    const P string_end = prev_bit<P>(string_index, sw, j - 1, line_start);
+                    const int64_t string_start = static_cast<int64_t>(string_end) - want_len;
                     if (string_start >= line_start &&
                         (string_start == guess ? at_guess : file[string_start]) == '"') {
                         bool same = true;
-                        for (int64_t k = 0; k < want_len; k++) {
+                        for (P k = 0; k < want_len; k++) {
                             if (want[k] != file[string_start + k + 1]) {
                                 same = false;
                                 break;
@@ -339,7 +354,7 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
                 }
             } else if (type == 5) {  // index match at a structural ',' (:252-259)
                 if (structural && at == ',') {
-                    const int64_t count = lv.idx(cur) + 1;
+                    const P count = lv.idx(cur) + 1;
                     lv.set_idx(cur, count);
                     if (want_index == count) execute = true;
                 }
@@ -349,12 +364,12 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
         found = false;
         if (!execute) {
             // Nothing happens until the next structural bit of this level.
-            const int64_t lim = cend < n ? cend : n;
+            const P lim = cend < n ? cend : n;
             if (j < lim) {
-                if (v.colon)
-                    j = next_bit_filtered(v.levels + v.level_size * cur, v.colon, type != 4, j, lim);
+                if (colon)
+                    j = next_bit_filtered<P>(levels + level_size * cur, colon, type != 4, j, lim);
                 else
-                    j = next_bit(v.levels + v.level_size * cur, j, lim, cw, cv);
+                    j = next_bit<P>(levels + level_size * cur, j, lim, cw, cv);
                 found = j < lim;
             }
         } else {
@@ -364,7 +379,41 @@ GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end
     return kLineDone;
 }
 
-GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir, int64_t* res) {
+// The interpreter on a view's positions as they are (64-bit), with the
+// per-level state in `lv` (LocalLevels, PackedLevels).
+template <typename Levels>
+GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
+                         int64_t* res, Levels& lv) {
+    return run_line_core<int64_t>(v.file, v.n, v.hi, v.hi < v.n ? kLineDeferred : kLineDone, v.string_index,
+                                  v.levels, v.level_size, v.colon, line_start, line_end, ir, res, 0, lv);
+}
+
+// Largest line-relative position the 32-bit interpreter handles.
+constexpr int64_t kRelLimit = (1ll << 31) - 4096;
+
+// run_line_with with positions relative to the line's first 64-byte word
+// in 32 bits (the usual case: half the integer work per step).  Lines whose
+// end lies more than rel_limit (<= kRelLimit) bytes past that word run in
+// 64 bits; a whitespace skip that reaches rel_limit (bytes past it exist)
+// stops there and the line is evaluated again in 64 bits from -1 results
+// (res_len entries).
+GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir, int64_t* res,
+                    int64_t res_len, int64_t rel_limit = kRelLimit) {
+    const int64_t base = line_start & ~static_cast<int64_t>(63);
+    if (line_end - base <= rel_limit) {
+        const bool clamped = v.hi - base > rel_limit;
+        const int32_t hi = static_cast<int32_t>(clamped ? rel_limit : v.hi - base);
+        const int32_t n = static_cast<int32_t>(v.n - base > rel_limit ? rel_limit : v.n - base);
+        const int skip_end = clamped || v.hi < v.n ? kLineDeferred : kLineDone;
+        const int64_t w = base >> 6;
+        LocalLevelsT<int32_t> lv;
+        const int r = run_line_core<int32_t>(v.file + base, n, hi, skip_end, v.string_index + w, v.levels + w,
+                                             v.level_size, v.colon ? v.colon + w : nullptr,
+                                             static_cast<int32_t>(line_start - base),
+                                             static_cast<int32_t>(line_end - base), ir, res, base, lv);
+        if (r != kLineDeferred || !clamped || v.hi < v.n) return r;
+        for (int64_t k = 0; k < res_len; k++) res[k] = -1;
+    }
     LocalLevels lv;
     return run_line_with(v, line_start, line_end, ir, res, lv);
 }

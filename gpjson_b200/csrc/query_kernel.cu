@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
         const int64_t end = to_eof ? p.n : p.newlines[i + 1];
         int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + i) * per_line;
         for (int64_t k = 0; k < per_line; k++) res[k] = -1;
-        run_line(view, start, end, p.bytecode + p.offsets[q], res);
+        run_line(view, start, end, p.bytecode + p.offsets[q], res, per_line);
     }
 }
 
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(256) find_value_batch_kernel(const QueryFile* 
         const int64_t per_line = 2 * static_cast<int64_t>(F.slots);
         int64_t* res = F.out + (q * F.out_lines + i) * per_line;
         for (int64_t r = 0; r < per_line; r++) res[r] = -1;
-        run_line(view, start, end, F.bytecode + F.offsets[q], res);
+        run_line(view, start, end, F.bytecode + F.offsets[q], res, per_line);
     }
 }
 

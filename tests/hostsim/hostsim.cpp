@@ -187,8 +187,9 @@ int64_t hs_build_index_lines(const uint8_t* f, int64_t n, int num_levels, uint64
 // Runs each query's bytecode on every line with the device interpreter.
 // out: [nq][lines][slots][2], filled with -1 here.  `colon` (may be null)
 // is the bitmap of ':' outside strings that the fused kernel's key searches
-// jump along; `packed` selects the 32-bit level state the fused kernel keeps
-// in shared memory.
+// jump along; `packed` = 1 selects the 32-bit level state the fused kernel
+// keeps in shared memory, 2 the line-relative 32-bit interpreter with a
+// 64-byte limit (so that its 64-bit fallbacks run).
 void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t lines,
                     const uint64_t* str, const uint64_t* lvl, int nq, const uint8_t* const* irs,
                     int slots, int64_t* out, const uint64_t* colon, int packed) {
@@ -205,7 +206,7 @@ void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t line
                 PackedLevels lv{ends, index, 1, kLevelSlots, start};
                 run_line_with(v, start, end, irs[q], res, lv);
             } else {
-                run_line(v, start, end, irs[q], res);
+                run_line(v, start, end, irs[q], res, slots * 2, packed == 2 ? 64 : kRelLimit);
             }
         }
     }
