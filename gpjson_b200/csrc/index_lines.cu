@@ -166,43 +166,42 @@ struct SlotInfo {
     int byte_slot;
 };
 
-// Summary of a word for the tile scan: the Span arithmetic of word_ops.cuh
-// plus a reset at newlines.  A word holding a '\n' starts a line there; in
-// NDJSON every line starts outside strings at level -1, so the state after
-// such a word is known absolutely from its bytes past its first '\n'
-// (reset = 1, d0 = the level after the word).  Otherwise (reset = 0) d0 and
-// dt are the relative level changes of Span.  The exclusive scan of a word
-// then says whether a line starts before it in the tile (reset set) and, if
-// so, its state: composing from the last reset is exact because the kernel
-// checks the state at every later '\n' (a mismatch sends the input to the
-// exact kernel).  nl counts newlines.
-struct RSpan {
-    int32_t rq;  // 2 * reset + quote parity
-    int32_t d0;
-    int32_t dt;
-    int32_t nl;
+// The tile scan.  A word holding a '\n' starts a line there; in NDJSON
+// every line starts outside strings at level -1, so the state after such a
+// word is known absolutely from its bytes past its first '\n' (a reset).
+// Any other word changes the state relatively: it flips the string state
+// with its quote parity and changes the level by d_out when entered outside
+// a string, by d_in when entered inside (starting inside a string flips
+// every in-string bit of the word; the Span arithmetic of word_ops.cuh).  A
+// word's state is that of the last reset before it in the tile carried over
+// the words between; composing from the last reset is exact because the
+// kernel checks the state at every later '\n' (a mismatch sends the input to
+// the exact kernel).
+//
+// Within a warp the string states come from two ballots (resets, parities)
+// and a popcount, and the levels from one shuffle prefix sum carrying both
+// variants (entered outside / inside) as biased 16-bit halves; the eight
+// warp summaries are combined the same way in the first nine lanes of every
+// warp (lane 8 = the state after the whole slot).
+struct WarpSum {
+    int32_t reset;  // a line of the tile starts in the warp
+    int32_t s;      // reset: string state after the warp; else: its quote parity
+    int32_t d_out;  // reset: level after the warp; else: level change when entered outside a string
+    int32_t d_in;   // no reset: level change when entered inside a string
+    int32_t nl;     // newlines: of tile words in the low 16 bits, of look-ahead words above
 };
 
-__device__ __forceinline__ RSpan rspan_compose(const RSpan& a, const RSpan& b) {
-    const int aq = a.rq & 1;
-    RSpan r;
-    r.nl = a.nl + b.nl;
-    if (b.rq & 2) {
-        r.rq = b.rq;
-        r.d0 = b.d0;
-        r.dt = 0;
-    } else {
-        r.rq = (a.rq & 2) | (aq ^ (b.rq & 1));
-        r.d0 = a.d0 + (aq ? b.dt - b.d0 : b.d0);
-        r.dt = (a.rq & 2) ? 0 : a.dt + b.dt;
-    }
-    return r;
-}
-
-__device__ __forceinline__ RSpan shfl_rspan_up(const RSpan& v, int off) {
-    return RSpan{__shfl_up_sync(~0u, v.rq, off), __shfl_up_sync(~0u, v.d0, off), __shfl_up_sync(~0u, v.dt, off),
-                 __shfl_up_sync(~0u, v.nl, off)};
-}
+// A word's state at its first byte, and the slot's totals.
+struct TileScan {
+    int reset;       // a line of the tile starts before the word (s, d valid)
+    int s;           // in a string
+    int d;           // level
+    int nl_before;   // newlines before the word (tile words low 16 bits, look-ahead above)
+    int lines_here;  // a line starts in the tile
+    int s_end;       // state after the slot's last word
+    int d_end;
+    int nl_total;    // newlines of the slot, as nl_before
+};
 
 template <int LV>
 struct FShared {
@@ -226,7 +225,7 @@ struct FShared {
     uint64_t mready[kMaskSlots];
     uint64_t mfree[kMaskSlots];
     Span span_scratch[kTileWarps];
-    RSpan rscan[2][kTileWarps];  // tile scan, alternating between tiles
+    WarpSum rscan[2][kTileWarps];  // tile scan, alternating between tiles
     int carry_esc;
     int64_t first_line;  // start of the tile's first line (its first '\n')
     int64_t ext_b;       // end of the tile's last line when it ends in the look-ahead
@@ -242,7 +241,7 @@ struct TShared {
     uint64_t lvacc[kTileWarps][LV][32];
     uint64_t full[kRing];
     Span span_scratch[kTileWarps];
-    RSpan rscan[2][kTileWarps];
+    WarpSum rscan[2][kTileWarps];
     int carry_esc;
     int64_t first_line;
     int64_t ext_b;
@@ -273,35 +272,113 @@ __device__ __forceinline__ Span index_scan_span(Span mine, Span* scratch, Span* 
     return span_compose(prefix, excl);
 }
 
-// Exclusive RSpan scan over the 256 index threads, in word order; one
-// named barrier.  `scratch` must not be reused by the next tile (the caller
-// alternates two).
-__device__ __forceinline__ RSpan index_scan_rspan(RSpan mine, RSpan* scratch, RSpan* total) {
+// The tile scan over the 256 index threads in word order (see WarpSum);
+// one named barrier.  Per word: reset_w (a tile line starts in it), q (its
+// string state after the reset, else its quote parity), d_abs (reset: level
+// after it), d_out / d_in (no reset: level change entered outside / inside a
+// string), nl (as WarpSum::nl).  `sums` (kTileWarps entries) must not be
+// reused by the next tile (the caller alternates two).  `start_reset`: a
+// line starts at the slot's first byte (the file's first tile).
+__device__ __forceinline__ TileScan tile_scan(bool reset_w, int q, int d_abs, int d_out, int d_in, int nl,
+                                              bool start_reset, WarpSum* sums) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    RSpan incl = mine;
+    const unsigned lt = (1u << lane) - 1;
+    // ---- within the warp
+    const unsigned b_reset = __ballot_sync(~0u, reset_w);
+    const unsigned b_q = __ballot_sync(~0u, q != 0);
+    const unsigned before = b_reset & lt;
+    const int r = before ? 31 - __clz(before) : 0;  // the last reset lane before this one
+    const int s_loc = __popc(b_q & (before ? lt & ~((1u << r) - 1) : lt)) & 1;
+    // this word's level change for the words after it, the warp entered outside (a) / inside (b) a string
+    int da = 0, db = 0;
+    if (!reset_w) {
+        da = s_loc ? d_in : d_out;
+        db = before ? da : (s_loc ? d_out : d_in);
+    }
+    const uint32_t mine = static_cast<uint32_t>(da + 64) | (static_cast<uint32_t>(db + 64) << 16);
+    uint32_t incl = mine;
+    int nl_incl = nl;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
-        const RSpan o = shfl_rspan_up(incl, off);
-        if (lane >= off) incl = rspan_compose(o, incl);
+        const uint32_t o = __shfl_up_sync(~0u, incl, off);
+        const int on = __shfl_up_sync(~0u, nl_incl, off);
+        if (lane >= off) {
+            incl += o;
+            nl_incl += on;
+        }
     }
-    if (lane == 31) scratch[warp] = incl;
-    RSpan excl = shfl_rspan_up(incl, 1);
-    if (lane == 0) excl = RSpan{0, 0, 0, 0};
+    const uint32_t excl = incl - mine;
+    const int ea = static_cast<int>(excl & 0xFFFF) - 64 * lane;
+    const int eb = static_cast<int>(excl >> 16) - 64 * lane;
+    const int a_r = __shfl_sync(~0u, d_abs, r);
+    const int pa_r = static_cast<int>(__shfl_sync(~0u, incl, r) & 0xFFFF) - 64 * (r + 1);
+    // the warp's summary
+    const uint32_t all = __shfl_sync(~0u, incl, 31);
+    const int last = b_reset ? 31 - __clz(b_reset) : 0;
+    const int a_last = __shfl_sync(~0u, d_abs, last);
+    const int pa_last = static_cast<int>(__shfl_sync(~0u, incl, last) & 0xFFFF) - 64 * (last + 1);
+    const int nl_warp = __shfl_sync(~0u, nl_incl, 31);
+    if (lane == 0) {
+        WarpSum w;
+        w.reset = b_reset != 0;
+        w.nl = nl_warp;
+        if (b_reset) {
+            w.s = __popc(b_q & ~((1u << last) - 1)) & 1;
+            w.d_out = a_last + (static_cast<int>(all & 0xFFFF) - 64 * 32) - pa_last;
+            w.d_in = w.d_out;
+        } else {
+            w.s = __popc(b_q) & 1;
+            w.d_out = static_cast<int>(all & 0xFFFF) - 64 * 32;
+            w.d_in = static_cast<int>(all >> 16) - 64 * 32;
+        }
+        sums[warp] = w;
+    }
     group_sync(kBarIndex, kIndexThreads);
-    // every warp scans the eight warp totals in its first eight lanes
-    RSpan wv = lane < kTileWarps ? scratch[lane] : RSpan{0, 0, 0, 0};
+    // ---- across the warps: lane w < 8 holds warp w's summary, lane 8 an empty one
+    WarpSum w{0, 0, 0, 0, 0};
+    if (lane < kTileWarps) w = sums[lane];
+    const unsigned c_reset = __ballot_sync(~0u, w.reset != 0);
+    const unsigned c_q = __ballot_sync(~0u, w.s != 0);
+    const unsigned cb = c_reset & lt;
+    const int cr = cb ? 31 - __clz(cb) : 0;
+    // state at the start of warp `lane`: from its last reset warp, else from the slot start
+    const int cs = __popc(c_q & (cb ? lt & ~((1u << cr) - 1) : lt)) & 1;
+    const int cdelta = w.reset ? 0 : (cs ? w.d_in : w.d_out);
+    int cincl = cdelta, cnl = w.nl;
 #pragma unroll
-    for (int off = 1; off < kTileWarps; off <<= 1) {
-        const RSpan o = shfl_rspan_up(wv, off);
-        if (lane >= off) wv = rspan_compose(o, wv);
+    for (int off = 1; off <= kTileWarps; off <<= 1) {
+        const int o = __shfl_up_sync(~0u, cincl, off);
+        const int on = __shfl_up_sync(~0u, cnl, off);
+        if (lane >= off) {
+            cincl += o;
+            cnl += on;
+        }
     }
-    *total = RSpan{__shfl_sync(~0u, wv.rq, kTileWarps - 1), __shfl_sync(~0u, wv.d0, kTileWarps - 1),
-                   __shfl_sync(~0u, wv.dt, kTileWarps - 1), __shfl_sync(~0u, wv.nl, kTileWarps - 1)};
-    const int src = warp > 0 ? warp - 1 : 0;
-    RSpan prefix{__shfl_sync(~0u, wv.rq, src), __shfl_sync(~0u, wv.d0, src), __shfl_sync(~0u, wv.dt, src),
-                 __shfl_sync(~0u, wv.nl, src)};
-    if (warp == 0) prefix = RSpan{0, 0, 0, 0};
-    return rspan_compose(prefix, excl);
+    const int c_abs = __shfl_sync(~0u, w.d_out, cr);
+    const int c_incl_r = __shfl_sync(~0u, cincl, cr);
+    const int c_has = (cb != 0 || start_reset) ? 1 : 0;
+    const int cd = cb ? c_abs + (cincl - cdelta) - c_incl_r : (start_reset ? -1 : 0) + (cincl - cdelta);
+    const int cnl_excl = cnl - w.nl;
+    const int in_has = __shfl_sync(~0u, c_has, warp);
+    const int in_s = __shfl_sync(~0u, cs, warp);
+    const int in_d = __shfl_sync(~0u, cd, warp);
+    const int in_nl = __shfl_sync(~0u, cnl_excl, warp);
+    TileScan out;
+    if (before) {
+        out.reset = 1;
+        out.s = s_loc;
+        out.d = a_r + ea - pa_r;
+    } else {
+        out.reset = in_has;
+        out.s = in_s ^ s_loc;
+        out.d = in_d + (in_s ? eb : ea);
+    }
+    out.nl_before = in_nl + (nl_incl - nl);
+    out.lines_here = __shfl_sync(~0u, c_has, kTileWarps);
+    out.s_end = __shfl_sync(~0u, cs, kTileWarps);
+    out.d_end = __shfl_sync(~0u, cd, kTileWarps);
+    out.nl_total = __shfl_sync(~0u, cnl_excl, kTileWarps);
+    return out;
 }
 
 // Issues the TMA load of [start, start + bytes) into `dst` on `bar` (one thread).
@@ -600,29 +677,24 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
         const uint64_t after = has_nl ? (f == 63 ? 0ull : (~0ull << (f + 1))) : ~0ull;
         // in-string bits past the first '\n' when a line starts there
         const uint64_t pa = (p0 ^ (((p0 >> f) & 1ull) ? ~0ull : 0ull)) & after;
-        RSpan mine;
-        // newlines of the tile count in the low 16 bits, of the look-ahead above
-        mine.nl = ahead ? (popc64(m.newline) << 16) : popc64(m.newline);
-        if (has_nl && !ahead) {  // only the tile's own newlines start lines here
-            mine.rq = 2 | (popc64(quotes & after) & 1);
-            mine.d0 = -1 + popc64(m.open & after & ~pa) - popc64(m.close & after & ~pa);
-            mine.dt = 0;
+        const bool reset_w = has_nl && !ahead;  // only the tile's own newlines start lines here
+        int q_w, d_abs = 0, dout_w = 0, din_w = 0;
+        if (reset_w) {
+            q_w = popc64(quotes & after) & 1;
+            d_abs = -1 + popc64(m.open & after & ~pa) - popc64(m.close & after & ~pa);
         } else {
-            mine.rq = popc64(quotes) & 1;
-            mine.d0 = popc64(m.open & ~p0) - popc64(m.close & ~p0);
-            mine.dt = popc64(m.open) - popc64(m.close);
+            q_w = popc64(quotes) & 1;
+            dout_w = popc64(m.open & ~p0) - popc64(m.close & ~p0);
+            din_w = popc64(m.open) - popc64(m.close) - dout_w;
         }
+        // newlines of the tile count in the low 16 bits, of the look-ahead above
+        const int nl_w = ahead ? (popc64(m.newline) << 16) : popc64(m.newline);
         if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(cout);
-        RSpan total;
-        RSpan ex = index_scan_rspan(mine, sh.rscan[k & 1], &total);
-        if (lt == 0) {  // the file's first line starts at byte 0
-            const RSpan init{2, -1, 0, 0};
-            ex = rspan_compose(init, ex);
-            total = rspan_compose(init, total);
-        }
-        const int tile_nl = total.nl & 0xFFFF;
-        const int ahead_nl = total.nl >> 16;
-        const bool lines_here = (total.rq & 2) != 0;  // a line starts in this tile
+        // the file's first line starts at byte 0
+        const TileScan sc = tile_scan(reset_w, q_w, d_abs, dout_w, din_w, nl_w, lt == 0, sh.rscan[k & 1]);
+        const int tile_nl = sc.nl_total & 0xFFFF;
+        const int ahead_nl = sc.nl_total >> 16;
+        const bool lines_here = sc.lines_here != 0;  // a line starts in this tile
         if constexpr (kLines) {
             if (tid == 0) st_release(nl_agg + t, tag48(p.epoch, static_cast<unsigned long long>(tile_nl)));
             // the mask slot was last used two tiles ago
@@ -636,11 +708,11 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
         bool act = false, own = true;
         ClassMasks wm = m;
         uint64_t wp0 = p0, check = 0;
-        int ws_in = ex.rq & 1;
-        int64_t wd_in = ex.d0;
+        int ws_in = sc.s;
+        int64_t wd_in = sc.d;
         if (!ahead) {
             if constexpr (kLines) {
-                const int excl = ex.nl & 0xFFFF;
+                const int excl = sc.nl_before & 0xFFFF;
                 sh.nlmask[ms][tid] = m.newline;
                 sh.nlexcl[ms][tid] = excl;
                 uint64_t nm = m.newline;
@@ -652,7 +724,7 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
             } else {
                 if (ws < tile_end) F.newline_bits[ws >> 6] = m.newline;
             }
-            if (ex.rq & 2) {
+            if (sc.reset) {
                 // every byte of the word belongs to lines that start in this tile
                 act = ws < tile_end;
                 check = m.newline;
@@ -667,7 +739,7 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                 wd_in = -1;
                 check = m.newline & after;
             }
-        } else if (lines_here && (ex.nl >> 16) == 0 && valid) {
+        } else if (lines_here && (sc.nl_before >> 16) == 0 && valid) {
             // No '\n' between the tile end and this word: the tile's last line
             // runs into it.  The line ends at this word's first '\n' (the only
             // one checked here); a word that starts with it belongs to the next tile.
@@ -690,8 +762,8 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
             } else {
                 // a line longer than the look-ahead: continue past the slot
                 // straight from device memory
-                const int s_in = total.rq & 1;
-                const int64_t d_in = total.d0;
+                const int s_in = sc.s_end;
+                const int64_t d_in = sc.d_end;
                 const int esc_in = sh.carry_esc;
                 if (tid < 32) {
                     const int64_t e2 = find_line_end(F, loaded_end, tile_end);
