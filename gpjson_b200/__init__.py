@@ -182,6 +182,78 @@ class Result(Sequence):
         return ResultArray(self.offsets[q], self.file_bytes)
 
 
+VALUE_NULL, VALUE_PRESENT, VALUE_UNREADABLE = 0, 1, 2
+
+
+class Values(Sequence):
+    """Values gathered on the device (gpj_query_values): [query][line][slot]
+    -> str | None with ResultItem's semantics (result/ResultItem.java:32-52),
+    read from one compact buffer instead of the file.  ``kinds`` is uint8
+    [queries][lines][slots] (VALUE_*), ``offsets`` int64 [items + 1] into
+    ``data``."""
+
+    def __init__(self, kinds: np.ndarray, offsets: np.ndarray, data: bytes, paths: list[str]):
+        self.kinds = kinds
+        self.offsets = offsets
+        self.data = data
+        self.paths = paths
+
+    def __len__(self) -> int:
+        return self.kinds.shape[0]
+
+    def value(self, q: int, line: int, slot: int):
+        kind = int(self.kinds[q, line, slot])
+        if kind == VALUE_NULL:
+            return None
+        if kind == VALUE_UNREADABLE:
+            raise GPJSONException(f"result of query {q}, line {line}, slot {slot} has no end offset")
+        i = (q * self.kinds.shape[1] + line) * self.kinds.shape[2] + slot
+        return self.data[int(self.offsets[i]):int(self.offsets[i + 1])].decode("utf-8", "replace")
+
+    def __getitem__(self, q):
+        if isinstance(q, slice):
+            return [self[i] for i in range(*q.indices(len(self)))]
+        if q < 0:
+            q += len(self)
+        if not 0 <= q < len(self):
+            raise IndexError(q)
+        return _ValuesArray(self, q)
+
+
+class _ValuesArray(Sequence):
+    def __init__(self, values: Values, q: int):
+        self._v, self._q = values, q
+
+    def __len__(self) -> int:
+        return self._v.kinds.shape[1]
+
+    def __getitem__(self, line):
+        if isinstance(line, slice):
+            return [self[i] for i in range(*line.indices(len(self)))]
+        if line < 0:
+            line += len(self)
+        if not 0 <= line < len(self):
+            raise IndexError(line)
+        return _ValuesItem(self._v, self._q, line)
+
+
+class _ValuesItem(Sequence):
+    def __init__(self, values: Values, q: int, line: int):
+        self._v, self._q, self._line = values, q, line
+
+    def __len__(self) -> int:
+        return self._v.kinds.shape[2]
+
+    def __getitem__(self, slot):
+        if isinstance(slot, slice):
+            return [self[i] for i in range(*slot.indices(len(self)))]
+        if slot < 0:
+            slot += len(self)
+        if not 0 <= slot < len(self):
+            raise IndexError(slot)
+        return self._v.value(self._q, self._line, slot)
+
+
 def prepare_queries(queries, options=None) -> tuple[list[str], list[CompiledQuery]]:
     """Argument handling and compilation of QueryFunction.call
     (QueryFunction.java:64-136): a path or a list of 1..255 paths, an
@@ -327,6 +399,26 @@ class File:
             return np.array(buf, dtype=np.int64, copy=True).reshape(nq, lines, slots, 2)
         finally:
             lib.gpj_result_release(r)
+
+    def query_values(self, paths: list[str]) -> Values:
+        """gpj_query_values: the paths evaluated as by query_paths and the
+        matched values gathered on the device (no host read of the file)."""
+        arr = (c_char_p * len(paths))(*[p.encode("utf-8") for p in paths])
+        v = c_void_p()
+        self._native.check(self._native.lib.gpj_query_values(self._native.h, self._h, len(paths), arr, byref(v)))
+        lib = self._native.lib
+        try:
+            nq, lines, slots = lib.gpj_values_num_queries(v), lib.gpj_values_num_lines(v), lib.gpj_values_slots(v)
+            items = nq * lines * slots
+            kinds = np.zeros(items, dtype=np.uint8)
+            if items:
+                kinds[:] = np.ctypeslib.as_array((ctypes.c_uint8 * items).from_address(lib.gpj_values_kinds(v)))
+            offsets = np.ctypeslib.as_array((ctypes.c_int64 * (items + 1)).from_address(lib.gpj_values_offsets(v)))
+            size = lib.gpj_values_size(v)
+            data = ctypes.string_at(lib.gpj_values_bytes(v), size) if size else b""
+            return Values(kinds.reshape(nq, lines, slots), offsets.copy(), data, list(paths))
+        finally:
+            lib.gpj_values_release(v)
 
     def index_and_query_device(self, queries: list[CompiledQuery], num_levels: int, d_out: int, out_lines: int,
                                slots: int | None = None) -> None:
@@ -490,6 +582,17 @@ class GPJSON:
             size = os.fstat(fh.fileno()).st_size
             file_bytes = mmap.mmap(fh.fileno(), 0, access=mmap.ACCESS_READ) if size else b""
         return Result(offsets, file_bytes, paths)
+
+    def query_values(self, filename, queries, options=None) -> Values:
+        """query() with the matched values gathered on the device
+        (gpj_query_values): the same [query][line][slot] -> str | None view,
+        without reading the file again on the host."""
+        paths, _ = prepare_queries(queries, options)
+        f = self.open(filename)
+        try:
+            return f.query_values(paths)
+        finally:
+            f.release()
 
     def exportTimings(self) -> str:  # noqa: N802  (reference member name)
         """ExportTimingsFunction: the context's phase timings as JSON."""

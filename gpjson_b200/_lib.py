@@ -87,6 +87,18 @@ SIGNATURES: dict[str, tuple] = {
     "gpj_result_slots": (c_int, [c_void_p]),
     "gpj_result_offsets": (c_void_p, [c_void_p]),
     "gpj_result_release": (None, [c_void_p]),
+    "gpj_values_device": (
+        c_int, [c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)]
+    ),
+    "gpj_query_values": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_char_p), POINTER(c_void_p)]),
+    "gpj_values_num_queries": (c_int64, [c_void_p]),
+    "gpj_values_num_lines": (c_int64, [c_void_p]),
+    "gpj_values_slots": (c_int, [c_void_p]),
+    "gpj_values_kinds": (c_void_p, [c_void_p]),
+    "gpj_values_offsets": (c_void_p, [c_void_p]),
+    "gpj_values_bytes": (c_void_p, [c_void_p]),
+    "gpj_values_size": (c_int64, [c_void_p]),
+    "gpj_values_release": (None, [c_void_p]),
     "gpj_get_timings": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
     "gpj_reset_timings": (None, [c_void_p]),
     "gpj_kernel_launches": (c_int64, [c_void_p]),

@@ -19,6 +19,7 @@
 #include "index_kernel.h"
 #include "jsonpath.h"
 #include "query_kernel.h"
+#include "values.h"
 
 namespace {
 
@@ -97,6 +98,15 @@ struct gpj_result {
     int64_t nq = 0, lines = 0;
     int slots = 0;
     std::vector<int64_t> offsets;
+};
+
+// Values of a query call gathered on the device (gpj_query_values).
+struct gpj_values {
+    int64_t nq = 0, lines = 0;
+    int slots = 0;
+    std::vector<uint8_t> kinds;     // [nq][lines][slots]
+    std::vector<int64_t> offsets;   // [nq * lines * slots + 1]
+    std::vector<uint8_t> bytes;     // offsets.back() bytes
 };
 
 // Requests (file, paths) evaluated together by gpj_batch_run.
@@ -750,6 +760,47 @@ int ensure_out(gpj_ctx* ctx, gpj_file* f, size_t elems) {
     return GPJ_OK;
 }
 
+// Value extraction over result pairs of file f (values.cu): kinds and
+// offsets, then (d_bytes_out given) a device buffer of exactly the total is
+// allocated into *d_bytes_out, else the values go into d_bytes (cap bytes;
+// null when cap is 0).  *total receives the byte total; synchronous.
+int gather_values(gpj_ctx* ctx, gpj_file* f, const int64_t* d_pairs, int64_t npairs, int64_t per_query,
+                  int64_t stride, uint8_t* d_kinds, int64_t* d_offsets, uint8_t* d_bytes, int64_t cap,
+                  uint8_t** d_bytes_out, int64_t* total) {
+    int64_t* scratch = nullptr;  // [block sums..., total]
+    const int64_t blocks = gpj::value_scan_blocks(npairs);
+    int rc = device_alloc(ctx, &scratch, static_cast<size_t>(blocks + 1), "cudaMalloc(value scan)");
+    if (rc) return rc;
+    int64_t* d_total = scratch + blocks;
+    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((npairs + 255) / 256, static_cast<int64_t>(ctx->sms) * 8));
+    auto run = [&]() -> int {
+        GPJ_CUDA(ctx, gpj::launch_value_sizes(d_pairs, npairs, std::max<int64_t>(per_query, 1), stride, f->n, d_kinds,
+                                              d_offsets, scratch, d_total, ctx->stream));
+        ctx->launches += npairs > 0 ? 2 : 1;
+        if (d_bytes_out) {
+            GPJ_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
+            GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            *total = static_cast<int64_t>(ctx->h_status[0]);
+            int r = device_alloc(ctx, d_bytes_out, static_cast<size_t>(std::max<int64_t>(*total, 1)),
+                                 "cudaMalloc(values)");
+            if (r) return r;
+            d_bytes = *d_bytes_out;
+            cap = *total;
+        }
+        GPJ_CUDA(ctx, gpj::launch_value_copy(f->d_data, d_pairs, npairs, std::max<int64_t>(per_query, 1), stride,
+                                             d_kinds, d_offsets, scratch, d_total, d_bytes, cap, static_cast<int>(grid),
+                                             ctx->stream));
+        ctx->launches++;
+        GPJ_CUDA(ctx, cudaMemcpyAsync(ctx->h_status, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
+        GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        *total = static_cast<int64_t>(ctx->h_status[0]);
+        return GPJ_OK;
+    };
+    rc = run();
+    device_free(ctx, scratch);
+    return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1230,10 +1281,12 @@ int gpj_index_query_device(gpj_ctx* ctx, gpj_file* f, int num_levels, int nq, co
     return index_and_query(ctx, f, num_levels, nq, bc, len, slots, d_out, out_lines, nullptr);
 }
 
-int gpj_query_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths, gpj_result** out) {
+// gpj_query_paths up to the results in f->d_out: [nq][*cap][*slots][2].
+static int run_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths, int* slots_out,
+                     int64_t* cap_out) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!f || !paths || !out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (!f || !paths) return fail(ctx, GPJ_EINVAL, "bad arguments");
     if (nq > GPJ_MAX_QUERIES) return fail(ctx, GPJ_ELIMIT, "Maximum size of queries is 255");
     if (nq < 1) return fail(ctx, GPJ_EINVAL, "expected queries to contain at least one query");
     std::vector<gpj::CompiledPath> compiled(static_cast<size_t>(nq));
@@ -1272,6 +1325,19 @@ int gpj_query_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths,
         break;
     }
     if (rc) return rc;
+    *slots_out = slots;
+    *cap_out = cap;
+    return GPJ_OK;
+}
+
+int gpj_query_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths, gpj_result** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    int slots = 0;
+    int64_t cap = 0;
+    rc = run_paths(ctx, f, nq, paths, &slots, &cap);
+    if (rc) return rc;
     gpj_result* r = new (std::nothrow) gpj_result;
     if (!r) return fail(ctx, GPJ_ENOMEM, "out of host memory");
     r->nq = nq;
@@ -1308,6 +1374,91 @@ int64_t gpj_result_num_lines(const gpj_result* r) { return r ? r->lines : -1; }
 int gpj_result_slots(const gpj_result* r) { return r ? r->slots : -1; }
 const int64_t* gpj_result_offsets(const gpj_result* r) { return r ? r->offsets.data() : nullptr; }
 void gpj_result_release(gpj_result* r) { delete r; }
+
+int gpj_values_device(gpj_ctx* ctx, gpj_file* f, const int64_t* d_pairs, int64_t npairs, uint8_t* d_kinds,
+                      int64_t* d_offsets, uint8_t* d_bytes, int64_t bytes_cap, int64_t* total_bytes) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!f || npairs < 0 || (npairs > 0 && (!d_pairs || !d_kinds)) || !d_offsets || bytes_cap < 0 ||
+        (bytes_cap > 0 && !d_bytes) || !total_bytes)
+        return fail(ctx, GPJ_EINVAL, "bad arguments");
+    const double t0 = now_ms();
+    GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    // with bytes_cap 0 the copy kernel writes no byte, so d_bytes may be null
+    rc = gather_values(ctx, f, d_pairs, npairs, npairs, npairs, d_kinds, d_offsets, bytes_cap > 0 ? d_bytes : nullptr,
+                       bytes_cap, nullptr, total_bytes);
+    if (rc) return rc;
+    rc = end_phase(ctx, "gather_values", t0);
+    if (rc) return rc;
+    if (*total_bytes > bytes_cap)
+        return fail(ctx, GPJ_ELIMIT, "values take " + std::to_string(*total_bytes) + " bytes, the buffer holds " +
+                                         std::to_string(bytes_cap));
+    return GPJ_OK;
+}
+
+int gpj_query_values(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths, gpj_values** out) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    int slots = 0;
+    int64_t cap = 0;
+    rc = run_paths(ctx, f, nq, paths, &slots, &cap);
+    if (rc) return rc;
+    gpj_values* v = new (std::nothrow) gpj_values;
+    if (!v) return fail(ctx, GPJ_ENOMEM, "out of host memory");
+    v->nq = nq;
+    v->lines = f->num_lines;
+    v->slots = slots;
+    const int64_t per_query = f->num_lines * slots;
+    const int64_t npairs = per_query * nq;
+    uint8_t* d_kinds = nullptr;
+    int64_t* d_offsets = nullptr;
+    uint8_t* d_bytes = nullptr;
+    int64_t total = 0;
+    const double t0 = now_ms();
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    rc = device_alloc(ctx, &d_kinds, static_cast<size_t>(std::max<int64_t>(npairs, 1)), "cudaMalloc(value kinds)");
+    if (!rc) rc = device_alloc(ctx, &d_offsets, static_cast<size_t>(npairs + 1), "cudaMalloc(value offsets)");
+    if (!rc)
+        rc = gather_values(ctx, f, f->d_out, npairs, per_query, cap * slots, d_kinds, d_offsets, nullptr, 0, &d_bytes,
+                           &total);
+    if (!rc) {
+        try {
+            v->kinds.resize(static_cast<size_t>(npairs));
+            v->offsets.resize(static_cast<size_t>(npairs + 1));
+            v->bytes.resize(static_cast<size_t>(total));
+        } catch (const std::bad_alloc&) {
+            rc = fail(ctx, GPJ_ENOMEM, "out of host memory for values");
+        }
+    }
+    cudaError_t e = cudaSuccess;
+    if (!rc && npairs > 0) e = cudaMemcpyAsync(v->kinds.data(), d_kinds, npairs, cudaMemcpyDeviceToHost, ctx->stream);
+    if (!rc && e == cudaSuccess)
+        e = cudaMemcpyAsync(v->offsets.data(), d_offsets, (npairs + 1) * 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (!rc && e == cudaSuccess && total > 0)
+        e = cudaMemcpyAsync(v->bytes.data(), d_bytes, total, cudaMemcpyDeviceToHost, ctx->stream);
+    if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "copy of values");
+    device_free(ctx, d_kinds);
+    device_free(ctx, d_offsets);
+    device_free(ctx, d_bytes);
+    if (!rc) rc = end_phase(ctx, "gather_values", t0);
+    if (rc) {
+        delete v;
+        return rc;
+    }
+    *out = v;
+    return GPJ_OK;
+}
+
+int64_t gpj_values_num_queries(const gpj_values* v) { return v ? v->nq : 0; }
+int64_t gpj_values_num_lines(const gpj_values* v) { return v ? v->lines : 0; }
+int gpj_values_slots(const gpj_values* v) { return v ? v->slots : 0; }
+const uint8_t* gpj_values_kinds(const gpj_values* v) { return v ? v->kinds.data() : nullptr; }
+const int64_t* gpj_values_offsets(const gpj_values* v) { return v ? v->offsets.data() : nullptr; }
+const uint8_t* gpj_values_bytes(const gpj_values* v) { return v ? v->bytes.data() : nullptr; }
+int64_t gpj_values_size(const gpj_values* v) { return v ? static_cast<int64_t>(v->bytes.size()) : 0; }
+void gpj_values_release(gpj_values* v) { delete v; }
 
 int gpj_get_timings(gpj_ctx* ctx, char* json, size_t cap, size_t* len) {
     if (!ctx) return GPJ_EINVAL;

@@ -58,6 +58,7 @@ extern "C" {
 typedef struct gpj_ctx gpj_ctx;
 typedef struct gpj_file gpj_file;
 typedef struct gpj_result gpj_result;
+typedef struct gpj_values gpj_values;
 
 /* ---- context ------------------------------------------------------------ */
 
@@ -259,6 +260,40 @@ int gpj_result_slots(const gpj_result *r);
 /* Pointer to int64[num_queries][num_lines][slots][2], valid until release. */
 const int64_t *gpj_result_offsets(const gpj_result *r);
 void gpj_result_release(gpj_result *r);
+
+/* ---- values ------------------------------------------------------------------ */
+
+/* Kinds of a (start, end) result pair in value extraction. */
+#define GPJ_VALUE_NULL 0       /* start == -1: no match (ResultItem returns null) */
+#define GPJ_VALUE_PRESENT 1    /* the bytes file[start, end) */
+#define GPJ_VALUE_UNREADABLE 2 /* end before start (or past the file): the reference's
+                                  ResultItem fails to build it (NegativeArraySizeException) */
+
+/* Value extraction on the device (result/ResultItem.java:32-52 slices the
+ * memory-mapped file on the host, one String per access): for `npairs`
+ * (start, end) pairs of `file` in device memory (e.g. gpj_query_device
+ * output), writes the kind of each pair to d_kinds[npairs], the byte offset
+ * of its value to d_offsets[npairs + 1] (d_offsets[npairs] = the total;
+ * non-values take no bytes) and the values back to back to d_bytes.  Returns
+ * GPJ_ELIMIT with *total_bytes set when bytes_cap is too small (kinds and
+ * offsets are complete then).  Synchronous. */
+int gpj_values_device(gpj_ctx *ctx, gpj_file *file, const int64_t *d_pairs, int64_t npairs,
+                      uint8_t *d_kinds, int64_t *d_offsets, uint8_t *d_bytes, int64_t bytes_cap,
+                      int64_t *total_bytes);
+
+/* gpj_query_paths with the values instead of the offsets: the paths are
+ * evaluated as there, the values gathered on the device and copied to the
+ * host compactly.  Item i = (query * lines + line) * slots + slot. */
+int gpj_query_values(gpj_ctx *ctx, gpj_file *file, int nq, const char *const *paths,
+                     gpj_values **out);
+int64_t gpj_values_num_queries(const gpj_values *v);
+int64_t gpj_values_num_lines(const gpj_values *v);
+int gpj_values_slots(const gpj_values *v);
+const uint8_t *gpj_values_kinds(const gpj_values *v);   /* [items] GPJ_VALUE_* */
+const int64_t *gpj_values_offsets(const gpj_values *v); /* [items + 1] */
+const uint8_t *gpj_values_bytes(const gpj_values *v);   /* gpj_values_size bytes */
+int64_t gpj_values_size(const gpj_values *v);
+void gpj_values_release(gpj_values *v);
 
 /* ---- batches ---------------------------------------------------------------- */
 
