@@ -383,6 +383,23 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         assert np.array_equal(res_host.numpy(), out.cpu().numpy()), "e2e results differ"
     e2e_value = world * n / e2e_s / 1e9
 
+    # ---- value extraction (gpj_query_values): the matched values gathered on
+    # the device into one compact buffer instead of the (start, end) pairs
+    value_info = None
+    if args.mode != "index":
+        lib.gpj_reset_timings(ctx)
+        vals = f.query_values(QUERIES)
+        vphase = {ph["name"]: ph["device_ms"] for ph in g.timings()["phases"]}
+        value_info = {
+            "gather_and_copy_ms": round(vphase.get("gather_values", float("nan")), 4),
+            "values": int((vals.kinds == gj.VALUE_PRESENT).sum()),
+            "value_bytes": len(vals.data),
+            "pair_bytes": int(out.numel() * 8),
+            "note": "gpj_query_values on the resident index: device time of the gather (sizes, scan, byte copy) "
+                    "and of the copies of kinds + offsets + value bytes to pageable host memory",
+        }
+        del vals
+
     # ---- roofline of the dominant kernel ----------------------------------------
     # Algorithmic bytes of one index (+query) pass = the input bytes n (each
     # byte is read once; the index it writes is reported beside it).  The
@@ -450,6 +467,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
             "two_call_path": "gpj_file_from_host_indexed (copy overlapped with indexing) + gpj_query",
             "pinned_h2d_copy_gbs": round(h2d_gbs, 2),
         },
+        "value_extraction": value_info,
         "gpu_launches": int(launches),
         "clocks": clock_info,
     }

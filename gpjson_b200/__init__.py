@@ -385,8 +385,9 @@ class File:
         return out
 
     def query_paths(self, paths: list[str]) -> np.ndarray:
-        """gpj_query_paths: compile, index and evaluate in one pass; returns
-        int64 [nq][lines][slots][2]."""
+        """gpj_query_paths: compile, index and evaluate in one pass (an index
+        already built with enough levels is reused); returns int64
+        [nq][lines][slots][2]."""
         arr = (c_char_p * len(paths))(*[p.encode("utf-8") for p in paths])
         r = c_void_p()
         self._native.check(self._native.lib.gpj_query_paths(self._native.h, self._h, len(paths), arr, byref(r)))

@@ -1310,9 +1310,20 @@ static int run_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths
         bcs[i] = compiled[i].bytecode.data();
         lens[i] = compiled[i].bytecode.size();
     }
+    if (f->indexed && f->num_levels >= depth) {
+        // the resident index has enough levels: the queries alone
+        rc = ensure_out(ctx, f, static_cast<size_t>(nq) * f->num_lines * slots * 2);
+        if (!rc) rc = query_common(ctx, f, nq, bcs.data(), lens.data(), slots, f->d_out,
+                                   static_cast<int64_t>(nq) * f->num_lines * slots * 2, false, nullptr);
+        if (!rc) rc = end_phase(ctx, "find_value", now_ms());
+        if (rc) return rc;
+        *slots_out = slots;
+        *cap_out = f->num_lines;
+        return GPJ_OK;
+    }
     // One pass for index and queries, with results strided by a line
-    // capacity (the known line count, else the newline-index estimate).
-    int64_t cap = f->indexed ? f->num_lines : std::min<int64_t>(f->n + 1, f->n / 256 + 1024);
+    // capacity (the newline-index estimate).
+    int64_t cap = std::min<int64_t>(f->n + 1, f->n / 256 + 1024);
     for (int attempt = 0; attempt < 2; attempt++) {
         rc = ensure_out(ctx, f, static_cast<size_t>(nq) * cap * slots * 2);
         if (rc) return rc;

@@ -27,6 +27,23 @@ def build(force: bool = False) -> Path:
     return LIB_PATH
 
 
+# Where the reference's CUDA kernels are read from to build oracle/_ref
+# (ref_gpu_driver.cu); absent on hosts that only run the prebuilt library.
+REF_KERNELS = Path("/root/reference/gpjson/src/main/resources/com/koenv/gpjson/kernels")
+
+
+def build_reference_kernels(force: bool = False) -> Path | None:
+    """Builds oracle/_ref/libref_gpu.so from the reference's kernel sources
+    when they are present; returns its path, or None without them."""
+    target = HERE / "_ref" / "libref_gpu.so"
+    if not REF_KERNELS.is_dir():
+        return target if target.exists() else None
+    deps = [HERE / "ref_gpu_driver.cu"] + sorted(REF_KERNELS.glob("*.cu"))
+    if force or not target.exists() or any(d.stat().st_mtime > target.stat().st_mtime for d in deps):
+        subprocess.run(["make", "-s", "-C", str(HERE), f"REF_KERNELS={REF_KERNELS}", "_ref/libref_gpu.so"], check=True)
+    return target
+
+
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:

@@ -62,14 +62,18 @@ def run_gpu(gpjson, data: bytes, paths: list[str]) -> np.ndarray:
     f = gpjson.load_bytes(data)
     try:
         two_pass = f.query_paths(paths)
-        gpjson.set_query_fusion(True)
-        try:
-            fused = f.query_paths(paths)
-        finally:
-            gpjson.set_query_fusion(False)
+        again = f.query_paths(paths)  # the resident index is reused: queries only
         f.build_index(max(c.max_depth for c in compiled))
         separate = f.run(compiled)
     finally:
+        f.release()
+    assert np.array_equal(again, two_pass), "query on the resident index differs"
+    f = gpjson.load_bytes(data)  # a fresh file, so the index is built with the queries inside
+    gpjson.set_query_fusion(True)
+    try:
+        fused = f.query_paths(paths)
+    finally:
+        gpjson.set_query_fusion(False)
         f.release()
     assert np.array_equal(fused, separate), "in-kernel and separate query paths differ"
     assert np.array_equal(two_pass, separate), "two-pass and separate query paths differ"

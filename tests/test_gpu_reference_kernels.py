@@ -36,3 +36,43 @@ def test_equal_to_reference_kernels(gpjson, size):
         f.release()
     assert np.array_equal(got, ref["results"])
     assert (got[:, :, 0, 0] >= 0).sum() > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not ref_gpu.available(), reason="oracle/_ref/libref_gpu.so not built (needs the reference sources)")
+def test_faster_than_reference_kernels(gpjson, capsys):
+    """The reference's GPU path (its kernels and host scans, input resident
+    on the device, 4 queries each with a find_value launch) against this
+    library's index build + one find_value launch, on the same 1 GiB of
+    tweet-like NDJSON on the same GPU (the reference's counters overflow at
+    2 GiB).  Prints both; requires a 20x margin."""
+    import statistics
+
+    size = 1 << 30
+    data = datagen.tweets(size, seed=datagen.SEED_BASE + 1)
+    compiled = [gj.compile_path(p) for p in PATHS]
+    ref = ref_gpu.run(data, 4, [c.bytecode for c in compiled], 1, repeats=2, outputs=False)
+    f = gpjson.load_bytes(data)
+    try:
+        for _ in range(2):
+            f.build_index(4)
+            f.run(compiled)
+        gpjson._native.lib.gpj_reset_timings(gpjson._native.h)
+        for _ in range(3):
+            f.build_index(4)
+            f.run(compiled)
+        phases = {}
+        for ph in gpjson.timings()["phases"]:
+            phases.setdefault(ph["name"], []).append(ph["device_ms"])
+    finally:
+        f.release()
+    ours_index = statistics.mean(phases["build_index"])
+    ours_query = statistics.mean(phases["find_value"])
+    ref_total = ref["index_ms"] + ref["query_ms"]
+    ours_total = ours_index + ours_query
+    with capsys.disabled():
+        print(f"\n1 GiB, {ref['lines']} lines, 4 queries: reference kernels index {ref['index_ms']:.2f} ms + "
+              f"queries {ref['query_ms']:.2f} ms = {size / ref_total / 1e6:.2f} GB/s; this library index "
+              f"{ours_index:.3f} ms + queries {ours_query:.3f} ms = {size / ours_total / 1e6:.1f} GB/s; "
+              f"{ref_total / ours_total:.0f}x")
+    assert ours_total * 20 < ref_total
