@@ -62,10 +62,12 @@ GPJ_HD uint32_t mulhi32(uint32_t a, uint32_t b) {
 // 0x80 in every byte of x equal to the byte replicated in `pattern`
 // (pattern bytes < 0x80), 0 elsewhere.  Exact for all 256 byte values:
 // the low seven bits are compared with a carry-free add, bit 7 must be 0.
-GPJ_HD uint32_t eq_bytes(uint32_t x, uint32_t pattern) {
-    const uint32_t low = ((x ^ pattern) & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
-    return ~(low | x) & 0x80808080u;
+GPJ_HD uint32_t low_differs(uint32_t x, uint32_t pattern) {
+    // bit 7 of each byte: the low seven bits of x and pattern differ there
+    return ((x ^ pattern) & 0x7F7F7F7Fu) + 0x7F7F7F7Fu;
 }
+
+GPJ_HD uint32_t eq_bytes(uint32_t x, uint32_t pattern) { return ~(low_differs(x, pattern) | x) & 0x80808080u; }
 
 // 4x4 byte transpose of rows r0..r3: column c = {r0.b_c, r1.b_c, r2.b_c, r3.b_c}.
 GPJ_HD void transpose4(uint32_t r0, uint32_t r1, uint32_t r2, uint32_t r3, uint32_t& c0,
@@ -107,10 +109,14 @@ GPJ_HD void classify32(const uint32_t v[8], uint32_t& bs, uint32_t& qt, uint32_t
         const uint32_t fb = eq_bytes(x, 0x5C5C5C5Cu);
         const uint32_t fq = eq_bytes(x, 0x22222222u);
         const uint32_t fn = eq_bytes(x, 0x0A0A0A0Au);
-        const uint32_t fo = eq_bytes(y, 0x7B7B7B7Bu);
-        const uint32_t fc = eq_bytes(y, 0x7D7D7D7Du);
-        const uint32_t fk = eq_bytes(x, 0x3A3A3A3Au);
-        const uint32_t fs = fo | fc | fk | eq_bytes(x, 0x2C2C2C2Cu);
+        // a byte is structural when it equals any of the four patterns: the
+        // "differs" bits AND together (y has x's bit 7)
+        const uint32_t lo = low_differs(y, 0x7B7B7B7Bu), lc = low_differs(y, 0x7D7D7D7Du);
+        const uint32_t lk = low_differs(x, 0x3A3A3A3Au), lm = low_differs(x, 0x2C2C2C2Cu);
+        const uint32_t fo = ~(lo | x) & 0x80808080u;
+        const uint32_t fc = ~(lc | x) & 0x80808080u;
+        const uint32_t fk = ~(lk | x) & 0x80808080u;
+        const uint32_t fs = ~((lo & lc & lk & lm) | x) & 0x80808080u;
         // flags of different w occupy different bits, so adding equals OR;
         // the high half of f * 2^(25+w) is f >> (7-w) (one multiply-add)
         if (w < 7) {

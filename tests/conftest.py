@@ -44,6 +44,8 @@ def hostsim():
                                  ctypes.c_int]
     L.hs_query_items.restype = ctypes.c_int64
     L.hs_query_items.argtypes = [ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int64, P]
+    L.hs_classify.restype = None
+    L.hs_classify.argtypes = [P, ctypes.c_int64, P]
     L.hs_escaped_mask.restype = ctypes.c_uint64
     L.hs_escaped_mask.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
     return L

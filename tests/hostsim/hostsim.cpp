@@ -212,6 +212,18 @@ void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t line
     }
 }
 
+// The byte classes of `words` 64-byte words: out[7 * w + c] = class c
+// (backslash, quote, newline, open, close, structural, colon) of word w.
+void hs_classify(const uint8_t* bytes, int64_t words, uint64_t* out) {
+    for (int64_t w = 0; w < words; w++) {
+        uint32_t v[16];
+        std::memcpy(v, bytes + 64 * w, 64);
+        const ClassMasks m = classify64(v);
+        const uint64_t c[7] = {m.backslash, m.quote, m.newline, m.open, m.close, m.structural, m.colon};
+        for (int k = 0; k < 7; k++) out[7 * w + k] = c[k];
+    }
+}
+
 // Escape-mask check on one word against a byte loop.
 uint64_t hs_escaped_mask(uint64_t bs, uint32_t cin, uint32_t* cout) {
     return escaped_mask(bs, cin, cout);

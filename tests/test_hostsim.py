@@ -190,3 +190,28 @@ def test_query_item_numbering(hostsim, lines, nq, stride):
             real = warp[warp[:, 0] >= 0]
             assert len(set(real[:, 1].tolist())) <= 1
             assert (np.diff(real[:, 0]) == 1).all()
+
+
+def test_classification_every_byte_value(hostsim):
+    """The SWAR byte classes of the index kernels are exact for all 256 byte
+    values at every position of a word (each value once at each of the 64
+    positions, among the other values)."""
+    rng = np.random.default_rng(11)
+    words = []
+    for pos in range(64):
+        for v in range(256):
+            w = rng.integers(0, 256, 64, dtype=np.uint8)
+            w[pos] = v
+            words.append(w)
+    data = np.concatenate(words)
+    out = np.zeros(len(words) * 7, dtype=np.uint64)
+    hostsim.hs_classify(data.ctypes.data, len(words), out.ctypes.data)
+    got = out.reshape(-1, 7)
+    b = data.reshape(-1, 64)
+    classes = [b == ord("\\"), b == ord('"'), b == ord("\n"), (b == ord("{")) | (b == ord("[")),
+               (b == ord("}")) | (b == ord("]")),
+               np.isin(b, np.frombuffer(b"{}[]:,", dtype=np.uint8)), b == ord(":")]
+    weights = (np.uint64(1) << np.arange(64, dtype=np.uint64))
+    for k, flags in enumerate(classes):
+        want = (flags.astype(np.uint64) * weights).sum(axis=1, dtype=np.uint64)
+        assert np.array_equal(got[:, k], want), k
