@@ -663,13 +663,20 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
         const int slot = kLines ? tid : -1;    // masks kept in shared memory for the line warps
         const uint64_t valid = bits_between(0, (ahead ? loaded_end : tile_end) - ws);
         ClassMasks m = load_classify(buf, tid);
-        restrict_masks(m, valid);
+        if (valid != ~0ull) restrict_masks(m, valid);
         // Escapes: a backslash run never crosses a '\n', so for every byte at
         // or after the tile's first line start the run found inside the slot
         // is the whole run (floor 0, parity 0 is exact there).
-        const uint32_t cin = escape_carry_in(buf, tid, m.backslash, 0, 0);
-        uint32_t cout;
-        const uint64_t esc = escaped_mask(m.backslash, cin, &cout);
+        uint32_t cout = 0;
+        uint64_t esc;
+        if (__any_sync(~0u, m.backslash != 0)) {
+            const uint32_t cin = escape_carry_in(buf, tid, m.backslash, 0, 0);
+            esc = escaped_mask(m.backslash, cin, &cout);
+        } else {
+            // no backslash in the warp's words: only the first byte of its
+            // first word can be escaped, by a run ending just before it
+            esc = (tid & 31) == 0 ? escape_scan_back(buf, tid, 0, 0) : 0u;
+        }
         const uint64_t quotes = m.quote & ~esc;
         const uint64_t p0 = prefix_xor(quotes);
         const bool has_nl = m.newline != 0;
@@ -679,11 +686,13 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
         const uint64_t pa = (p0 ^ (((p0 >> f) & 1ull) ? ~0ull : 0ull)) & after;
         const bool reset_w = has_nl && !ahead;  // only the tile's own newlines start lines here
         int q_w, d_abs = 0, dout_w = 0, din_w = 0;
+        // quote parities from the prefix XOR: p0's bit 63 covers the word, bit f the bytes up to the '\n'
+        const int par_all = static_cast<int>(p0 >> 63);
         if (reset_w) {
-            q_w = popc64(quotes & after) & 1;
+            q_w = par_all ^ static_cast<int>((p0 >> f) & 1ull);
             d_abs = -1 + popc64(m.open & after & ~pa) - popc64(m.close & after & ~pa);
         } else {
-            q_w = popc64(quotes) & 1;
+            q_w = par_all;
             dout_w = popc64(m.open & ~p0) - popc64(m.close & ~p0);
             din_w = popc64(m.open) - popc64(m.close) - dout_w;
         }

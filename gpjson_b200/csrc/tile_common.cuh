@@ -68,14 +68,10 @@ __device__ __forceinline__ void restrict_masks(ClassMasks& m, uint64_t keep) {
 // word, scans the bytes before it in shared memory down to `floor` (a byte
 // index in buf) and adds `parity_at_floor` (the escape state of byte floor)
 // when the run reaches it.  Must be called by all 32 lanes.
-__device__ __forceinline__ uint32_t escape_carry_in(const uint8_t* buf, int w, uint64_t backslash, int floor,
-                                                    int parity_at_floor) {
-    const int lane = threadIdx.x & 31;
-    const bool all_bs = backslash == ~0ull;
-    const int trail_par = all_bs ? 0 : (clz64(~backslash) & 1);
-    const int prev_par = __shfl_up_sync(~0u, trail_par, 1);
-    const int prev_all = __shfl_up_sync(~0u, all_bs ? 1 : 0, 1);
-    if (lane > 0 && !prev_all) return static_cast<uint32_t>(prev_par);
+// Escape state of byte 64w from the bytes before it in buf: parity of the
+// backslash run ending at byte 64w - 1, scanned down to `floor` (plus
+// `parity_at_floor` when the run reaches it).
+__device__ __forceinline__ uint32_t escape_scan_back(const uint8_t* buf, int w, int floor, int parity_at_floor) {
     int run = 0, k = 64 * w - 1;
     while (k >= floor && buf[k] == '\\') {
         ++run;
@@ -84,6 +80,17 @@ __device__ __forceinline__ uint32_t escape_carry_in(const uint8_t* buf, int w, u
     int c = run & 1;
     if (k < floor) c ^= parity_at_floor;
     return static_cast<uint32_t>(c);
+}
+
+__device__ __forceinline__ uint32_t escape_carry_in(const uint8_t* buf, int w, uint64_t backslash, int floor,
+                                                    int parity_at_floor) {
+    const int lane = threadIdx.x & 31;
+    const bool all_bs = backslash == ~0ull;
+    const int trail_par = all_bs ? 0 : (clz64(~backslash) & 1);
+    const int prev_par = __shfl_up_sync(~0u, trail_par, 1);
+    const int prev_all = __shfl_up_sync(~0u, all_bs ? 1 : 0, 1);
+    if (lane > 0 && !prev_all) return static_cast<uint32_t>(prev_par);
+    return escape_scan_back(buf, w, floor, parity_at_floor);
 }
 
 __device__ __forceinline__ Span shfl_span_up(const Span& v, int off) {
