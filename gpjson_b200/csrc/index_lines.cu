@@ -205,8 +205,11 @@ struct TileScan {
 
 template <int LV>
 struct FShared {
-    uint8_t bytes[kRing][kSlotBytes];
-    TileFile desc[kRing];  // the file of the tile in each byte slot
+    // the line warps read a tile's bytes while the next tile is indexed and
+    // the one after is copied: three byte slots
+    static constexpr int kByteSlots = kRing;
+    uint8_t bytes[kByteSlots][kSlotBytes];
+    TileFile desc[kRing];  // the file of the tile (by tile number modulo kRing)
     uint64_t str[kMaskSlots][kSlotWords];
     uint64_t colon[kMaskSlots][kSlotWords];
     uint64_t lv[kMaskSlots][LV][kSlotWords];
@@ -236,10 +239,14 @@ struct FShared {
 // Shared memory of the standalone index kernel (no line warps, no queries).
 template <int LV>
 struct TShared {
-    uint8_t bytes[kRing][kSlotBytes];
+    // nothing reads a tile's bytes after its last barrier, so the copy of
+    // tile k+1 can go into the slot of tile k-1: two byte slots (and room for
+    // five CTAs per SM); the file descriptors, read after that barrier, keep three
+    static constexpr int kByteSlots = 2;
+    uint8_t bytes[kByteSlots][kSlotBytes];
     TileFile desc[kRing];
     uint64_t lvacc[kTileWarps][LV][32];
-    uint64_t full[kRing];
+    uint64_t full[kByteSlots];
     Span span_scratch[kTileWarps];
     WarpSum rscan[2][kTileWarps];
     int carry_esc;
@@ -610,11 +617,11 @@ __device__ __forceinline__ void fetch_tile_file(const IndexParams& p, int64_t t,
 }
 
 // Starts the TMA copy of tile t into byte slot `slot` (one thread); the
-// tile's file goes into sh.desc[slot] before the copy's mbarrier arrive, so
+// tile's file goes into sh.desc[dslot] before the copy's mbarrier arrive, so
 // the threads that wait for the copy also see it.
 template <class Sh>
-__device__ __forceinline__ void start_tile(const IndexParams& p, Sh& sh, int64_t t, int slot) {
-    TileFile& F = sh.desc[slot];
+__device__ __forceinline__ void start_tile(const IndexParams& p, Sh& sh, int64_t t, int slot, int dslot) {
+    TileFile& F = sh.desc[dslot];
     fetch_tile_file(p, t, &F);
     const int64_t start = (t - F.tile_begin) * kTile;
     load_slot(F.file, start, F.avail - start < kSlotBytes ? F.avail - start : kSlotBytes, sh.bytes[slot],
@@ -631,24 +638,27 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
     const int tid = threadIdx.x;  // 0..255
     unsigned long long* nl_agg = p.tile_state;
     const int64_t first_tile = p.tile_begin + blockIdx.x, stride = gridDim.x;
-    if (tid == 0 && first_tile < p.tile_end) start_tile(p, sh, first_tile, 0);
+    if (tid == 0 && first_tile < p.tile_end) start_tile(p, sh, first_tile, 0, 0);
     int64_t k = 0;
     for (int64_t t = first_tile; t < p.tile_end; t += stride, ++k) {
-        const int bs = static_cast<int>(k % kRing), ms = static_cast<int>(k & 1);
-        const uint32_t buse = static_cast<uint32_t>(k / kRing), muse = static_cast<uint32_t>(k >> 1);
-        // start the copy of the next tile (its byte slot was last used three tiles ago)
+        constexpr int kSlots = Sh::kByteSlots;
+        const int bs = static_cast<int>(k % kSlots), ds = static_cast<int>(k % kRing), ms = static_cast<int>(k & 1);
+        const uint32_t buse = static_cast<uint32_t>(k / kSlots), muse = static_cast<uint32_t>(k >> 1);
+        // start the copy of the next tile: its byte slot was last used kSlots
+        // tiles ago (two in the standalone kernel: tile k-1, whose bytes no
+        // thread reads after that tile's last barrier)
         if (tid == 0 && t + stride < p.tile_end) {
-            const int nb = static_cast<int>((k + 1) % kRing);
-            const uint32_t nuse = static_cast<uint32_t>((k + 1) / kRing);
+            const int nb = static_cast<int>((k + 1) % kSlots);
+            const uint32_t nuse = static_cast<uint32_t>((k + 1) / kSlots);
             if constexpr (kLines) {
                 if (nuse > 0 && !mbar_wait_idle(&sh.bfree[nb], (nuse - 1) & 1))
                     atomicOr(p.status + 1, kErrCopyTimeout);
             }
-            start_tile(p, sh, t + stride, nb);
+            start_tile(p, sh, t + stride, nb, static_cast<int>((k + 1) % kRing));
         }
         if (!mbar_wait_bounded(&sh.full[bs], buse & 1) && tid == 0) atomicOr(p.status + 1, kErrCopyTimeout);
         const uint8_t* buf = sh.bytes[bs];
-        const TileFile& F = sh.desc[bs];
+        const TileFile& F = sh.desc[ds];
         const int64_t lt = t - F.tile_begin;  // the tile's index in its file
 
         const int64_t tile_start = lt * kTile;
@@ -968,11 +978,11 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
 // Index only: the index warps alone, three CTAs per SM; no tile waits for
 // another, since the newline index is built afterwards from the counts.
 template <int LV>
-__global__ void __launch_bounds__(kIndexThreads, 3) tile_index_kernel(IndexParams p) {
+__global__ void __launch_bounds__(kIndexThreads, 5) tile_index_kernel(IndexParams p) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
     TShared<LV>& sh = *reinterpret_cast<TShared<LV>*>(smem_raw);
     if (threadIdx.x == 0) {
-        for (int i = 0; i < kRing; i++) mbar_init(&sh.full[i], 1);
+        for (int i = 0; i < TShared<LV>::kByteSlots; i++) mbar_init(&sh.full[i], 1);
         fence_mbar_init();
     }
     __syncthreads();
