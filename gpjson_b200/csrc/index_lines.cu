@@ -25,7 +25,8 @@
 // Each CTA is a three-stage pipeline over its tiles (tile blockIdx.x, then
 // every gridDim.x-th):
 //  * copies: 1-D TMA bulk loads of tile + look-ahead (16 KiB) into a ring
-//    of three byte slots, issued one tile ahead;
+//    of byte slots (three here; two in the standalone kernel, whose tiles'
+//    bytes nobody reads after the tile's last barrier), issued one tile ahead;
 //  * index warps (0-7, one 64-byte word of the slot per thread): classify,
 //    resolve escapes and strings, one block scan with a reset at newlines
 //    (line starts, newline counts and each word's state at once), split
