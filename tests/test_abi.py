@@ -108,3 +108,24 @@ def test_result_views_follow_reference_layout():
         r[1]
     with pytest.raises(IndexError):
         r[0][3]
+
+
+def test_values_view_follows_result_item():
+    """The compact value view (gj.Values) answers like ResultItem: null for
+    a miss, the value's text, an error for a pair without an end, UTF-8
+    decoded with replacement."""
+    import numpy as np
+
+    kinds = np.array([[[gj.VALUE_PRESENT], [gj.VALUE_NULL], [gj.VALUE_UNREADABLE], [gj.VALUE_PRESENT]]],
+                     dtype=np.uint8)
+    data = '"x"12"été"'.encode() + b"\xff"
+    offsets = np.array([0, 3, 3, 3, len(data)], dtype=np.int64)
+    v = gj.Values(kinds, offsets, data, ["$.a"])
+    assert len(v) == 1 and len(v[0]) == 4 and len(v[0][0]) == 1
+    assert v[0][0][0] == '"x"' and v[0][1][0] is None
+    with pytest.raises(gj.GPJSONException):
+        v[0][2][0]
+    assert v[0][3][0] == '12"été"�'
+    assert v[-1][-1][:] == ['12"été"�']
+    with pytest.raises(IndexError):
+        v[0][4]
