@@ -77,6 +77,8 @@ struct gpj_file {
     int64_t words = 0;
 
     uint64_t* d_str = nullptr;
+    uint64_t* d_colon = nullptr;  // ':' outside strings, for find_value's key searches
+    bool colon_valid = false;     // d_colon belongs to the current index
     uint64_t* d_lvl = nullptr;
     int lvl_cap = 0;
     int64_t* d_nl = nullptr;
@@ -316,10 +318,13 @@ int finish_tiles(gpj_ctx* ctx, const gpj::IndexParams& p, const TileScratch& ts)
 // same pass when given), and again with the exact kernel when the input is
 // not well-formed NDJSON.  *lines receives the line count; *queries_done
 // tells whether every line's query results were written.
+// d_colon (optional) receives the ':' bitmap when the standalone kernel
+// builds the index; *colon_valid (optional) tells whether it did.
 int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, uint64_t* d_str,
               uint64_t* d_lvl, int64_t* d_nl, int64_t nl_cap, int64_t* lines, const FusedQueries* fq = nullptr,
-              bool* queries_done = nullptr) {
+              bool* queries_done = nullptr, uint64_t* d_colon = nullptr, bool* colon_valid = nullptr) {
     if (queries_done) *queries_done = false;
+    if (colon_valid) *colon_valid = false;
     if (n == 0) {
         if (nl_cap > 0) GPJ_CUDA(ctx, cudaMemsetAsync(d_nl, 0, 8, ctx->stream));
         GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -364,6 +369,7 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
             GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
             fused.newline_bits = ts.bits;
             fused.tile_newlines = ts.counts;
+            fused.colon = d_colon;
             fused.status = ctx->d_status;
             rc = launch_tiles(ctx, fused);
             if (!rc) rc = finish_tiles(ctx, fused, ts);
@@ -383,6 +389,7 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
     rc = status_error(ctx, errs);
     if (rc) return rc;
     *lines = static_cast<int64_t>(ctx->h_status[0]);
+    if (colon_valid) *colon_valid = d_colon && !exact && !(fq && fq->nq > 0);
     if (queries_done && fq && fq->nq > 0)
         *queries_done = !exact && !(errs & (gpj::kErrDeferred | gpj::kErrOutOverflow)) && *lines <= fq->out_lines;
     return GPJ_OK;
@@ -462,6 +469,7 @@ int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, i
     p.range = d_range;
     p.last = last ? 1 : 0;
     p.newline_cap = f->nl_cap;
+    p.colon = f->colon_valid ? f->d_colon : nullptr;
     const int64_t want = d_range ? INT64_MAX : (gpj::query_items(f->num_lines, nq) + 255) / 256;
     const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * ctx->query_occupancy));
     GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->stream));
@@ -481,6 +489,9 @@ int ensure_index_buffers(gpj_ctx* ctx, gpj_file* f, int num_levels) {
     if (num_levels < 1 || num_levels > GPJ_MAX_LEVELS)
         return fail(ctx, GPJ_ELIMIT, "Invalid number of levels: " + std::to_string(num_levels));
     if (!f->d_str && (rc = device_alloc(ctx, &f->d_str, static_cast<size_t>(f->words), "cudaMalloc(string index)")))
+        return rc;
+    if (!f->d_colon && (rc = device_alloc(ctx, &f->d_colon, static_cast<size_t>(std::max<int64_t>(f->words, 1)),
+                                          "cudaMalloc(colon bitmap)")))
         return rc;
     if (f->lvl_cap < num_levels) {
         device_free(ctx, f->d_lvl);
@@ -504,11 +515,12 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
     int rc = ensure_index_buffers(ctx, f, num_levels);
     if (rc) return rc;
     f->indexed = false;
+    f->colon_valid = false;
     const double t0 = now_ms();
     GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     int64_t lines = 0;
     rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, fq,
-                   queries_done);
+                   queries_done, f->d_colon, &f->colon_valid);
     if (rc) return rc;
     if (lines > f->nl_cap) {  // more lines than the first guess: size exactly and rebuild
         device_free(ctx, f->d_nl);
@@ -516,7 +528,7 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
         rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(lines), "cudaMalloc(newline index)");
         if (rc) return rc;
         rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, fq,
-                       queries_done);
+                       queries_done, f->d_colon, &f->colon_valid);
         if (rc) return rc;
     }
     rc = end_phase(ctx, fq && fq->nq ? "index_and_query" : "build_index", t0);
@@ -557,6 +569,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
     int rc = ensure_index_buffers(ctx, f, num_levels);
     if (rc) return rc;
     f->indexed = false;
+    f->colon_valid = false;
     const double t0 = now_ms();
     GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     const int64_t nchunks = (n + kLoadChunk - 1) / kLoadChunk;
@@ -565,7 +578,8 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         if (n > 0)
             GPJ_CUDA(ctx, cudaMemcpyAsync(f->d_owned, host, static_cast<size_t>(n), cudaMemcpyHostToDevice,
                                           ctx->stream));
-        rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
+        rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, nullptr,
+                           nullptr, f->d_colon, &f->colon_valid);
         if (rc) return rc;
     } else {
         while (static_cast<int64_t>(ctx->chunk_events.size()) < nchunks) {
@@ -584,6 +598,8 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         p.newlines = f->d_nl;
         p.newline_cap = f->nl_cap;
         p.materialize = 1;
+        p.colon = f->d_colon;
+        f->colon_valid = true;  // the chunks' queries read it as their tiles write it
         TileScratch ts;
         rc = alloc_tile_scratch(ctx, n, &ts);
         int64_t* d_lines = nullptr;  // [k + 1]: lines complete after chunk k
@@ -636,6 +652,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         free_tile_scratch(ctx, &ts);
         device_free(ctx, d_lines);
         if (rc) {
+            f->colon_valid = false;
             cudaStreamSynchronize(ctx->copy_stream);
             return rc;
         }
@@ -643,9 +660,11 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         lines = static_cast<int64_t>(ctx->h_status[0]);
         if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) {
             // the whole input is on the device now: index it in one launch (exact fallback inside)
-            rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
+            rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, nullptr,
+                           nullptr, f->d_colon, &f->colon_valid);
             if (rc) return rc;
         } else if ((rc = status_error(ctx, errs))) {
+            f->colon_valid = false;
             return rc;
         } else if (cq && lines <= f->nl_cap && lines <= cq->out_lines && queries_done) {
             *queries_done = true;
@@ -656,7 +675,8 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         f->nl_cap = lines;
         rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(lines), "cudaMalloc(newline index)");
         if (rc) return rc;
-        rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines);
+        rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, nullptr,
+                           nullptr, f->d_colon, &f->colon_valid);
         if (rc) return rc;
     }
     rc = end_phase(ctx, "load_and_index", t0);
@@ -1169,6 +1189,7 @@ void gpj_file_release(gpj_file* f) {
         gpj_ctx* ctx = f->ctx;
         device_free(ctx, f->d_owned);
         device_free(ctx, f->d_str);
+        device_free(ctx, f->d_colon);
         device_free(ctx, f->d_lvl);
         device_free(ctx, f->d_nl);
         device_free(ctx, f->d_ir);
@@ -1529,6 +1550,7 @@ int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
     for (gpj_file* f : need) {
         if ((rc = ensure_index_buffers(ctx, f, levels))) return rc;
         f->indexed = false;
+        f->colon_valid = false;
         if (f->n == 0) continue;  // indexed alone below
         batched.push_back(f);
         total_tiles += (f->n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
@@ -1557,7 +1579,7 @@ int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
                 gpj_file* f = batched[i];
                 const int64_t ntiles = (f->n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
                 tf.push_back(gpj::TileFile{f->d_data, f->n, f->n, f->d_str, f->d_lvl, f->words, bits + word,
-                                           status + 2 * i, tile});
+                                           status + 2 * i, tile, f->d_colon});
                 lf.push_back(gpj::LineFile{bits + word, f->words, f->d_nl, f->nl_cap, status + 2 * i, tile, ntiles});
                 tile += ntiles;
                 word += f->words;
@@ -1615,6 +1637,7 @@ int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
             f->num_lines = lines;
             f->num_levels = levels;
             f->indexed = true;
+            f->colon_valid = true;
         }
     }
     for (gpj_file* f : need)
@@ -1735,7 +1758,8 @@ int gpj_batch_run(gpj_batch* b) {
             qf.push_back(gpj::QueryFile{f->d_data, f->n, f->d_nl, fr.lines, f->d_str, f->d_lvl, f->words,
                                         d_blob + blob_at[i] + header,
                                         reinterpret_cast<const int32_t*>(d_blob + blob_at[i]),
-                                        static_cast<int>(nq), fr.slots, d_out + fr.out_offset, fr.lines, item});
+                                        static_cast<int>(nq), fr.slots, d_out + fr.out_offset, fr.lines, item,
+                                        f->colon_valid ? f->d_colon : nullptr});
             item += gpj::query_items(fr.lines, static_cast<int>(nq));
         }
         cudaError_t e = cudaMemcpyAsync(d_blob, blob.data(), blob.size(), cudaMemcpyHostToDevice, ctx->stream);

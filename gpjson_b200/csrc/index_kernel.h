@@ -30,6 +30,7 @@ struct TileFile {
     uint64_t* newline_bits;
     unsigned long long* status;  // [0] line count, [1] error bits
     int64_t tile_begin;
+    uint64_t* colon;          // optional: ':' outside strings (level_size words)
 };
 
 struct IndexParams {
@@ -60,6 +61,10 @@ struct IndexParams {
     // the newline count of every tile, in place of the newline index.
     uint64_t* newline_bits;
     int32_t* tile_newlines;
+    // Standalone kernel, optional: the ':' bytes outside strings
+    // (ceil(n/64) words), which lets find_value's key searches skip the ','
+    // candidates.
+    uint64_t* colon;
     // Standalone kernel over a batch of files (batch_files > 0): tiles
     // [tile_begin, tile_end) of the whole batch, file table `batch`
     // (ascending tile_begin); status then reports errors that concern no

@@ -553,6 +553,7 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, const TileFile
     }
     if (owned && p.materialize) {
         F.string_index[word] = in_str;
+        if (F.colon) F.colon[word] = m.colon & ~in_str;
 #pragma unroll
         for (int l = 0; l < LV; l++)
             if (l < p.num_levels) F.leveled[F.level_size * l + word] = lv[l];
@@ -603,7 +604,7 @@ __device__ int64_t find_line_end(const TileFile& p, int64_t from, int64_t tile_e
 __device__ __forceinline__ void fetch_tile_file(const IndexParams& p, int64_t t, TileFile* out) {
     if (p.batch_files == 0) {
         *out = TileFile{p.file,     p.n,     p.avail,        p.string_index, p.leveled,
-                        p.level_size, p.newline_bits, p.status, 0};
+                        p.level_size, p.newline_bits, p.status, 0, p.colon};
         return;
     }
     int lo = 0, hi = p.batch_files - 1;  // last file with tile_begin <= t

@@ -113,21 +113,28 @@ GPJ_HD P next_bit(const uint64_t* bm, P from, P limit) {
 }
 
 // First position in [from, limit) set in bm and (in `filt`, or not in it
-// when `invert`), or `limit`.
+// when `invert`), or `limit`; cw/cv as in next_bit, for the combined word
+// bm[w] & (filt[w] ^ flip).
 template <typename P>
-GPJ_HD P next_bit_filtered(const uint64_t* bm, const uint64_t* filt, bool invert, P from, P limit) {
+GPJ_HD P next_bit_filtered(const uint64_t* bm, const uint64_t* filt, bool invert, P from, P limit, P& cw,
+                           uint64_t& cv) {
     if (from >= limit) return limit;
     P w = from >> 6;
     const P wend = ((limit - 1) >> 6) + 1;
     const uint64_t flip = invert ? ~0ull : 0ull;
-    const uint64_t m = bm[w] & (filt[w] ^ flip) & (~0ull << (from & 63));
+    const uint64_t first = w == cw ? cv : bm[w] & (filt[w] ^ flip);
+    const uint64_t m = first & (~0ull << (from & 63));
     if (m) {
+        cw = w;
+        cv = first;
         const P p = (w << 6) + ctz64(m);
         return p < limit ? p : limit;
     }
     for (++w; w < wend && w < (from >> 6) + 3; ++w) {
         const uint64_t x = bm[w] & (filt[w] ^ flip);
         if (x) {
+            cw = w;
+            cv = x;
             const P p = (w << 6) + ctz64(x);
             return p < limit ? p : limit;
         }
@@ -137,7 +144,12 @@ GPJ_HD P next_bit_filtered(const uint64_t* bm, const uint64_t* filt, bool invert
         const uint64_t b = w + 1 < wend ? bm[w + 1] & (filt[w + 1] ^ flip) : 0;
         const uint64_t c = w + 2 < wend ? bm[w + 2] & (filt[w + 2] ^ flip) : 0;
         const uint64_t d = w + 3 < wend ? bm[w + 3] & (filt[w + 3] ^ flip) : 0;
-        if (a | b | c | d) return first_of4<P>(w, a, b, c, d, limit);
+        if (a | b | c | d) {
+            const P p = first_of4<P>(w, a, b, c, d, limit);
+            cw = w + (a ? 0 : (b ? 1 : (c ? 2 : 3)));
+            cv = a ? a : (b ? b : (c ? c : d));
+            return p;
+        }
     }
     return limit;
 }
@@ -367,7 +379,7 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
             const P lim = cend < n ? cend : n;
             if (j < lim) {
                 if (colon)
-                    j = next_bit_filtered<P>(levels + level_size * cur, colon, type != 4, j, lim);
+                    j = next_bit_filtered<P>(levels + level_size * cur, colon, type != 4, j, lim, cw, cv);
                 else
                     j = next_bit<P>(levels + level_size * cur, j, lim, cw, cv);
                 found = j < lim;

@@ -24,7 +24,7 @@ namespace {
 
 __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-    LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size, p.n, nullptr};
+    LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size, p.n, p.colon};
     const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
     // lines [first, first + lines); the file's last line ends at p.n
     int64_t first = 0, lines = p.num_lines, file_lines = p.num_lines;
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256) find_value_batch_kernel(const QueryFile* 
         int64_t i;
         int q;
         if (!query_item(g - F.item_begin, F.item_begin, F.num_lines, F.num_queries, stride, &i, &q)) continue;
-        LineView view{F.file, F.n, F.string_index, F.leveled, F.level_size, F.n, nullptr};
+        LineView view{F.file, F.n, F.string_index, F.leveled, F.level_size, F.n, F.colon};
         const int64_t start = F.newlines[i];
         const int64_t end = i + 1 < F.num_lines ? F.newlines[i + 1] : F.n;
         const int64_t per_line = 2 * static_cast<int64_t>(F.slots);

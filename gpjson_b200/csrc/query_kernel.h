@@ -32,6 +32,10 @@ struct QueryParams {
     const int64_t* range;
     int last;
     int64_t newline_cap;
+    // Optional ':' outside strings (level_size words): key searches jump
+    // between structural colons, index searches between the other
+    // structural bytes (the bytes each search ignores).
+    const uint64_t* colon;
 };
 
 cudaError_t launch_find_value(const QueryParams& p, int grid, cudaStream_t stream);
@@ -57,6 +61,7 @@ struct QueryFile {
     // first of the file's items in the batch: ceil(num_lines / 32) blocks of
     // 32 lines x num_queries (a multiple of 32, so no warp spans two files)
     int64_t item_begin;
+    const uint64_t* colon;  // optional, as QueryParams::colon
 };
 
 // Every (line, query) item of every file of the batch (`files`: device

@@ -48,10 +48,10 @@ POOL_LEVELS = 6  # every pool path needs at most 6 levels
 
 
 def resident_bytes(n: int, levels: int = POOL_LEVELS) -> int:
-    """Device bytes of a resident corpus: input, string index, leveled
-    bitmaps and a newline-index allowance."""
+    """Device bytes of a resident corpus: input, string index, ':' bitmap,
+    leveled bitmaps and a newline-index allowance."""
     words = (n + 63) // 64
-    return n + 8 * words * (1 + levels) + 8 * (n // 256 + 1024)
+    return n + 8 * words * (2 + levels) + 8 * (n // 256 + 1024)
 
 
 @dataclass

@@ -35,4 +35,4 @@ def test_stats_percentiles():
 
 def test_resident_bytes():
     n = 1 << 20
-    assert serve.resident_bytes(n, 6) == n + 8 * (n // 64) * 7 + 8 * (n // 256 + 1024)
+    assert serve.resident_bytes(n, 6) == n + 8 * (n // 64) * 8 + 8 * (n // 256 + 1024)
