@@ -79,15 +79,21 @@ class CompiledQuery:
         return f"CompiledQuery({self.path!r}, depth={self.max_depth}, results={self.num_results})"
 
 
-def compile_path(path: str) -> CompiledQuery:
-    """JSONPathParser(path).compile() via the native compiler."""
+# JSONPath beyond the reference's subset (GPJ_PATH_* flags; none by default)
+PATH_INDEX_UNIONS = 1
+
+
+def compile_path(path: str, extensions: int = 0) -> CompiledQuery:
+    """JSONPathParser(path).compile() via the native compiler; `extensions`
+    (PATH_* flags) admits paths beyond the reference's subset."""
     lib = _lib.load()
     cap = 4096 + 16 * len(path.encode("utf-8"))
     while True:
         out = (c_uint8 * cap)()
         n, depth, res = c_size_t(), c_int(), c_int()
         err = ctypes.create_string_buffer(512)
-        rc = lib.gpj_compile(path.encode("utf-8"), out, cap, byref(n), byref(depth), byref(res), err, 512)
+        rc = lib.gpj_compile_ex(path.encode("utf-8"), extensions, out, cap, byref(n), byref(depth), byref(res), err,
+                                512)
         if rc == _lib.GPJ_ELIMIT and n.value > cap:
             cap = n.value
             continue
@@ -254,7 +260,7 @@ class _ValuesItem(Sequence):
         return self._v.value(self._q, self._line, slot)
 
 
-def prepare_queries(queries, options=None) -> tuple[list[str], list[CompiledQuery]]:
+def prepare_queries(queries, options=None, extensions: int = 0) -> tuple[list[str], list[CompiledQuery]]:
     """Argument handling and compilation of QueryFunction.call
     (QueryFunction.java:64-136): a path or a list of 1..255 paths, an
     optional mapping with `disable_fallback`, every path compiled, the depth
@@ -278,7 +284,7 @@ def prepare_queries(queries, options=None) -> tuple[list[str], list[CompiledQuer
     compiled = []
     for i, p in enumerate(paths):
         try:
-            compiled.append(compile_path(p))
+            compiled.append(compile_path(p, extensions))
         except UnsupportedJSONPathException as e:
             how = "fallback disabled" if disable_fallback else "no CPU fallback in this library"
             raise UnsupportedJSONPathException(f"Unsupported JSON path ({i}, {how}): {e}", e.code) from e
@@ -504,6 +510,7 @@ class GPJSON:
 
     def __init__(self, device: int = 0):
         self._native = _Native(device)
+        self._extensions = 0
 
     # -- files ---------------------------------------------------------------
     def open(self, filename: str | os.PathLike) -> File:
@@ -562,6 +569,13 @@ class GPJSON:
     def batch(self) -> Batch:
         return Batch(self._native)
 
+    def set_path_extensions(self, extensions: int) -> None:
+        """JSONPath extensions (PATH_* flags) for the calls that take path
+        strings (query, query_paths, query_values, batches); 0 = the
+        reference's subset exactly."""
+        self._native.check(self._native.lib.gpj_set_path_extensions(self._native.h, extensions))
+        self._extensions = extensions
+
     def set_query_fusion(self, enabled: bool) -> None:
         """Evaluate queries inside the index kernel (True) or with one
         find_value launch after it (False, the default)."""
@@ -573,7 +587,7 @@ class GPJSON:
     # -- the reference members ------------------------------------------------
     def query(self, filename, queries, options=None) -> Result:
         """QueryFunction.call: query(file, path | [paths], options?)."""
-        paths, _ = prepare_queries(queries, options)
+        paths, _ = prepare_queries(queries, options, self._extensions)
         f = self.open(filename)
         try:
             offsets = f.query_paths(paths)
@@ -588,7 +602,7 @@ class GPJSON:
         """query() with the matched values gathered on the device
         (gpj_query_values): the same [query][line][slot] -> str | None view,
         without reading the file again on the host."""
-        paths, _ = prepare_queries(queries, options)
+        paths, _ = prepare_queries(queries, options, self._extensions)
         f = self.open(filename)
         try:
             return f.query_values(paths)

@@ -8,7 +8,7 @@ built: there is no CPU implementation behind this package.
 from __future__ import annotations
 
 import ctypes
-from ctypes import POINTER, c_char_p, c_int, c_int64, c_size_t, c_uint8, c_uint64, c_void_p
+from ctypes import POINTER, c_char_p, c_int, c_int64, c_size_t, c_uint, c_uint8, c_uint64, c_void_p
 from pathlib import Path
 
 LIB_PATH = Path(__file__).resolve().parent / "_native" / "libgpjson_b200.so"
@@ -59,6 +59,12 @@ SIGNATURES: dict[str, tuple] = {
         [c_void_p, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)],
     ),
     "gpj_set_query_fusion": (c_int, [c_void_p, c_int]),
+    "gpj_set_path_extensions": (c_int, [c_void_p, c_uint]),
+    "gpj_compile_ex": (
+        c_int,
+        [c_char_p, c_uint, POINTER(c_uint8), c_size_t, POINTER(c_size_t), POINTER(c_int), POINTER(c_int),
+         c_char_p, c_size_t],
+    ),
     "gpj_file_from_host_indexed": (c_int, [c_void_p, c_void_p, c_int64, c_int, POINTER(c_void_p)]),
     "gpj_file_from_host_query": (
         c_int,

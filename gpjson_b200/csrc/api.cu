@@ -58,6 +58,7 @@ struct gpj_ctx {
     int tile_occupancy[3] = {0, 0, 0};   // its standalone form (index builds without queries)
     int64_t exact_fallbacks = 0;         // builds that needed the exact kernel
     bool fuse_queries = false;           // evaluate queries inside the index kernel
+    unsigned path_extensions = 0;        // GPJ_PATH_* flags for calls that compile paths
     int query_occupancy = 0;
 
     // pinned staging for file reads
@@ -922,6 +923,16 @@ int gpj_set_query_fusion(gpj_ctx* ctx, int enabled) {
     return GPJ_OK;
 }
 
+static_assert(GPJ_PATH_INDEX_UNIONS == gpj::kPathIndexUnions, "extension flags of the ABI and the compiler");
+
+int gpj_set_path_extensions(gpj_ctx* ctx, unsigned extensions) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (extensions & ~GPJ_PATH_INDEX_UNIONS) return fail(ctx, GPJ_EINVAL, "unknown JSONPath extension flags");
+    ctx->path_extensions = extensions;
+    return GPJ_OK;
+}
+
 int gpj_set_stream(gpj_ctx* ctx, void* stream) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
@@ -933,6 +944,11 @@ int gpj_set_stream(gpj_ctx* ctx, void* stream) {
 
 int gpj_compile(const char* path, uint8_t* out, size_t cap, size_t* len, int* max_depth,
                 int* num_results, char* err, size_t err_cap) {
+    return gpj_compile_ex(path, 0, out, cap, len, max_depth, num_results, err, err_cap);
+}
+
+int gpj_compile_ex(const char* path, unsigned extensions, uint8_t* out, size_t cap, size_t* len, int* max_depth,
+                   int* num_results, char* err, size_t err_cap) {
     auto set_err = [&](const std::string& m) {
         if (err && err_cap > 0) {
             std::strncpy(err, m.c_str(), err_cap - 1);
@@ -944,7 +960,11 @@ int gpj_compile(const char* path, uint8_t* out, size_t cap, size_t* len, int* ma
         return GPJ_EINVAL;
     }
     try {
-        gpj::CompiledPath r = gpj::compile_path(path);
+        if (extensions & ~GPJ_PATH_INDEX_UNIONS) {
+            set_err("unknown JSONPath extension flags");
+            return GPJ_EINVAL;
+        }
+        gpj::CompiledPath r = gpj::compile_path(path, extensions);
         *len = r.bytecode.size();
         *max_depth = r.max_depth;
         *num_results = r.num_results;
@@ -1314,7 +1334,7 @@ static int run_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths
     int depth = 0, slots = 0;
     for (int i = 0; i < nq; i++) {
         try {
-            compiled[i] = gpj::compile_path(paths[i] ? paths[i] : "");
+            compiled[i] = gpj::compile_path(paths[i] ? paths[i] : "", ctx->path_extensions);
         } catch (const gpj::PathError& e) {
             if (e.unsupported)
                 return fail(ctx, GPJ_EUNSUPPORTED, "Unsupported JSON path (" + std::to_string(i) + "): " + e.what());
@@ -1672,7 +1692,7 @@ int gpj_batch_add(gpj_batch* b, gpj_file* f, int nq, const char* const* paths, i
     it.file = f;
     for (int i = 0; i < nq; i++) {
         try {
-            it.queries.push_back(gpj::compile_path(paths[i] ? paths[i] : ""));
+            it.queries.push_back(gpj::compile_path(paths[i] ? paths[i] : "", ctx->path_extensions));
         } catch (const gpj::PathError& e) {
             if (e.unsupported)
                 return fail(ctx, GPJ_EUNSUPPORTED, "Unsupported JSON path (" + std::to_string(i) + "): " + e.what());

@@ -92,7 +92,7 @@ class Emitter {  // IRBuilder.java + IRByteOutputBuffer.java
 
 class Compiler {
    public:
-    explicit Compiler(const std::string& path) : in_(path) {}
+    Compiler(const std::string& path, unsigned extensions) : in_(path), extensions_(extensions) {}
 
     CompiledPath run() {  // JSONPathParser.compile (:20-29)
         in_.expect('$');
@@ -109,6 +109,7 @@ class Compiler {
    private:
     Cursor in_;
     Emitter ir_;
+    unsigned extensions_ = 0;
     int depth_ = 0;  // JSONPathParser.maxLevel
 
     void step() {  // compileNextExpression (:31-43)
@@ -144,7 +145,12 @@ class Compiler {
                 range_step(idx);  // the range compiles the rest of the path
                 return;
             }
-            if (t == ',') throw in_.unsupported_next("Unsupported multiple index expression");
+            if (t == ',') {
+                if (!(extensions_ & kPathIndexUnions))
+                    throw in_.unsupported_next("Unsupported multiple index expression");
+                union_step(idx);  // like a range, the union compiles the rest of the path
+                return;
+            }
             if (t == ']') index_step(idx);
         } else if (c == '*') {
             throw in_.unsupported_next("Unsupported wildcard expression");
@@ -164,17 +170,38 @@ class Compiler {
         in_.expect(':');
         int last = integer("]");
         in_.expect(']');
+        std::vector<int> indices;
+        for (int i = first; i < last; i++) indices.push_back(i);
+        branches(indices);
+    }
+
+    // `[i,j,...]` (kPathIndexUnions): strictly ascending indices, one branch
+    // each, as a range.
+    void union_step(int first) {
+        std::vector<int> indices{first};
+        while (in_.skip(',')) {
+            while (in_.skip(' ')) {
+            }
+            const int next = integer(",]");
+            if (next <= indices.back()) throw in_.unsupported_next("Unsupported multiple index expression (indices must ascend)");
+            indices.push_back(next);
+        }
+        in_.expect(']');
+        branches(indices);
+    }
+
+    void branches(const std::vector<int>& indices) {
         int deepest = depth_;
-        for (int i = first; i < last; i++) {
+        for (size_t b = 0; b < indices.size(); b++) {
             int base_level = ir_.level;
-            ir_.index(i);
+            ir_.index(indices[b]);
             ir_.down();
             in_.push_mark();
             int saved = depth_;
             if (in_.more()) step();
             if (depth_ > deepest) deepest = depth_;
             depth_ = saved;
-            if (i == last - 1) break;
+            if (b + 1 == indices.size()) break;
             ir_.store();
             in_.pop_mark();
             for (int k = ir_.level - base_level; k > 0; --k) ir_.up();
@@ -265,7 +292,7 @@ class Compiler {
 
 }  // namespace
 
-CompiledPath compile_path(const std::string& path) { return Compiler(path).run(); }
+CompiledPath compile_path(const std::string& path, unsigned extensions) { return Compiler(path, extensions).run(); }
 
 bool validate_bytecode(const uint8_t* ir, size_t len, int max_levels, int max_stores, int* depth,
                        int* stores, std::string* why) {

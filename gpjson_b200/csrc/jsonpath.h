@@ -36,7 +36,18 @@ struct PathError : std::runtime_error {
     PathError(const std::string& m, bool u) : std::runtime_error(m), unsupported(u) {}
 };
 
-CompiledPath compile_path(const std::string& path);
+// Extensions beyond the reference's subset, off by default (with none set,
+// the compiler accepts and rejects exactly what the reference does).
+// kPathIndexUnions: `[i,j,...]` with strictly ascending indices, compiled
+// like the reference's `[a:b]` ranges (one branch per index: index, down,
+// the rest of the path, store, ups back to the array's level), so every
+// index keeps its own result slot.  Descending or repeated indices stay
+// unsupported: the array's elements are visited once, in order.  As after a
+// reference range, an index step later in the path sees the element counter
+// of its array carried over from the previous branch.
+constexpr unsigned kPathIndexUnions = 1u;
+
+CompiledPath compile_path(const std::string& path, unsigned extensions = 0);
 
 // Static check of bytecode handed to the query kernel: opcodes in range,
 // varints of at most 5 bytes with values < 2^31, strings inside the buffer,

@@ -86,6 +86,11 @@ int gpj_set_stream(gpj_ctx *ctx, void *stream);
  * find_value.  Results are identical either way. */
 int gpj_set_query_fusion(gpj_ctx *ctx, int enabled);
 
+/* The JSONPath extensions (GPJ_PATH_* flags, default none) the calls that
+ * take path strings compile with: gpj_query_paths, gpj_query_values,
+ * gpj_batch_add. */
+int gpj_set_path_extensions(gpj_ctx *ctx, unsigned extensions);
+
 /* Library version string, e.g. "gpjson_b200 0.1 sm_100a". */
 const char *gpj_version(void);
 
@@ -100,6 +105,21 @@ const char *gpj_version(void);
  * Returns GPJ_ELIMIT when the bytecode does not fit in `cap`. */
 int gpj_compile(const char *path, uint8_t *out, size_t cap, size_t *len, int *max_depth,
                 int *num_results, char *err, size_t err_cap);
+
+/* JSONPath beyond the reference's subset, off by default: with no flag set,
+ * paths are accepted and rejected exactly as the reference does (which
+ * sends the others to its CPU fallback, JSONPathParser.java:84).
+ * GPJ_PATH_INDEX_UNIONS: `[i,j,...]` with strictly ascending indices,
+ * compiled like the reference's `[a:b]` ranges (one result slot per index,
+ * each branch evaluating the rest of the path, with the ranges' behaviour
+ * for index steps later in the path: their array's element counter carries
+ * over from the previous branch); descending or repeated indices stay
+ * GPJ_EUNSUPPORTED. */
+#define GPJ_PATH_INDEX_UNIONS 1u
+
+/* gpj_compile with the extensions in `extensions` (GPJ_PATH_* flags). */
+int gpj_compile_ex(const char *path, unsigned extensions, uint8_t *out, size_t cap, size_t *len,
+                   int *max_depth, int *num_results, char *err, size_t err_cap);
 
 /* ---- input files ---------------------------------------------------------- */
 

@@ -253,3 +253,36 @@ def test_pipelined_query_equals_load_then_query(gpjson, case):
     if case == "small":
         ref = oracle.query(data.tobytes(), paths)
         assert np.array_equal(want, ref)
+
+
+@pytest.mark.gpu
+def test_index_union_extension(gpjson):
+    """`[i,j]` is rejected as the reference rejects it unless the context
+    enables PATH_INDEX_UNIONS; then each index has its own result slot, equal
+    to the single-index path's results (through query_paths and a batch)."""
+    data = datagen.tweets(2 << 20, seed=datagen.SEED_BASE + 91).tobytes()
+    union, singles = "$.entities.hashtags[0,2].text", ["$.entities.hashtags[0].text", "$.entities.hashtags[2].text"]
+    f = gpjson.load_bytes(data)
+    try:
+        with pytest.raises(gj.UnsupportedJSONPathException):
+            f.query_paths([union])
+        gpjson.set_path_extensions(gj.PATH_INDEX_UNIONS)
+        try:
+            got = f.query_paths([union, "$.id"])
+            b = gpjson.batch()
+            try:
+                it = b.add(f, [union])
+                b.run()
+                got_batch = b.result(it)
+            finally:
+                b.release()
+        finally:
+            gpjson.set_path_extensions(0)
+        want = f.query_paths(singles)
+    finally:
+        f.release()
+    assert got.shape[2] == 2
+    for k in range(2):
+        assert np.array_equal(got[0, :, k], want[k, :, 0])
+        assert np.array_equal(got_batch[0, :, k], want[k, :, 0])
+    assert (got[0, :, 1, 0] >= 0).sum() > 0 and (got[1, :, 1] == -1).all()

@@ -215,3 +215,56 @@ def test_classification_every_byte_value(hostsim):
     for k, flags in enumerate(classes):
         want = (flags.astype(np.uint64) * weights).sum(axis=1, dtype=np.uint64)
         assert np.array_equal(got[:, k], want), k
+
+
+def test_index_union_slots_equal_single_indices(hostsim):
+    """A union path `...[i,j,k]...` (the PATH_INDEX_UNIONS extension) gives
+    in slot b what the path with the single index of branch b gives, line by
+    line, under the device interpreter (compiled here, checked against the
+    oracle's evaluation of the single-index paths).  Unions compile like the
+    reference's ranges, so an index step after one behaves as after a range
+    in the reference (the inner array's element counter carries over from
+    one branch to the next: only the first branch finds its element); those
+    paths are checked against the equivalent range instead."""
+    import gpjson_b200 as gj
+
+    rng = random.Random(17)
+    docs = [
+        b'{"a":[{"b":0},{"b":1},{"b":2},{"b":[3]},{"c":4}],"x":{"y":[[1,2],[3],[],[4,[5,6]]]}}',
+        b'{"a":[ 10 , {"b":"q"} ,[1,{"b":2}], "s" ],"x":{"y":[]}}',
+        b'{"a":[],"x":{"y":[[0],[1],[2],[3]]}}',
+        b'{"a":{"b":1},"x":[1,2,3]}',
+        b'  {"x":{"y":[[ ], [ 7 , 8 , 9 ] , [{"z":1}] ]}, "a":[{"b":{"c":[1,2,3]}},{}]}',
+    ]
+    unions = {
+        "$.a[0,2,3].b": ["$.a[0].b", "$.a[2].b", "$.a[3].b"],
+        "$.a[1,4]": ["$.a[1]", "$.a[4]"],
+        "$.x.y[0,3]": ["$.x.y[0]", "$.x.y[3]"],
+        # an index step after the union: as after the range over the same indices
+        "$.x.y[1,2][0,1]": ["$.x.y[1:3][0:2]"],
+    }
+    for _ in range(20):
+        lines = [rng.choice(docs) for _ in range(rng.randint(1, 12))]
+        data = b"\n".join(lines)
+        f = np.frombuffer(data, dtype=np.uint8)
+        for union, singles in unions.items():
+            c = gj.compile_path(union, gj.PATH_INDEX_UNIONS)
+            idx = oracle.Index(data, c.max_depth)
+            irb = np.frombuffer(c.bytecode, dtype=np.uint8)
+            ptrs = (ctypes.c_void_p * 1)(irb.ctypes.data)
+            got = np.empty((1, len(idx.newlines), c.num_results, 2), dtype=np.int64)
+            hostsim.hs_find_values(f.ctypes.data, f.size, idx.newlines.ctypes.data, len(idx.newlines),
+                                   idx.strings.ctypes.data, idx.levels.ctypes.data, 1, ptrs, c.num_results,
+                                   got.ctypes.data, None, 0)
+            if len(singles) == 1:  # the equivalent range: all slots
+                ir, depth, slots = oracle.compile_path(singles[0])
+                sidx = oracle.Index(data, depth)
+                want = oracle.find_value(data, sidx.newlines, sidx.strings, sidx.levels, depth, ir, slots)
+                assert np.array_equal(got[0], want), (union, data[:80])
+                continue
+            assert c.num_results == len(singles)
+            for b, single in enumerate(singles):
+                ir, depth, slots = oracle.compile_path(single)
+                sidx = oracle.Index(data, depth)
+                want = oracle.find_value(data, sidx.newlines, sidx.strings, sidx.levels, depth, ir, slots)
+                assert np.array_equal(got[0, :, b], want[:, 0]), (union, single, data[:80])

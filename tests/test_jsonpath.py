@@ -152,3 +152,26 @@ def test_native_matches_oracle_random():
         except gj.JSONPathException:
             got, gerr = None, "parse"
         assert (got, gerr) == (want, werr), path
+
+
+def test_index_unions_are_an_opt_in_extension():
+    """`[i,j,...]` (strictly ascending) compiles only with PATH_INDEX_UNIONS,
+    to the same branches as the reference's ranges: a union of consecutive
+    indices is byte-identical to the range over them."""
+    with pytest.raises(gj.UnsupportedJSONPathException):
+        gj.compile_path("$.a[1,2].b")
+    ext = gj.PATH_INDEX_UNIONS
+    for union, rng in (("$.a[1,2].b", "$.a[1:3].b"), ("$[0,1,2]", "$[0:3]"), ("$.x[4, 5].y[0,1]", "$.x[4:6].y[0:2]")):
+        u, r = gj.compile_path(union, ext), gj.compile_path(rng)
+        assert (u.bytecode, u.max_depth, u.num_results) == (r.bytecode, r.max_depth, r.num_results), union
+    c = gj.compile_path("$.a[1,3,7].b", ext)
+    assert c.num_results == 3 and c.max_depth == gj.compile_path("$.a[1:2].b").max_depth
+    for bad in ("$[3,1]", "$[1,1]", "$[0,2,2]"):
+        with pytest.raises(gj.UnsupportedJSONPathException):
+            gj.compile_path(bad, ext)
+    for bad in ("$[1,]", "$[1,x]", "$[1,2"):
+        with pytest.raises(gj.JSONPathException) as ei:
+            gj.compile_path(bad, ext)
+        assert not isinstance(ei.value, gj.UnsupportedJSONPathException)
+    # without the flag, errors and bytecode stay the reference's
+    assert gj.compile_path("$.a[1:3].b", ext).bytecode == gj.compile_path("$.a[1:3].b").bytecode
