@@ -131,7 +131,7 @@ int gpj_file_open(gpj_ctx *ctx, const char *filename, gpj_file **out);
 int gpj_file_from_host(gpj_ctx *ctx, const void *data, int64_t n, gpj_file **out);
 
 /* gpj_file_from_host followed by gpj_index_build, pipelined: the input is
- * copied in 64 MiB chunks on a second stream while the index kernel indexes
+ * copied in 56 MiB chunks on a second stream while the index kernel indexes
  * each chunk as soon as the chunk after it has arrived, so the copy and the
  * index build overlap (the reference reads and copies the whole file before
  * its first kernel, QueryFunction.java:316-335).  Same index as

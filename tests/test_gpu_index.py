@@ -147,7 +147,7 @@ def indexes_of(f, levels):
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["ndjson", "long_line", "newline_in_string"])
 def test_pipelined_load_and_index(gpjson, case):
-    """gpj_file_from_host_indexed (64 MiB chunks copied while earlier chunks
+    """gpj_file_from_host_indexed (56 MiB chunks copied while earlier chunks
     are indexed) equals the plain copy + index build, including inputs that
     need the rebuild: a line longer than a chunk, a raw newline in a string."""
     base = datagen.tweets(150 << 20)
