@@ -94,7 +94,7 @@ cudaError_t launch_line_index_kernel(const IndexParams& p, int grid, cudaStream_
 int line_index_max_ctas_per_sm(int num_levels);
 
 // Standalone form of the line-parallel kernel for index builds without
-// in-kernel queries: the index warps alone (five CTAs per SM), no tile
+// in-kernel queries: the index warps alone (up to five CTAs per SM), no tile
 // depending on another; writes string index and leveled bitmaps, and
 // newline_bits + tile_newlines instead of the newline index (same error
 // flags).  launch_newline_index then builds the newline index.

@@ -977,7 +977,8 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
         line_warps<LV>(p, sh);
 }
 
-// Index only: the index warps alone, five CTAs per SM; no tile waits for
+// Index only: the index warps alone, up to five CTAs per SM (at 4 levels; the
+// level slots of deeper indexes take more shared memory); no tile waits for
 // another, since the newline index is built afterwards from the counts.
 template <int LV>
 __global__ void __launch_bounds__(kIndexThreads, 5) tile_index_kernel(IndexParams p) {
