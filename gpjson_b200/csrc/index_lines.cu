@@ -977,11 +977,13 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
         line_warps<LV>(p, sh);
 }
 
-// Index only: the index warps alone, up to five CTAs per SM (at 4 levels; the
-// level slots of deeper indexes take more shared memory); no tile waits for
-// another, since the newline index is built afterwards from the counts.
+// Index only: the index warps alone, five CTAs per SM at up to 4 levels (48
+// registers), four at up to 8 and three at 16 (the level slots of deeper
+// indexes take more shared memory, so registers need no tighter cap); no
+// tile waits for another, since the newline index is built afterwards from
+// the counts.
 template <int LV>
-__global__ void __launch_bounds__(kIndexThreads, 5) tile_index_kernel(IndexParams p) {
+__global__ void __launch_bounds__(kIndexThreads, LV <= 4 ? 5 : (LV <= 8 ? 4 : 3)) tile_index_kernel(IndexParams p) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
     TShared<LV>& sh = *reinterpret_cast<TShared<LV>*>(smem_raw);
     if (threadIdx.x == 0) {
