@@ -367,7 +367,10 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
         TileScratch ts;
         rc = alloc_tile_scratch(ctx, n, &ts);
         if (!rc) {
-            GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
+            const cudaError_t e = cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream);
+            if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemsetAsync(status)");
+        }
+        if (!rc) {
             fused.newline_bits = ts.bits;
             fused.tile_newlines = ts.counts;
             fused.colon = d_colon;
@@ -400,6 +403,13 @@ int check_ctx(gpj_ctx* ctx) {
     if (!ctx) return GPJ_EINVAL;
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+    return GPJ_OK;
+}
+
+// A file is used with the context that made it (its buffers live in that
+// context's pool and are ordered on that context's stream).
+int check_file(gpj_ctx* ctx, const gpj_file* f) {
+    if (!f || f->ctx != ctx) return fail(ctx, GPJ_EINVAL, "file does not belong to this context");
     return GPJ_OK;
 }
 
@@ -605,19 +615,23 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         rc = alloc_tile_scratch(ctx, n, &ts);
         int64_t* d_lines = nullptr;  // [k + 1]: lines complete after chunk k
         if (!rc && cq) rc = device_alloc(ctx, &d_lines, static_cast<size_t>(nchunks + 1), "cudaMalloc(chunk lines)");
+        if (!rc) {
+            cudaError_t e = cq ? cudaMemsetAsync(d_lines, 0, sizeof(int64_t), ctx->stream) : cudaSuccess;
+            if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream);
+            // the copies start once the buffers exist (pool allocations are ordered on ctx->stream)
+            if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_ready, ctx->stream);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0);
+            if (e != cudaSuccess) rc = cuda_fail(ctx, e, "chunked index setup");
+        }
         if (rc) {
             free_tile_scratch(ctx, &ts);
             device_free(ctx, d_lines);
+            f->colon_valid = false;
             return rc;
         }
-        if (cq) GPJ_CUDA(ctx, cudaMemsetAsync(d_lines, 0, sizeof(int64_t), ctx->stream));
-        GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream));
         p.status = ctx->d_status;
         p.newline_bits = ts.bits;
         p.tile_newlines = ts.counts;
-        // the copies start once the buffers exist (pool allocations are ordered on ctx->stream)
-        GPJ_CUDA(ctx, cudaEventRecord(ctx->ev_ready, ctx->stream));
-        GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0));
         auto launch_chunk = [&](int64_t k) -> int {
             const int64_t t0 = k * kLoadTiles, t1 = std::min(p.ntiles, (k + 1) * kLoadTiles);
             set_tile_range(&p, t0, t1, std::min(n, (k + 2) * kLoadChunk));
@@ -1237,7 +1251,8 @@ int gpj_index_num_lines(const gpj_file* f, int64_t* lines) {
 int gpj_index_copy_newlines(gpj_ctx* ctx, const gpj_file* f, int64_t* host, int64_t count) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!f || !host) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if ((rc = check_file(ctx, f))) return rc;
+    if (!host) return fail(ctx, GPJ_EINVAL, "bad arguments");
     if (!f->indexed) return fail(ctx, GPJ_ESTATE, "file is not indexed");
     if (count < f->num_lines) return fail(ctx, GPJ_EINVAL, "host buffer too small");
     GPJ_CUDA(ctx, cudaMemcpyAsync(host, f->d_nl, f->num_lines * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1248,7 +1263,8 @@ int gpj_index_copy_newlines(gpj_ctx* ctx, const gpj_file* f, int64_t* host, int6
 int gpj_index_copy_string_index(gpj_ctx* ctx, const gpj_file* f, uint64_t* host, int64_t count) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!f || (!host && f->words > 0)) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if ((rc = check_file(ctx, f))) return rc;
+    if (!host && f->words > 0) return fail(ctx, GPJ_EINVAL, "bad arguments");
     if (!f->indexed) return fail(ctx, GPJ_ESTATE, "file is not indexed");
     if (count < f->words) return fail(ctx, GPJ_EINVAL, "host buffer too small");
     if (f->words == 0) return GPJ_OK;
@@ -1260,7 +1276,8 @@ int gpj_index_copy_string_index(gpj_ctx* ctx, const gpj_file* f, uint64_t* host,
 int gpj_index_copy_leveled_bitmaps(gpj_ctx* ctx, const gpj_file* f, uint64_t* host, int64_t count) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!f || (!host && f->words > 0)) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if ((rc = check_file(ctx, f))) return rc;
+    if (!host && f->words > 0) return fail(ctx, GPJ_EINVAL, "bad arguments");
     if (!f->indexed) return fail(ctx, GPJ_ESTATE, "file is not indexed");
     const int64_t total = f->words * f->num_levels;
     if (count < total) return fail(ctx, GPJ_EINVAL, "host buffer too small");
@@ -1298,7 +1315,8 @@ int gpj_query(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, const
               int slots, int64_t* host_out, int64_t out_count) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!f || !bc || !len || !host_out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if ((rc = check_file(ctx, f))) return rc;
+    if (!bc || !len || !host_out) return fail(ctx, GPJ_EINVAL, "bad arguments");
     if (f->indexed) {
         rc = ensure_out(ctx, f, static_cast<size_t>(std::max(nq, 1)) * f->num_lines * std::max(slots, 1) * 2);
         if (rc) return rc;
@@ -1310,7 +1328,8 @@ int gpj_query_device(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc
                      int slots, int64_t* d_out, int64_t out_count) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!f || !bc || !len || !d_out) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if ((rc = check_file(ctx, f))) return rc;
+    if (!bc || !len || !d_out) return fail(ctx, GPJ_EINVAL, "bad arguments");
     return query_common(ctx, f, nq, bc, len, slots, d_out, out_count, false, nullptr);
 }
 
@@ -1327,7 +1346,8 @@ static int run_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths
                      int64_t* cap_out) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!f || !paths) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if ((rc = check_file(ctx, f))) return rc;
+    if (!paths) return fail(ctx, GPJ_EINVAL, "bad arguments");
     if (nq > GPJ_MAX_QUERIES) return fail(ctx, GPJ_ELIMIT, "Maximum size of queries is 255");
     if (nq < 1) return fail(ctx, GPJ_EINVAL, "expected queries to contain at least one query");
     std::vector<gpj::CompiledPath> compiled(static_cast<size_t>(nq));
@@ -1431,7 +1451,8 @@ int gpj_values_device(gpj_ctx* ctx, gpj_file* f, const int64_t* d_pairs, int64_t
                       int64_t* d_offsets, uint8_t* d_bytes, int64_t bytes_cap, int64_t* total_bytes) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
-    if (!f || npairs < 0 || (npairs > 0 && (!d_pairs || !d_kinds)) || !d_offsets || bytes_cap < 0 ||
+    if ((rc = check_file(ctx, f))) return rc;
+    if (npairs < 0 || (npairs > 0 && (!d_pairs || !d_kinds)) || !d_offsets || bytes_cap < 0 ||
         (bytes_cap > 0 && !d_bytes) || !total_bytes)
         return fail(ctx, GPJ_EINVAL, "bad arguments");
     const double t0 = now_ms();

@@ -19,6 +19,9 @@
  *  - Host output buffers are owned by the caller; device buffers are owned by
  *    the gpj_file they belong to, except where a function takes device
  *    pointers explicitly.
+ *  - A gpj_file is used with the context that made it; the other contexts'
+ *    entry points refuse it with GPJ_EINVAL (gpj_batch_add alone takes
+ *    files of other contexts on the same device).
  *  - One gpj_ctx must not be used by two threads at the same time.
  *  - All device work of a context runs on one CUDA stream (gpj_set_stream).
  */

@@ -202,6 +202,31 @@ def test_errors(gpjson):
         gpjson.query(str(FIXTURES / "does-not-exist.ldjson"), "$.a")
 
 
+@pytest.mark.gpu
+def test_file_of_another_context(gpjson):
+    """A file is used only with the context that made it: the query and
+    index-read entry points refuse another context's file (GPJ_EINVAL)
+    and leave it usable by its own."""
+    other = gj.GPJSON(0)
+    f = gpjson.load_bytes(b'{"a":1}\n{"a":[2]}\n')
+    foreign = gj.File(other._native, f._h)  # the same handle through the other context
+    try:
+        f.build_index(2)
+        q = [gj.compile_path("$.a")]
+        with pytest.raises(gj.GPJSONException) as e:
+            foreign.run(q)
+        assert e.value.code == gj._lib.GPJ_EINVAL
+        with pytest.raises(gj.GPJSONException):
+            foreign.query_paths(["$.a"])
+        with pytest.raises(gj.GPJSONException):
+            foreign.newline_index()
+        assert f.run(q)[0, :, 0, 0].tolist() == [5, 13, -1]
+    finally:
+        foreign._h = None  # the handle is f's to release
+        f.release()
+        other.close()
+
+
 def _pipelined_case(case: str) -> tuple[np.ndarray, list[str]]:
     if case == "small":
         return datagen.tweets(1 << 20, seed=datagen.SEED_BASE + 61), TWEET_PATHS
