@@ -6,12 +6,20 @@
 // functions/QueryFunction.java:48-265 and the stages/ classes.
 #include <cuda_runtime.h>
 
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <cerrno>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <condition_variable>
+#include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/gpjson_b200.h"
@@ -836,6 +844,99 @@ int gather_values(gpj_ctx* ctx, gpj_file* f, const int64_t* d_pairs, int64_t npa
     return rc;
 }
 
+// Reads byte ranges of a file into host memory with up to `threads`
+// threads: each range is cut into one slice per thread, read concurrently
+// by preads.  A file load is bound by this copy out of the page cache,
+// which one thread does at a fraction of host memory bandwidth.  The
+// workers live for one load, so a range costs two condition-variable
+// round trips, not thread starts.
+class SliceReader {
+  public:
+    SliceReader(int fd, int threads) : fd_(fd) {
+        try {
+            for (int i = 1; i < threads; i++) workers_.emplace_back([this, i] { work(i); });
+        } catch (const std::exception&) {
+            // fewer threads than asked: the ranges are cut into fewer slices
+        }
+        parts_ = static_cast<int>(workers_.size()) + 1;
+    }
+
+    ~SliceReader() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            quit_ = true;
+        }
+        go_.notify_all();
+        for (auto& t : workers_) t.join();
+    }
+
+    // Bytes [pos, pos + len) into dst; false on an I/O error or a short
+    // read (the file shrank).
+    bool read(uint8_t* dst, int64_t pos, size_t len) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            dst_ = dst;
+            pos_ = pos;
+            len_ = len;
+            ok_ = true;
+            pending_ = parts_ - 1;
+            ++round_;
+        }
+        go_.notify_all();
+        const bool mine = read_slice(0);
+        std::unique_lock<std::mutex> g(mu_);
+        done_.wait(g, [this] { return pending_ == 0; });
+        return mine && ok_;
+    }
+
+  private:
+    // Slice i of the current range (the range is fixed until every slice is read).
+    bool read_slice(int i) const {
+        const size_t slice = (len_ + parts_ - 1) / parts_;
+        const size_t off = std::min(len_, slice * static_cast<size_t>(i));
+        const size_t want = std::min(slice, len_ - off);
+        size_t got = 0;
+        while (got < want) {
+            const ssize_t r = ::pread(fd_, dst_ + off + got, want - got, static_cast<off_t>(pos_ + off + got));
+            if (r < 0 && errno == EINTR) continue;
+            if (r <= 0) return false;
+            got += static_cast<size_t>(r);
+        }
+        return true;
+    }
+
+    void work(int i) {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                go_.wait(g, [&] { return quit_ || round_ != seen; });
+                if (quit_) return;
+                seen = round_;
+            }
+            const bool ok = read_slice(i);
+            {
+                std::lock_guard<std::mutex> g(mu_);
+                ok_ = ok_ && ok;
+                --pending_;
+            }
+            done_.notify_one();
+        }
+    }
+
+    const int fd_;
+    int parts_ = 1;
+    std::vector<std::thread> workers_;
+    std::mutex mu_;
+    std::condition_variable go_, done_;
+    uint64_t round_ = 0;
+    int pending_ = 0;
+    bool ok_ = true, quit_ = false;
+    uint8_t* dst_ = nullptr;
+    int64_t pos_ = 0;
+    size_t len_ = 0;
+};
+
 }  // namespace
 
 extern "C" {
@@ -1142,65 +1243,70 @@ int gpj_file_open(gpj_ctx* ctx, const char* filename, gpj_file** out) {
     int rc = check_ctx(ctx);
     if (rc) return rc;
     if (!filename || !out) return fail(ctx, GPJ_EINVAL, "bad arguments");
-    FILE* fp = std::fopen(filename, "rb");
-    if (!fp) return fail(ctx, GPJ_EIO, std::string("Failed to open file ") + filename);
-    std::fseek(fp, 0, SEEK_END);
-    const int64_t n = static_cast<int64_t>(std::ftell(fp));
-    std::fseek(fp, 0, SEEK_SET);
-    if (n < 0) {
-        std::fclose(fp);
+    const int fd = ::open(filename, O_RDONLY | O_CLOEXEC);
+    if (fd < 0) return fail(ctx, GPJ_EIO, std::string("Failed to open file ") + filename);
+    struct stat st;
+    if (::fstat(fd, &st) != 0 || !S_ISREG(st.st_mode) || st.st_size < 0) {
+        ::close(fd);
         return fail(ctx, GPJ_EIO, std::string("Failed to get size of file ") + filename);
     }
+    const int64_t n = static_cast<int64_t>(st.st_size);
     gpj_file* f = nullptr;
     rc = make_file(ctx, n, &f);
     if (rc) {
-        std::fclose(fp);
+        ::close(fd);
         return rc;
     }
     rc = device_alloc(ctx, &f->d_owned, static_cast<size_t>(n), "cudaMalloc(file)");
     if (rc) {
-        std::fclose(fp);
+        ::close(fd);
         delete f;
         return rc;
     }
     f->d_data = f->d_owned;
-    // Two pinned halves: the disk read of one chunk overlaps the copy of the other.
+    // Two pinned halves: the read of one chunk overlaps the copy of the other.
     const size_t chunk = 32u << 20;
     if (!ctx->h_stage) {
         cudaError_t e = cudaMallocHost(&ctx->h_stage, 2 * chunk);
         if (e != cudaSuccess) {
-            std::fclose(fp);
+            ::close(fd);
             gpj_file_release(f);
             return cuda_fail(ctx, e, "cudaMallocHost(staging)");
         }
         ctx->stage_bytes = 2 * chunk;
     }
+    // one reader thread per 2 MiB of a chunk, at most one per host thread (and 16)
+    const int threads = static_cast<int>(std::min<int64_t>(
+        std::min<int64_t>(16, std::max(1u, std::thread::hardware_concurrency())), std::max<int64_t>(1, n >> 21)));
     const double t0 = now_ms();
     cudaEventRecord(ctx->ev0, ctx->stream);
     cudaEvent_t done[2] = {nullptr, nullptr};
     cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
-    int64_t pos = 0;
-    int half = 0;
     rc = GPJ_OK;
-    while (pos < n) {
-        const size_t want = static_cast<size_t>(std::min<int64_t>(static_cast<int64_t>(chunk), n - pos));
-        uint8_t* stage = ctx->h_stage + half * chunk;
-        cudaEventSynchronize(done[half]);  // the copy that last used this half is done
-        if (std::fread(stage, 1, want, fp) != want) {
-            rc = fail(ctx, GPJ_EIO, std::string("Size of file has changed while reading ") + filename);
-            break;
+    {
+        SliceReader reader(fd, threads);
+        int64_t pos = 0;
+        int half = 0;
+        while (pos < n) {
+            const size_t want = static_cast<size_t>(std::min<int64_t>(static_cast<int64_t>(chunk), n - pos));
+            uint8_t* stage = ctx->h_stage + half * chunk;
+            cudaEventSynchronize(done[half]);  // the copy that last used this half is done
+            if (!reader.read(stage, pos, want)) {
+                rc = fail(ctx, GPJ_EIO, std::string("Size of file has changed while reading ") + filename);
+                break;
+            }
+            cudaError_t e = cudaMemcpyAsync(f->d_owned + pos, stage, want, cudaMemcpyHostToDevice, ctx->stream);
+            if (e != cudaSuccess) {
+                rc = cuda_fail(ctx, e, "cudaMemcpyAsync(file)");
+                break;
+            }
+            cudaEventRecord(done[half], ctx->stream);
+            pos += static_cast<int64_t>(want);
+            half ^= 1;
         }
-        cudaError_t e = cudaMemcpyAsync(f->d_owned + pos, stage, want, cudaMemcpyHostToDevice, ctx->stream);
-        if (e != cudaSuccess) {
-            rc = cuda_fail(ctx, e, "cudaMemcpyAsync(file)");
-            break;
-        }
-        cudaEventRecord(done[half], ctx->stream);
-        pos += static_cast<int64_t>(want);
-        half ^= 1;
     }
-    std::fclose(fp);
+    ::close(fd);
     if (rc == GPJ_OK) rc = end_phase(ctx, "read_file", t0);
     else cudaStreamSynchronize(ctx->stream);
     cudaEventDestroy(done[0]);

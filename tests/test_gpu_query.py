@@ -203,6 +203,35 @@ def test_errors(gpjson):
 
 
 @pytest.mark.gpu
+def test_file_open_reads_every_chunk(gpjson, tmp_path):
+    """gpj_file_open reads 32 MiB chunks, each as slices read concurrently:
+    a file of several chunks with a ragged tail holds the same bytes on the
+    device as the input loaded from memory (the values of large members, the
+    string and newline indexes, the query results); a directory fails like
+    a missing file."""
+    data = np.concatenate([datagen.tweets(100 << 20, seed=datagen.SEED_BASE + 77),
+                           np.frombuffer(b'{"id": 7}', dtype=np.uint8)])
+    path = tmp_path / "chunks.ldjson"
+    data.tofile(path)
+    f = gpjson.open(path)
+    g = gpjson.load_bytes(data)
+    try:
+        assert f.size == data.size
+        members = ["$.text", "$.user", "$.source", "$.entities"]
+        got, want = f.query_values(members), g.query_values(members)
+        assert got.data == want.data and np.array_equal(got.offsets, want.offsets)
+        assert len(got.data) > data.size // 2
+        assert np.array_equal(f.query_paths(TWEET_PATHS), g.query_paths(TWEET_PATHS))
+        assert np.array_equal(f.string_index(), g.string_index())
+        assert np.array_equal(f.newline_index(), g.newline_index())
+    finally:
+        f.release()
+        g.release()
+    with pytest.raises(gj.GPJSONException):
+        gpjson.open(tmp_path)
+
+
+@pytest.mark.gpu
 def test_file_of_another_context(gpjson):
     """A file is used only with the context that made it: the query and
     index-read entry points refuse another context's file (GPJ_EINVAL)
