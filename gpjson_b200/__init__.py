@@ -397,15 +397,7 @@ class File:
         arr = (c_char_p * len(paths))(*[p.encode("utf-8") for p in paths])
         r = c_void_p()
         self._native.check(self._native.lib.gpj_query_paths(self._native.h, self._h, len(paths), arr, byref(r)))
-        lib = self._native.lib
-        try:
-            nq, lines, slots = lib.gpj_result_num_queries(r), lib.gpj_result_num_lines(r), lib.gpj_result_slots(r)
-            count = nq * lines * slots * 2
-            ptr = lib.gpj_result_offsets(r)
-            buf = (ctypes.c_int64 * count).from_address(ptr) if count else []
-            return np.array(buf, dtype=np.int64, copy=True).reshape(nq, lines, slots, 2)
-        finally:
-            lib.gpj_result_release(r)
+        return _result_array(self._native.lib, r)
 
     def query_values(self, paths: list[str]) -> Values:
         """gpj_query_values: the paths evaluated as by query_paths and the
@@ -451,16 +443,33 @@ class File:
             pass
 
 
+class _ResultBuffer:
+    """Owns a gpj_result and exposes its offsets to numpy without a copy;
+    arrays made from it keep it (and so the native result) alive."""
+
+    def __init__(self, lib, r, count: int):
+        self._lib, self._r = lib, r
+        self.__array_interface__ = {
+            "shape": (count,), "typestr": "<i8", "data": (lib.gpj_result_offsets(r), False), "version": 3,
+        }
+
+    def __del__(self):
+        if self._r:
+            self._lib.gpj_result_release(self._r)
+            self._r = None
+
+
 def _result_array(lib, r) -> np.ndarray:
-    """Copies a gpj_result into int64 [nq][lines][slots][2] and releases it."""
+    """int64 [nq][lines][slots][2] over a gpj_result's offsets (no copy: the
+    array owns the result and releases it when it is collected)."""
     try:
         nq, lines, slots = lib.gpj_result_num_queries(r), lib.gpj_result_num_lines(r), lib.gpj_result_slots(r)
         count = nq * lines * slots * 2
-        ptr = lib.gpj_result_offsets(r)
-        buf = (ctypes.c_int64 * count).from_address(ptr) if count else []
-        return np.array(buf, dtype=np.int64, copy=True).reshape(nq, lines, slots, 2)
-    finally:
+        holder = _ResultBuffer(lib, r, count)
+    except BaseException:
         lib.gpj_result_release(r)
+        raise
+    return np.asarray(holder).reshape(nq, lines, slots, 2)
 
 
 class Batch:

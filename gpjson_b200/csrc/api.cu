@@ -13,9 +13,9 @@
 #include <algorithm>
 #include <cerrno>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
-#include <condition_variable>
 #include <mutex>
 #include <new>
 #include <string>
@@ -105,10 +105,76 @@ struct gpj_file {
     size_t d_out_cap = 0;  // elements
 };
 
+namespace {
+
+// Host memory for results.  A new buffer's first touch (page faults) costs
+// several times the device-to-host copy into it, and a copy that faults in
+// its own pages is slower still, so the largest released buffer (up to
+// kKeepElems) is kept for the next result of the process, and a new one is
+// touched once before the copy.
+class ResultBuffers {
+  public:
+    static constexpr size_t kKeepElems = size_t(64) << 20;  // 512 MiB
+
+    int64_t* take(size_t count, size_t* cap) {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            if (kept_ && kept_cap_ >= count) {
+                int64_t* p = kept_;
+                *cap = kept_cap_;
+                kept_ = nullptr;
+                kept_cap_ = 0;
+                return p;
+            }
+        }
+        int64_t* p = new (std::nothrow) int64_t[count];
+        if (p) std::memset(p, 0, count * sizeof(int64_t));
+        *cap = count;
+        return p;
+    }
+
+    void give(int64_t* p, size_t cap) {
+        if (!p) return;
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            if (cap <= kKeepElems && cap > kept_cap_) {
+                std::swap(p, kept_);
+                std::swap(cap, kept_cap_);
+            }
+        }
+        delete[] p;
+    }
+
+  private:
+    std::mutex mu_;
+    int64_t* kept_ = nullptr;
+    size_t kept_cap_ = 0;
+};
+
+// Never destroyed, so that results released during process exit find it.
+ResultBuffers& result_buffers() {
+    static ResultBuffers* b = new ResultBuffers;
+    return *b;
+}
+
+}  // namespace
+
 struct gpj_result {
     int64_t nq = 0, lines = 0;
     int slots = 0;
-    std::vector<int64_t> offsets;
+    // [nq][lines][slots][2], every element copied in
+    int64_t* offsets = nullptr;
+    size_t cap = 0;  // elements of `offsets`
+
+    gpj_result() = default;
+    gpj_result(const gpj_result&) = delete;
+    gpj_result& operator=(const gpj_result&) = delete;
+    ~gpj_result() { result_buffers().give(offsets, cap); }
+
+    bool allocate(size_t count) {
+        offsets = result_buffers().take(std::max<size_t>(count, 1), &cap);
+        return offsets != nullptr;
+    }
 };
 
 // Values of a query call gathered on the device (gpj_query_values).
@@ -1522,16 +1588,14 @@ int gpj_query_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths,
     r->lines = f->num_lines;
     r->slots = slots;
     const size_t per_query = static_cast<size_t>(f->num_lines) * slots * 2;
-    try {
-        r->offsets.resize(static_cast<size_t>(nq) * per_query);
-    } catch (const std::bad_alloc&) {
+    if (!r->allocate(static_cast<size_t>(nq) * per_query)) {
         delete r;
         return fail(ctx, GPJ_ENOMEM, "out of host memory for results");
     }
     const double t1 = now_ms();
     cudaEventRecord(ctx->ev0, ctx->stream);
     for (int q = 0; q < nq; q++) {
-        cudaError_t e = cudaMemcpyAsync(r->offsets.data() + q * per_query, f->d_out + static_cast<size_t>(q) * cap * slots * 2,
+        cudaError_t e = cudaMemcpyAsync(r->offsets + q * per_query, f->d_out + static_cast<size_t>(q) * cap * slots * 2,
                                         per_query * 8, cudaMemcpyDeviceToHost, ctx->stream);
         if (e != cudaSuccess) {
             delete r;
@@ -1550,7 +1614,7 @@ int gpj_query_paths(gpj_ctx* ctx, gpj_file* f, int nq, const char* const* paths,
 int64_t gpj_result_num_queries(const gpj_result* r) { return r ? r->nq : -1; }
 int64_t gpj_result_num_lines(const gpj_result* r) { return r ? r->lines : -1; }
 int gpj_result_slots(const gpj_result* r) { return r ? r->slots : -1; }
-const int64_t* gpj_result_offsets(const gpj_result* r) { return r ? r->offsets.data() : nullptr; }
+const int64_t* gpj_result_offsets(const gpj_result* r) { return r ? r->offsets : nullptr; }
 void gpj_result_release(gpj_result* r) { delete r; }
 
 int gpj_values_device(gpj_ctx* ctx, gpj_file* f, const int64_t* d_pairs, int64_t npairs, uint8_t* d_kinds,
@@ -1961,12 +2025,11 @@ int gpj_batch_result(gpj_batch* b, int item, gpj_result** out) {
     r->slots = fr.slots;
     const size_t per_query = static_cast<size_t>(fr.lines) * fr.slots * 2;
     const int64_t* src = b->results + fr.out_offset + it.q0 * per_query;
-    try {
-        r->offsets.assign(src, src + r->nq * per_query);
-    } catch (const std::bad_alloc&) {
+    if (!r->allocate(static_cast<size_t>(r->nq) * per_query)) {
         delete r;
         return fail(ctx, GPJ_ENOMEM, "out of host memory for results");
     }
+    std::memcpy(r->offsets, src, static_cast<size_t>(r->nq) * per_query * sizeof(int64_t));
     *out = r;
     return GPJ_OK;
 }

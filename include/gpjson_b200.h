@@ -282,6 +282,9 @@ int64_t gpj_result_num_lines(const gpj_result *r);
 int gpj_result_slots(const gpj_result *r);
 /* Pointer to int64[num_queries][num_lines][slots][2], valid until release. */
 const int64_t *gpj_result_offsets(const gpj_result *r);
+/* The memory of the largest released result (up to 512 MiB) is kept for
+ * the next result of the process: its pages are already mapped, which
+ * makes that result's copy from the device several times cheaper. */
 void gpj_result_release(gpj_result *r);
 
 /* ---- values ------------------------------------------------------------------ */

@@ -129,3 +129,48 @@ def test_values_view_follows_result_item():
     assert v[-1][-1][:] == ['12"été"�']
     with pytest.raises(IndexError):
         v[0][4]
+
+
+def test_result_array_is_a_view_that_owns_the_result():
+    """Result offsets reach numpy without a copy: the array reads the native
+    result's memory, and the result is released once, when the last array
+    over it is collected."""
+    import ctypes
+    import gc
+
+    import numpy as np
+
+    from gpjson_b200 import _result_array
+
+    store = (ctypes.c_int64 * 12)(*range(12))
+    released = []
+
+    class FakeLib:  # the gpj_result accessors of the C ABI
+        def gpj_result_num_queries(self, r):
+            return 2
+
+        def gpj_result_num_lines(self, r):
+            return 3
+
+        def gpj_result_slots(self, r):
+            return 1
+
+        def gpj_result_offsets(self, r):
+            return ctypes.addressof(store)
+
+        def gpj_result_release(self, r):
+            released.append(r.value)
+
+    a = _result_array(FakeLib(), ctypes.c_void_p(0x1234))
+    assert a.shape == (2, 3, 1, 2) and a.dtype == np.int64
+    assert a.reshape(-1).tolist() == list(range(12))
+    store[5] = 99  # the array reads the result's memory
+    assert a[0, 2, 0, 1] == 99
+    q0 = a[0]
+    del a
+    gc.collect()
+    assert released == []  # a slice still holds the result
+    assert q0[1, 0, 0] == 2
+    del q0
+    gc.collect()
+    assert released == [0x1234]
