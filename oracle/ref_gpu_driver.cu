@@ -179,7 +179,7 @@ __attribute__((visibility("default"))) int ref_gpu_run(const uint8_t* host, int6
             REF_CHECK(cudaDeviceSynchronize());
             return 0;
         };
-        for (int r = 0; r <= repeats; r++) {  // round 0 untimed
+        for (int r = 0; r <= repeats; r++) {  // repeat 0 untimed (warm-up)
             const double t0 = now_ms();
             int rc = build_index(b, n, num_levels, &count);
             if (rc) return rc;
