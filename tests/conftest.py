@@ -28,10 +28,12 @@ def pytest_configure(config):
 @pytest.fixture(scope="session")
 def hostsim():
     """The device code's arithmetic compiled for the host (test-only)."""
-    deps = [HOSTSIM_SRC] + list((ROOT / "gpjson_b200" / "csrc").glob("*.cuh"))
+    csrc = ROOT / "gpjson_b200" / "csrc"
+    deps = [HOSTSIM_SRC, csrc / "host_io.h"] + list(csrc.glob("*.cuh"))
     if not HOSTSIM_LIB.exists() or any(d.stat().st_mtime > HOSTSIM_LIB.stat().st_mtime for d in deps):
         subprocess.run(
-            ["g++", "-std=c++17", "-O2", "-shared", "-fPIC", "-o", str(HOSTSIM_LIB), str(HOSTSIM_SRC)], check=True
+            ["g++", "-std=c++17", "-O2", "-shared", "-fPIC", "-pthread", "-o", str(HOSTSIM_LIB), str(HOSTSIM_SRC)],
+            check=True,
         )
     L = ctypes.CDLL(str(HOSTSIM_LIB))
     P = ctypes.c_void_p
@@ -48,6 +50,18 @@ def hostsim():
     L.hs_classify.argtypes = [P, ctypes.c_int64, P]
     L.hs_escaped_mask.restype = ctypes.c_uint64
     L.hs_escaped_mask.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+    L.hs_read_ranges.restype = ctypes.c_int
+    L.hs_read_ranges.argtypes = [ctypes.c_char_p, P, P, P, ctypes.c_int, ctypes.c_int]
+    L.hs_rb_new.restype = P
+    L.hs_rb_new.argtypes = []
+    L.hs_rb_delete.restype = None
+    L.hs_rb_delete.argtypes = [P]
+    L.hs_rb_take.restype = P
+    L.hs_rb_take.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
+    L.hs_rb_give.restype = None
+    L.hs_rb_give.argtypes = [P, P, ctypes.c_uint64]
+    L.hs_rb_keep_elems.restype = ctypes.c_uint64
+    L.hs_rb_keep_elems.argtypes = []
     return L
 
 

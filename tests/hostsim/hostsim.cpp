@@ -1,13 +1,15 @@
 // Test-only CPU harness: runs the device code's per-word arithmetic
 // (gpjson_b200/csrc/word_ops.cuh) and line interpreter (interp.cuh) on the
 // host, in the same tile/word decomposition the index kernel uses, so the
-// test suite can compare them with the oracle without a GPU.  It is built
-// by tests/conftest.py and never used by the library.
+// test suite can compare them with the oracle without a GPU; and the C
+// ABI's host I/O (host_io.h).  It is built by tests/conftest.py and never
+// used by the library.
 #include <cstdint>
 #include <algorithm>
 #include <cstring>
 #include <vector>
 
+#include "../../gpjson_b200/csrc/host_io.h"
 #include "../../gpjson_b200/csrc/interp.cuh"
 #include "../../gpjson_b200/csrc/query_items.cuh"
 #include "../../gpjson_b200/csrc/word_ops.cuh"
@@ -246,5 +248,35 @@ int64_t hs_query_items(int64_t item_begin, int64_t num_lines, int num_queries, i
     }
     return count;
 }
+
+// Reads ranges [pos[i], pos[i] + len[i]) of `path` back to back into dst
+// through one gpj::SliceReader of `threads` threads; returns how many
+// ranges were read before the first failure (-1: the file does not open).
+int hs_read_ranges(const char* path, uint8_t* dst, const int64_t* pos, const int64_t* len, int ranges, int threads) {
+    const int fd = ::open(path, O_RDONLY);
+    if (fd < 0) return -1;
+    int done = 0;
+    {
+        gpj::SliceReader reader(fd, threads);
+        for (; done < ranges; done++) {
+            if (!reader.read(dst, pos[done], static_cast<size_t>(len[done]))) break;
+            dst += len[done];
+        }
+    }
+    ::close(fd);
+    return done;
+}
+
+// gpj::ResultBuffers, one instance per test.
+void* hs_rb_new() { return new gpj::ResultBuffers; }
+void hs_rb_delete(void* b) { delete static_cast<gpj::ResultBuffers*>(b); }
+int64_t* hs_rb_take(void* b, uint64_t count, uint64_t* cap) {
+    size_t c = 0;
+    int64_t* p = static_cast<gpj::ResultBuffers*>(b)->take(count, &c);
+    *cap = c;
+    return p;
+}
+void hs_rb_give(void* b, int64_t* p, uint64_t cap) { static_cast<gpj::ResultBuffers*>(b)->give(p, cap); }
+uint64_t hs_rb_keep_elems() { return gpj::ResultBuffers::kKeepElems; }
 
 }  // extern "C"

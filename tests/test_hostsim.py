@@ -268,3 +268,66 @@ def test_index_union_slots_equal_single_indices(hostsim):
                 sidx = oracle.Index(data, depth)
                 want = oracle.find_value(data, sidx.newlines, sidx.strings, sidx.levels, depth, ir, slots)
                 assert np.array_equal(got[0, :, b], want[:, 0]), (union, single, data[:80])
+
+
+@pytest.mark.parametrize("threads", [1, 3, 16])
+def test_slice_reader_reads_ranges(hostsim, tmp_path, threads):
+    """gpj::SliceReader (gpj_file_open's reader): ranges of every size,
+    including ragged ones shorter than a slice per thread, read back to back
+    through one reader equal the file's bytes; a range past the end of the
+    file fails (the file shrank) and reading stops there."""
+    rng = np.random.default_rng(5)
+    data = rng.integers(0, 256, size=(5 << 20) + 4321, dtype=np.uint8)
+    path = tmp_path / "f.bin"
+    data.tofile(path)
+    spans = [(0, 1), (7, 3 << 20), (0, data.size), (data.size - 17, 17), ((1 << 20) + 5, 999), (123, 0)]
+    pos = np.array([p for p, _ in spans], dtype=np.int64)
+    ln = np.array([n for _, n in spans], dtype=np.int64)
+    out = np.zeros(int(ln.sum()), dtype=np.uint8)
+    got = hostsim.hs_read_ranges(str(path).encode(), out.ctypes.data, pos.ctypes.data, ln.ctypes.data, len(spans),
+                                 threads)
+    assert got == len(spans)
+    want = np.concatenate([data[p:p + n] for p, n in spans])
+    assert np.array_equal(out, want)
+    # a short read ends the sequence at that range
+    pos2 = np.array([0, data.size - 10, 0], dtype=np.int64)
+    ln2 = np.array([100, 20, 100], dtype=np.int64)
+    out2 = np.zeros(220, dtype=np.uint8)
+    assert hostsim.hs_read_ranges(str(path).encode(), out2.ctypes.data, pos2.ctypes.data, ln2.ctypes.data, 3,
+                                  threads) == 1
+    assert hostsim.hs_read_ranges(str(tmp_path / "missing").encode(), out2.ctypes.data, pos2.ctypes.data,
+                                  ln2.ctypes.data, 1, threads) == -1
+
+
+def test_result_buffers_keep_the_largest(hostsim):
+    """gpj::ResultBuffers (host memory of gpj_result): a released buffer is
+    handed to the next result that fits in it, the larger of two released
+    buffers is the one kept (up to 512 MiB), and a new buffer starts zeroed
+    (touched before the copy into it)."""
+    import ctypes
+
+    b = hostsim.hs_rb_new()
+    try:
+        cap = ctypes.c_uint64()
+        p1 = hostsim.hs_rb_take(b, 1000, ctypes.byref(cap))
+        assert p1 and cap.value == 1000
+        assert np.ctypeslib.as_array((ctypes.c_int64 * 1000).from_address(p1)).sum() == 0
+        hostsim.hs_rb_give(b, p1, cap.value)
+        p2 = hostsim.hs_rb_take(b, 600, ctypes.byref(cap))
+        assert p2 == p1 and cap.value == 1000  # reused, with its full capacity
+        p3 = hostsim.hs_rb_take(b, 2000, ctypes.byref(cap))
+        assert p3 != p1 and cap.value == 2000  # nothing kept: a new buffer
+        hostsim.hs_rb_give(b, p2, 1000)
+        hostsim.hs_rb_give(b, p3, 2000)  # the larger one is kept
+        p4 = hostsim.hs_rb_take(b, 1500, ctypes.byref(cap))
+        assert p4 == p3 and cap.value == 2000
+        p5 = hostsim.hs_rb_take(b, 3000, ctypes.byref(cap))  # larger than the kept one
+        assert p5 != p4 and cap.value == 3000
+        hostsim.hs_rb_give(b, p5, cap.value)
+        hostsim.hs_rb_give(b, p4, 2000)  # smaller than the kept one: freed
+        p6 = hostsim.hs_rb_take(b, 2500, ctypes.byref(cap))
+        assert p6 == p5 and cap.value == 3000
+        hostsim.hs_rb_give(b, p6, cap.value)
+        assert hostsim.hs_rb_keep_elems() == 64 << 20  # 512 MiB at most are kept
+    finally:
+        hostsim.hs_rb_delete(b)
