@@ -174,3 +174,20 @@ def test_result_array_is_a_view_that_owns_the_result():
     del q0
     gc.collect()
     assert released == [0x1234]
+
+
+@pytest.mark.parametrize("lang,std", [("c", "c99"), ("c++", "c++17")])
+def test_header_compiles_standalone(lang, std):
+    """include/gpjson_b200.h is a plain C header: a C99 or C++17 caller
+    includes it alone, without warnings."""
+    cc = "gcc" if lang == "c" else "g++"
+    subprocess.run([cc, f"-std={std}", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only", "-x", lang,
+                    str(ROOT / "include" / "gpjson_b200.h")], check=True)
+
+
+def test_host_io_header_compiles_cleanly():
+    """The C ABI's host I/O header (parallel file reader, result buffers)
+    builds without warnings on its own."""
+    header = ROOT / "gpjson_b200" / "csrc" / "host_io.h"
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-x", "c++", "-"],
+                   input=f'#include "{header}"\n'.encode(), check=True)
