@@ -438,7 +438,8 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
             "queries": QUERIES,
             "bytes_per_gpu": n,
             "lines_per_gpu": lines,
-            "l2": "input larger than L2 (2 GiB vs 126 MB)",
+            "l2": (f"input larger than L2 ({n / 2**20:.0f} MiB vs 126 MB)" if n > 126_000_000
+                   else f"input within L2 ({n / 2**20:.0f} MiB vs 126 MB): not a valid bench size"),
             "parallelism": f"replicas x{world} (one file per GPU)",
         },
         "pass_ms": round(pass_ms, 4),
