@@ -406,18 +406,16 @@ class File:
         v = c_void_p()
         self._native.check(self._native.lib.gpj_query_values(self._native.h, self._h, len(paths), arr, byref(v)))
         lib = self._native.lib
-        try:
-            nq, lines, slots = lib.gpj_values_num_queries(v), lib.gpj_values_num_lines(v), lib.gpj_values_slots(v)
-            items = nq * lines * slots
-            kinds = np.zeros(items, dtype=np.uint8)
-            if items:
-                kinds[:] = np.ctypeslib.as_array((ctypes.c_uint8 * items).from_address(lib.gpj_values_kinds(v)))
-            offsets = np.ctypeslib.as_array((ctypes.c_int64 * (items + 1)).from_address(lib.gpj_values_offsets(v)))
-            size = lib.gpj_values_size(v)
-            data = ctypes.string_at(lib.gpj_values_bytes(v), size) if size else b""
-            return Values(kinds.reshape(nq, lines, slots), offsets.copy(), data, list(paths))
-        finally:
-            lib.gpj_values_release(v)
+        # kinds and offsets stay in the native object (numpy views own it);
+        # the value bytes are copied once, into the bytes object Values holds
+        owner = _NativeOwner(lib.gpj_values_release, v)
+        nq, lines, slots = lib.gpj_values_num_queries(v), lib.gpj_values_num_lines(v), lib.gpj_values_slots(v)
+        items = nq * lines * slots
+        kinds = _native_view(owner, lib.gpj_values_kinds(v), items, "|u1")
+        offsets = _native_view(owner, lib.gpj_values_offsets(v), items + 1, "<i8")
+        size = lib.gpj_values_size(v)
+        data = ctypes.string_at(lib.gpj_values_bytes(v), size) if size else b""
+        return Values(kinds.reshape(nq, lines, slots), offsets, data, list(paths))
 
     def index_and_query_device(self, queries: list[CompiledQuery], num_levels: int, d_out: int, out_lines: int,
                                slots: int | None = None) -> None:
@@ -443,33 +441,41 @@ class File:
             pass
 
 
-class _ResultBuffer:
-    """Owns a gpj_result and exposes its offsets to numpy without a copy;
-    arrays made from it keep it (and so the native result) alive."""
+class _NativeOwner:
+    """Owns a native object (gpj_result, gpj_values) and releases it when
+    the last numpy view of its memory is collected."""
 
-    def __init__(self, lib, r, count: int):
-        self._lib, self._r = lib, r
-        self.__array_interface__ = {
-            "shape": (count,), "typestr": "<i8", "data": (lib.gpj_result_offsets(r), False), "version": 3,
-        }
+    def __init__(self, release, handle):
+        self._release, self._h = release, handle
 
     def __del__(self):
-        if self._r:
-            self._lib.gpj_result_release(self._r)
-            self._r = None
+        if self._h:
+            self._release(self._h)
+            self._h = None
+
+
+class _NativeView:
+    """`count` elements of numpy type `typestr` at `addr`, memory owned by
+    `owner`; np.asarray of it is a view that keeps the owner alive."""
+
+    def __init__(self, owner: _NativeOwner, addr: int, count: int, typestr: str):
+        self._owner = owner
+        self.__array_interface__ = {"shape": (count,), "typestr": typestr, "data": (addr, False), "version": 3}
+
+
+def _native_view(owner: _NativeOwner, addr, count: int, typestr: str) -> np.ndarray:
+    if count == 0:
+        return np.zeros(0, dtype=np.dtype(typestr))
+    return np.asarray(_NativeView(owner, addr, count, typestr))
 
 
 def _result_array(lib, r) -> np.ndarray:
     """int64 [nq][lines][slots][2] over a gpj_result's offsets (no copy: the
     array owns the result and releases it when it is collected)."""
-    try:
-        nq, lines, slots = lib.gpj_result_num_queries(r), lib.gpj_result_num_lines(r), lib.gpj_result_slots(r)
-        count = nq * lines * slots * 2
-        holder = _ResultBuffer(lib, r, count)
-    except BaseException:
-        lib.gpj_result_release(r)
-        raise
-    return np.asarray(holder).reshape(nq, lines, slots, 2)
+    owner = _NativeOwner(lib.gpj_result_release, r)
+    nq, lines, slots = lib.gpj_result_num_queries(r), lib.gpj_result_num_lines(r), lib.gpj_result_slots(r)
+    count = nq * lines * slots * 2
+    return _native_view(owner, lib.gpj_result_offsets(r), count, "<i8").reshape(nq, lines, slots, 2)
 
 
 class Batch:

@@ -191,3 +191,75 @@ def test_host_io_header_compiles_cleanly():
     header = ROOT / "gpjson_b200" / "csrc" / "host_io.h"
     subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-x", "c++", "-"],
                    input=f'#include "{header}"\n'.encode(), check=True)
+
+
+def test_values_arrays_are_views_that_own_the_native_values():
+    """File.query_values hands the native kinds and offsets to numpy in
+    place (the value bytes are copied once into bytes); the gpj_values is
+    released once, when the Values and every array taken from it are gone."""
+    import ctypes
+    import gc
+
+    import numpy as np
+
+    kinds = (ctypes.c_uint8 * 6)(gj.VALUE_PRESENT, gj.VALUE_NULL, gj.VALUE_PRESENT, gj.VALUE_UNREADABLE,
+                                 gj.VALUE_PRESENT, gj.VALUE_NULL)
+    offs = (ctypes.c_int64 * 7)(0, 3, 3, 5, 5, 10, 10)
+    data = ctypes.create_string_buffer(b'"x"12"abc"', 10)
+    released = []
+
+    class FakeLib:  # the gpj_query_values / gpj_values_* entry points
+        def gpj_query_values(self, ctx, file, nq, paths, out):
+            out._obj.value = 0x77
+            return 0
+
+        def gpj_values_num_queries(self, v):
+            return 2
+
+        def gpj_values_num_lines(self, v):
+            return 3
+
+        def gpj_values_slots(self, v):
+            return 1
+
+        def gpj_values_kinds(self, v):
+            return ctypes.addressof(kinds)
+
+        def gpj_values_offsets(self, v):
+            return ctypes.addressof(offs)
+
+        def gpj_values_size(self, v):
+            return 10
+
+        def gpj_values_bytes(self, v):
+            return ctypes.addressof(data)
+
+        def gpj_values_release(self, v):
+            released.append(v.value)
+
+    class FakeNative:
+        lib, h = FakeLib(), None
+
+        def check(self, rc):
+            assert rc == 0
+
+    f = gj.File(FakeNative(), ctypes.c_void_p(1))
+    try:
+        vals = f.query_values(["$.a", "$.b"])
+    finally:
+        f._h = None  # no native file behind the fake
+    assert vals.kinds.shape == (2, 3, 1) and vals.data == b'"x"12"abc"'
+    assert [vals[0][i][0] for i in range(3)] == ['"x"', None, "12"]
+    with pytest.raises(gj.GPJSONException):
+        vals[1][0][0]
+    assert vals[1][1][0] == '"abc"' and vals[1][2][0] is None
+    offs[2] = 2  # the offsets are the native object's memory
+    assert vals.offsets[2] == 2
+    kept = vals.kinds
+    del vals
+    gc.collect()
+    assert released == []
+    assert np.array_equal(kept.reshape(-1), list(kinds))
+    del kept
+    gc.collect()
+    assert released == [0x77]
