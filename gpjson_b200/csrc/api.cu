@@ -1198,37 +1198,43 @@ int gpj_file_open(gpj_ctx* ctx, const char* filename, gpj_file** out) {
         std::min<int64_t>(16, std::max(1u, std::thread::hardware_concurrency())), std::max<int64_t>(1, n >> 21)));
     const double t0 = now_ms();
     cudaEventRecord(ctx->ev0, ctx->stream);
+    // done[h]: the copy out of staging half h has finished (a half is
+    // refilled only after that)
     cudaEvent_t done[2] = {nullptr, nullptr};
-    cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
-    rc = GPJ_OK;
-    {
+    cudaError_t ce = cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
+    rc = ce == cudaSuccess ? GPJ_OK : cuda_fail(ctx, ce, "cudaEventCreate(file chunks)");
+    if (!rc) {
         gpj::SliceReader reader(fd, threads);
         int64_t pos = 0;
         int half = 0;
         while (pos < n) {
             const size_t want = static_cast<size_t>(std::min<int64_t>(static_cast<int64_t>(chunk), n - pos));
             uint8_t* stage = ctx->h_stage + half * chunk;
-            cudaEventSynchronize(done[half]);  // the copy that last used this half is done
+            cudaError_t e = cudaEventSynchronize(done[half]);
+            if (e != cudaSuccess) {
+                rc = cuda_fail(ctx, e, "cudaEventSynchronize(file chunk)");
+                break;
+            }
             if (!reader.read(stage, pos, want)) {
                 rc = fail(ctx, GPJ_EIO, std::string("Size of file has changed while reading ") + filename);
                 break;
             }
-            cudaError_t e = cudaMemcpyAsync(f->d_owned + pos, stage, want, cudaMemcpyHostToDevice, ctx->stream);
+            e = cudaMemcpyAsync(f->d_owned + pos, stage, want, cudaMemcpyHostToDevice, ctx->stream);
+            if (e == cudaSuccess) e = cudaEventRecord(done[half], ctx->stream);
             if (e != cudaSuccess) {
                 rc = cuda_fail(ctx, e, "cudaMemcpyAsync(file)");
                 break;
             }
-            cudaEventRecord(done[half], ctx->stream);
             pos += static_cast<int64_t>(want);
             half ^= 1;
         }
     }
     ::close(fd);
     if (rc == GPJ_OK) rc = end_phase(ctx, "read_file", t0);
-    else cudaStreamSynchronize(ctx->stream);
-    cudaEventDestroy(done[0]);
-    cudaEventDestroy(done[1]);
+    else cudaStreamSynchronize(ctx->stream);  // no copy still reads the staging
+    if (done[0]) cudaEventDestroy(done[0]);
+    if (done[1]) cudaEventDestroy(done[1]);
     if (rc) {
         gpj_file_release(f);
         return rc;
