@@ -7,6 +7,7 @@ baseline legs of bench.py; never by the gpjson_b200 package.
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 from ctypes import c_int, c_int64, c_void_p
 from pathlib import Path
@@ -27,20 +28,31 @@ def build(force: bool = False) -> Path:
     return LIB_PATH
 
 
-# Where the reference's CUDA kernels are read from to build oracle/_ref
-# (ref_gpu_driver.cu); absent on hosts that only run the prebuilt library.
-REF_KERNELS = Path("/root/reference/gpjson/src/main/resources/com/koenv/gpjson/kernels")
+# The reference checkout whose CUDA kernels oracle/_ref is built from
+# (ref_gpu_driver.cu) is named by the GPJSON_REFERENCE environment variable;
+# hosts without it use the prebuilt library that travels with the tree.
+REF_KERNELS_REL = Path("gpjson/src/main/resources/com/koenv/gpjson/kernels")
 
 
-def build_reference_kernels(force: bool = False) -> Path | None:
+def reference_kernels_dir(reference: str | os.PathLike | None = None) -> Path | None:
+    root = reference if reference is not None else os.environ.get("GPJSON_REFERENCE")
+    if not root:
+        return None
+    d = Path(root) / REF_KERNELS_REL
+    return d if d.is_dir() else None
+
+
+def build_reference_kernels(force: bool = False, reference: str | os.PathLike | None = None) -> Path | None:
     """Builds oracle/_ref/libref_gpu.so from the reference's kernel sources
-    when they are present; returns its path, or None without them."""
+    (`reference`, else $GPJSON_REFERENCE, is the reference checkout) when
+    they are present; returns its path, or None without them."""
     target = HERE / "_ref" / "libref_gpu.so"
-    if not REF_KERNELS.is_dir():
+    kernels = reference_kernels_dir(reference)
+    if kernels is None:
         return target if target.exists() else None
-    deps = [HERE / "ref_gpu_driver.cu"] + sorted(REF_KERNELS.glob("*.cu"))
+    deps = [HERE / "ref_gpu_driver.cu"] + sorted(kernels.glob("*.cu"))
     if force or not target.exists() or any(d.stat().st_mtime > target.stat().st_mtime for d in deps):
-        subprocess.run(["make", "-s", "-C", str(HERE), f"REF_KERNELS={REF_KERNELS}", "_ref/libref_gpu.so"], check=True)
+        subprocess.run(["make", "-s", "-C", str(HERE), f"REF_KERNELS={kernels}", "_ref/libref_gpu.so"], check=True)
     return target
 
 

@@ -2,7 +2,7 @@
 
 Run in a container where the reference tree is mounted:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 It copies the reference's test fixtures (gpjson/src/test/resources/, BSD-3
 licensed, Copyright (c) 2021 Koen Vlaswinkel) into tests/golden/fixtures/ so
@@ -77,4 +77,6 @@ def main(reference_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference checkout>")
+    main(sys.argv[1])

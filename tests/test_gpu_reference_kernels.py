@@ -38,6 +38,44 @@ def test_equal_to_reference_kernels(gpjson, size):
     assert (got[:, :, 0, 0] >= 0).sum() > 0
 
 
+def _compare_with_reference_kernels(gpjson, data: np.ndarray, paths: list[str]) -> np.ndarray:
+    compiled = [gj.compile_path(p) for p in paths]
+    levels = max(c.max_depth for c in compiled)
+    slots = max(c.num_results for c in compiled)
+    ref = ref_gpu.run(data, levels, [c.bytecode for c in compiled], slots, max_lines=data.size // 64 + 16)
+    f = gpjson.load_bytes(data)
+    try:
+        f.build_index(levels)
+        assert np.array_equal(f.newline_index(), ref["newlines"])
+        assert np.array_equal(f.string_index(), ref["strings"])
+        assert np.array_equal(f.leveled_bitmaps(levels), ref["levels"])
+        got = f.run(compiled, slots)
+    finally:
+        f.release()
+    assert np.array_equal(got, ref["results"])
+    return got
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not ref_gpu.available(), reason="oracle/_ref/libref_gpu.so not built (needs the reference sources)")
+def test_plain_small_configuration_equal_to_reference_kernels(gpjson):
+    """64 MiB of tweet-like NDJSON from the generator's first seed, $.user.lang."""
+    data = datagen.tweets(64 << 20, seed=datagen.SEED_BASE + 0, p_empty_hashtags=0.3)
+    got = _compare_with_reference_kernels(gpjson, data, ["$.user.lang"])
+    assert (got[0, :, 0, 0] >= 0).mean() > 0.99
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not ref_gpu.available(), reason="oracle/_ref/libref_gpu.so not built (needs the reference sources)")
+def test_adversarial_sample_equal_to_reference_kernels(gpjson):
+    """256 MiB of the adversarial generator (lines to 1 MiB, nesting to 16,
+    backslash runs; well-formed, and index steps only meet arrays, so the
+    reference kernels stay inside their buffers) with its three queries."""
+    data = datagen.adversarial(256 << 20, seed=datagen.SEED_BASE + 2)
+    got = _compare_with_reference_kernels(gpjson, data, ["$.a.b.c.d", "$.arr[5]", "$.x[0].y[2].z"])
+    assert ((got[:, :, 0, 0] >= 0).sum(axis=1) > 0).all()
+
+
 @pytest.mark.gpu
 @pytest.mark.skipif(not ref_gpu.available(), reason="oracle/_ref/libref_gpu.so not built (needs the reference sources)")
 def test_faster_than_reference_kernels(gpjson, capsys):
