@@ -65,7 +65,7 @@ struct gpj_ctx {
     int64_t exact_fallbacks = 0;         // builds that needed the exact kernel
     bool fuse_queries = false;           // evaluate queries inside the index kernel
     unsigned path_extensions = 0;        // GPJ_PATH_* flags for calls that compile paths
-    int query_occupancy = 0;
+    int query_occupancy[3] = {0, 0, 0};  // find_value CTAs per SM, by register-state size (depth <= 4, <= 8, more)
 
     // pinned staging for file reads
     uint8_t* h_stage = nullptr;
@@ -96,6 +96,7 @@ struct gpj_file {
 
     // uploaded bytecode (cached across calls with identical queries)
     std::vector<uint8_t> ir_host;
+    int ir_depth = 0;  // deepest level of the uploaded queries
     uint8_t* d_ir = nullptr;
     size_t d_ir_cap = 0;
     // results of gpj_query with a host destination
@@ -461,6 +462,7 @@ int upload_queries(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, 
         packed.insert(packed.end(), bc[q], bc[q] + len[q]);
     }
     *depth_needed = deepest;
+    f->ir_depth = deepest;
     if (packed == f->ir_host && f->d_ir) return GPJ_OK;
     if (packed.size() > f->d_ir_cap) {
         device_free(ctx, f->d_ir);
@@ -473,6 +475,11 @@ int upload_queries(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, 
     GPJ_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     f->ir_host.swap(packed);
     return GPJ_OK;
+}
+
+// find_value CTAs per SM for queries no deeper than `depth`.
+int query_occupancy(const gpj_ctx* ctx, int depth) {
+    return ctx->query_occupancy[depth <= 4 ? 0 : (depth <= 8 ? 1 : 2)];
 }
 
 // find_value over the file's lines, or (d_range given) over lines
@@ -499,8 +506,10 @@ int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, i
     p.last = last ? 1 : 0;
     p.newline_cap = f->nl_cap;
     p.colon = f->colon_valid ? f->d_colon : nullptr;
+    p.depth = f->ir_depth;
     const int64_t want = d_range ? INT64_MAX : (gpj::query_items(f->num_lines, nq) + 255) / 256;
-    const int64_t grid = std::max<int64_t>(1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * ctx->query_occupancy));
+    const int64_t grid = std::max<int64_t>(
+        1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * query_occupancy(ctx, f->ir_depth)));
     GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->stream));
     ctx->launches++;
     return GPJ_OK;
@@ -915,8 +924,10 @@ int gpj_create(int device, gpj_ctx** out) {
         if (ctx->tile_occupancy[i] < 1) return bail(cudaGetLastError(), "tile index kernel occupancy");
         if (ctx->line_occupancy[i] < 1) return bail(cudaGetLastError(), "line index kernel occupancy");
     }
-    ctx->query_occupancy = gpj::find_value_max_ctas_per_sm();
-    if (ctx->query_occupancy < 1) return bail(cudaGetLastError(), "find_value occupancy");
+    for (int v = 0; v < 3; v++) {
+        ctx->query_occupancy[v] = gpj::find_value_max_ctas_per_sm(v == 0 ? 4 : (v == 1 ? 8 : GPJ_MAX_LEVELS));
+        if (ctx->query_occupancy[v] < 1) return bail(cudaGetLastError(), "find_value occupancy");
+    }
     *out = ctx;
     return GPJ_OK;
 }
@@ -1836,10 +1847,12 @@ int gpj_batch_run(gpj_batch* b) {
             e = cudaMemcpyAsync(d_qf, qf.data(), sizeof(gpj::QueryFile) * qf.size(), cudaMemcpyHostToDevice,
                                 ctx->stream);
         if (e == cudaSuccess && total_items > 0) {
+            int depth = 0;
+            for (auto& fr : b->files) depth = std::max(depth, fr.depth);
             const int64_t grid =
                 std::max<int64_t>(1, std::min<int64_t>((total_items + 255) / 256, static_cast<int64_t>(ctx->sms) * 8));
-            e = gpj::launch_find_value_batch(d_qf, static_cast<int>(qf.size()), total_items, static_cast<int>(grid),
-                                             ctx->stream);
+            e = gpj::launch_find_value_batch(d_qf, static_cast<int>(qf.size()), total_items, depth,
+                                             static_cast<int>(grid), ctx->stream);
             ctx->launches++;
         }
         if (e == cudaSuccess && total_out > b->results_cap) {

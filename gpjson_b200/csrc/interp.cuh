@@ -14,6 +14,7 @@
 // CPU against the oracle.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 #include "word_ops.cuh"
@@ -43,6 +44,36 @@ struct LineView {
 enum LineStatus : int { kLineDone = 0, kLineDeferred = 1 };
 
 GPJ_HD bool is_ws(uint8_t c) { return c == '\n' || c == '\r' || c == '\t' || c == ' '; }
+
+// Every byte of x is one of the four whitespace bytes.
+GPJ_HD bool all_ws32(uint32_t x) {
+    return (eq_bytes(x, 0x20202020u) | eq_bytes(x, 0x0A0A0A0Au) | eq_bytes(x, 0x0D0D0D0Du) |
+            eq_bytes(x, 0x09090909u)) == 0x80808080u;
+}
+
+// First position at or after j that is >= hi or not whitespace.  Short runs
+// go byte by byte; a run longer than 32 bytes continues 32 aligned bytes per
+// step (independent loads), so a skip over a long run of blanks does not
+// wait for one memory round trip per byte.
+template <typename P>
+GPJ_HD P skip_ws(const uint8_t* file, P j, P hi) {
+    for (int k = 0; k < 32; k++, ++j)
+        if (j >= hi || !is_ws(file[j])) return j;
+    for (; j < hi && (reinterpret_cast<uintptr_t>(file + j) & 7) != 0; ++j)
+        if (!is_ws(file[j])) return j;
+    for (; j + 32 <= hi; j += 32) {
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(file + j);
+        uint32_t x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = w[i];
+        bool all = true;
+#pragma unroll
+        for (int i = 0; i < 8; i++) all = all && all_ws32(x[i]);
+        if (!all) break;
+    }
+    while (j < hi && is_ws(file[j])) ++j;
+    return j;
+}
 
 // The bit helpers and the interpreter below are templates on the position
 // type P: int64_t for positions in the file, int32_t for positions relative
@@ -212,6 +243,47 @@ struct LocalLevelsT {
 };
 using LocalLevels = LocalLevelsT<int64_t>;
 
+// In registers, for queries that go at most D - 1 levels down (a validated
+// query's level is in [0, D) at every step): the arrays are only ever
+// indexed by unrolled loops with constant indices, so they stay in
+// registers; an access costs D selects instead of a local-memory round trip.
+template <int D, typename P>
+struct RegLevelsT {
+    P ends[D];
+    P index[D];
+    GPJ_HD void reset(P line_end) {
+        ends[0] = line_end;
+#pragma unroll
+        for (int k = 1; k < D; k++) ends[k] = -1;
+#pragma unroll
+        for (int k = 0; k < D; k++) index[k] = -1;
+    }
+    GPJ_HD P end(int k) const {
+        P v = -1;
+#pragma unroll
+        for (int i = 0; i < D; i++) v = i == k ? ends[i] : v;
+        return v;
+    }
+    GPJ_HD void set_end(int k, P v) {
+#pragma unroll
+        for (int i = 0; i < D; i++) ends[i] = i == k ? v : ends[i];
+    }
+    GPJ_HD P idx(int k) const {
+        P v = -1;
+#pragma unroll
+        for (int i = 0; i < D; i++) v = i == k ? index[i] : v;
+        return v;
+    }
+    GPJ_HD void set_idx(int k, P v) {
+#pragma unroll
+        for (int i = 0; i < D; i++) index[i] = i == k ? v : index[i];
+    }
+};
+
+// Level slots a query needs: one more than its deepest level, rounded up to
+// the register-state sizes the kernels are built for.
+GPJ_HD int level_slots_for_depth(int depth) { return depth <= 4 ? 5 : (depth <= 8 ? 9 : kLevelSlots); }
+
 // In caller-provided storage (e.g. shared memory, entries `stride` apart),
 // as 32-bit offsets from the line start: for lines shorter than 2 GiB and
 // queries no deeper than `slots - 1` levels.
@@ -246,10 +318,11 @@ struct PackedLevels {
 template <typename P, typename Levels>
 GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uint64_t* string_index,
                          const uint64_t* levels, int64_t level_size, const uint64_t* colon, P line_start,
-                         P line_end, const uint8_t* ir, int64_t* res, int64_t base, Levels& lv) {
+                         P line_end, const uint8_t* ir, int64_t* res, int64_t base, Levels& lv, int& stored) {
     lv.reset(line_end);
 
     int pc = 0, cur = 0, result_index = 0;
+    stored = 0;
     uint8_t type = 0xFF;
     P want_len = 0;
     int64_t want_index = -1;
@@ -263,6 +336,7 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
     P cw = -1;
     uint64_t cv = 0;
     P cend = lv.end(cur);  // lv.end(cur), kept while searching (only opcodes change it)
+    P cidx = -1;           // lv.idx(cur) during an index search, written back at its match
     while (j < cend && j < n) {
         const bool ran = execute;
         while (execute) {
@@ -271,12 +345,12 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
                 case 0:  // END
                     return kLineDone;
                 case 1: {  // STORE_RESULT (find_value.cu:59-82)
-                    while (j < hi && is_ws(file[j])) ++j;  // [bounded] stops at end of file
+                    j = skip_ws<P>(file, j, hi);  // [bounded] stops at end of file
                     if (j >= hi && skip_end) return kLineDeferred;
                     const P e = lv.end(cur);
                     res[2 * result_index] = base + j;
                     res[2 * result_index + 1] = e < 0 ? -1 : base + e;
-                    ++result_index;
+                    stored = ++result_index;
                     break;
                 }
                 case 2:  // MOVE_UP (:83-90)
@@ -317,13 +391,14 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
                         execute = true;
                     } else {
                         execute = false;
+                        cidx = lv.idx(cur);
                     }
                     break;
                 case 6: {  // EXPRESSION_STRING_EQUALS (:170-210)
                     want_len = static_cast<P>(read_varint(ir, pc));
                     want = ir + pc;
                     pc += static_cast<int>(want_len);
-                    while (j < hi && is_ws(file[j])) ++j;  // [bounded]
+                    j = skip_ws<P>(file, j, hi);  // [bounded]
                     if (j >= hi && skip_end) return kLineDeferred;
                     if (lv.end(cur) - j != want_len) return kLineDone;
                     for (P k = 0; k < want_len; k++)
@@ -366,9 +441,11 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
                 }
             } else if (type == 5) {  // index match at a structural ',' (:252-259)
                 if (structural && at == ',') {
-                    const P count = lv.idx(cur) + 1;
-                    lv.set_idx(cur, count);
-                    if (want_index == count) execute = true;
+                    ++cidx;
+                    if (want_index == cidx) {
+                        lv.set_idx(cur, cidx);
+                        execute = true;
+                    }
                 }
             }
         }
@@ -392,42 +469,100 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
 }
 
 // The interpreter on a view's positions as they are (64-bit), with the
-// per-level state in `lv` (LocalLevels, PackedLevels).
+// per-level state in `lv` (LocalLevels, PackedLevels); res must hold -1 on
+// entry (only the stored results are written).
 template <typename Levels>
 GPJ_HD int run_line_with(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
                          int64_t* res, Levels& lv) {
+    int stored = 0;
     return run_line_core<int64_t>(v.file, v.n, v.hi, v.hi < v.n ? kLineDeferred : kLineDone, v.string_index,
-                                  v.levels, v.level_size, v.colon, line_start, line_end, ir, res, 0, lv);
+                                  v.levels, v.level_size, v.colon, line_start, line_end, ir, res, 0, lv, stored);
 }
 
 // Largest line-relative position the 32-bit interpreter handles.
 constexpr int64_t kRelLimit = (1ll << 31) - 4096;
 
+// The interpreter in 64-bit positions with the level state in local memory,
+// for lines the 32-bit form cannot hold; a separate function, so that its
+// state does not add to the registers of the 32-bit form's caller.  Writes
+// every one of the res_len entries once.
+#ifdef __CUDACC__
+static __host__ __device__ __noinline__
+#else
+static __attribute__((noinline))
+#endif
+int run_line_wide(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir, int64_t* res,
+                  int64_t res_len) {
+    LocalLevels lv;
+    int stored = 0;
+    const int r = run_line_core<int64_t>(v.file, v.n, v.hi, v.hi < v.n ? kLineDeferred : kLineDone, v.string_index,
+                                         v.levels, v.level_size, v.colon, line_start, line_end, ir, res, 0, lv,
+                                         stored);
+    for (int64_t k = 2 * static_cast<int64_t>(stored); k < res_len; k++) res[k] = -1;
+    return r;
+}
+
 // run_line_with with positions relative to the line's first 64-byte word
-// in 32 bits (the usual case: half the integer work per step).  Lines whose
-// end lies more than rel_limit (<= kRelLimit) bytes past that word run in
-// 64 bits; a whitespace skip that reaches rel_limit (bytes past it exist)
-// stops there and the line is evaluated again in 64 bits from -1 results
-// (res_len entries).
+// in 32 bits (the usual case: half the integer work per step) and the
+// per-level state in registers for queries whose level stays below D.
+// Every one of the res_len entries is written once: the stored results,
+// then -1 for the slots the line did not reach (res need not be
+// initialised).  Lines whose end lies more than rel_limit (<= kRelLimit)
+// bytes past that word run in 64 bits; a whitespace skip that reaches
+// rel_limit (bytes past it exist) stops there and the line is evaluated
+// again in 64 bits.
+template <int D = kLevelSlots>
 GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir, int64_t* res,
                     int64_t res_len, int64_t rel_limit = kRelLimit) {
     const int64_t base = line_start & ~static_cast<int64_t>(63);
+    int stored = 0;
     if (line_end - base <= rel_limit) {
         const bool clamped = v.hi - base > rel_limit;
         const int32_t hi = static_cast<int32_t>(clamped ? rel_limit : v.hi - base);
         const int32_t n = static_cast<int32_t>(v.n - base > rel_limit ? rel_limit : v.n - base);
         const int skip_end = clamped || v.hi < v.n ? kLineDeferred : kLineDone;
         const int64_t w = base >> 6;
-        LocalLevelsT<int32_t> lv;
+        RegLevelsT<D, int32_t> lv;
         const int r = run_line_core<int32_t>(v.file + base, n, hi, skip_end, v.string_index + w, v.levels + w,
                                              v.level_size, v.colon ? v.colon + w : nullptr,
                                              static_cast<int32_t>(line_start - base),
-                                             static_cast<int32_t>(line_end - base), ir, res, base, lv);
-        if (r != kLineDeferred || !clamped || v.hi < v.n) return r;
-        for (int64_t k = 0; k < res_len; k++) res[k] = -1;
+                                             static_cast<int32_t>(line_end - base), ir, res, base, lv, stored);
+        if (r != kLineDeferred || !clamped || v.hi < v.n) {
+            for (int64_t k = 2 * static_cast<int64_t>(stored); k < res_len; k++) res[k] = -1;
+            return r;
+        }
     }
-    LocalLevels lv;
-    return run_line_with(v, line_start, line_end, ir, res, lv);
+    return run_line_wide(v, line_start, line_end, ir, res, res_len);
+}
+
+// Deepest level a validated query's bytecode reaches (its MOVE_DOWNs).
+GPJ_HD int bytecode_depth(const uint8_t* ir) {
+    int pc = 0, level = 0, deepest = 0;
+    for (;;) {
+        const uint8_t op = ir[pc++];
+        if (op == 0 || op > 6) return deepest;
+        if (op == 2) --level;
+        if (op == 3 && ++level > deepest) deepest = level;
+        if (op == 4 || op == 6) {
+            const uint32_t len = read_varint(ir, pc);
+            pc += static_cast<int>(len);
+        }
+        if (op == 5) read_varint(ir, pc);
+    }
+}
+
+// run_line with the register state sized for queries no deeper than `depth`
+// (the sizes the kernels are instantiated for).
+GPJ_HD int run_line_depth(int depth, const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
+                          int64_t* res, int64_t res_len, int64_t rel_limit = kRelLimit) {
+    switch (level_slots_for_depth(depth)) {
+        case 5:
+            return run_line<5>(v, line_start, line_end, ir, res, res_len, rel_limit);
+        case 9:
+            return run_line<9>(v, line_start, line_end, ir, res, res_len, rel_limit);
+        default:
+            return run_line<kLevelSlots>(v, line_start, line_end, ir, res, res_len, rel_limit);
+    }
 }
 
 }  // namespace gpj

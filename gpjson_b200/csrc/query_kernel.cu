@@ -22,6 +22,9 @@ namespace gpj {
 
 namespace {
 
+// D: level slots of the interpreter's register state (level_slots_for_depth
+// of the deepest query of the launch).
+template <int D>
 __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size, p.n, p.colon};
@@ -44,11 +47,11 @@ __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
         const int64_t start = p.newlines[i];
         const int64_t end = to_eof ? p.n : p.newlines[i + 1];
         int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + i) * per_line;
-        for (int64_t k = 0; k < per_line; k++) res[k] = -1;
-        run_line(view, start, end, p.bytecode + p.offsets[q], res, per_line);
+        run_line<D>(view, start, end, p.bytecode + p.offsets[q], res, per_line);  // writes every slot once
     }
 }
 
+template <int D>
 __global__ void __launch_bounds__(256) find_value_batch_kernel(const QueryFile* files, int nfiles,
                                                                 int64_t total_items) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
@@ -70,29 +73,55 @@ __global__ void __launch_bounds__(256) find_value_batch_kernel(const QueryFile* 
         const int64_t end = i + 1 < F.num_lines ? F.newlines[i + 1] : F.n;
         const int64_t per_line = 2 * static_cast<int64_t>(F.slots);
         int64_t* res = F.out + (q * F.out_lines + i) * per_line;
-        for (int64_t r = 0; r < per_line; r++) res[r] = -1;
-        run_line(view, start, end, F.bytecode + F.offsets[q], res, per_line);
+        run_line<D>(view, start, end, F.bytecode + F.offsets[q], res, per_line);
     }
 }
 
 }  // namespace
 
-cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_items, int grid,
+cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_items, int depth, int grid,
                                     cudaStream_t stream) {
-    find_value_batch_kernel<<<grid, 256, 0, stream>>>(files, nfiles, total_items);
+    switch (level_slots_for_depth(depth)) {
+        case 5:
+            find_value_batch_kernel<5><<<grid, 256, 0, stream>>>(files, nfiles, total_items);
+            break;
+        case 9:
+            find_value_batch_kernel<9><<<grid, 256, 0, stream>>>(files, nfiles, total_items);
+            break;
+        default:
+            find_value_batch_kernel<kLevelSlots><<<grid, 256, 0, stream>>>(files, nfiles, total_items);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_find_value(const QueryParams& p, int grid, cudaStream_t stream) {
-    find_value_kernel<<<grid, 256, 0, stream>>>(p);
+    switch (level_slots_for_depth(p.depth)) {
+        case 5:
+            find_value_kernel<5><<<grid, 256, 0, stream>>>(p);
+            break;
+        case 9:
+            find_value_kernel<9><<<grid, 256, 0, stream>>>(p);
+            break;
+        default:
+            find_value_kernel<kLevelSlots><<<grid, 256, 0, stream>>>(p);
+    }
     return cudaGetLastError();
 }
 
-int find_value_max_ctas_per_sm() {
+int find_value_max_ctas_per_sm(int depth) {
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel, 256, 0) != cudaSuccess)
-        return -1;
-    return blocks;
+    cudaError_t e;
+    switch (level_slots_for_depth(depth)) {
+        case 5:
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel<5>, 256, 0);
+            break;
+        case 9:
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel<9>, 256, 0);
+            break;
+        default:
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel<kLevelSlots>, 256, 0);
+    }
+    return e == cudaSuccess ? blocks : -1;
 }
 
 }  // namespace gpj

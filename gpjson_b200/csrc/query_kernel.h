@@ -36,10 +36,14 @@ struct QueryParams {
     // between structural colons, index searches between the other
     // structural bytes (the bytes each search ignores).
     const uint64_t* colon;
+    // deepest level of the launch's queries (sizes the interpreter's
+    // register state)
+    int depth;
 };
 
 cudaError_t launch_find_value(const QueryParams& p, int grid, cudaStream_t stream);
-int find_value_max_ctas_per_sm();
+// Resident CTAs per SM of the find_value kernel for queries of that depth.
+int find_value_max_ctas_per_sm(int depth);
 
 // One file of a batched find_value launch: its index, its queries and where
 // their results go ([num_queries][out_lines][slots][2]); its lines are
@@ -65,10 +69,11 @@ struct QueryFile {
 };
 
 // Every (line, query) item of every file of the batch (`files`: device
-// array, ascending item_begin, total_items items in all), one per thread:
+// array, ascending item_begin, total_items items in all; `depth` the deepest
+// level of any of their queries), one per thread:
 // a warp's lanes run one query on 32 lines of one file, and the warps of a
 // block of lines run its queries side by side.
-cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_items, int grid,
+cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_items, int depth, int grid,
                                     cudaStream_t stream);
 
 }  // namespace gpj

@@ -191,7 +191,10 @@ int64_t hs_build_index_lines(const uint8_t* f, int64_t n, int num_levels, uint64
 // is the bitmap of ':' outside strings that the fused kernel's key searches
 // jump along; `packed` = 1 selects the 32-bit level state the fused kernel
 // keeps in shared memory, 2 the line-relative 32-bit interpreter with a
-// 64-byte limit (so that its 64-bit fallbacks run).
+// 64-byte limit (so that its 64-bit fallbacks run), 3 the register state of
+// the deepest size (0 sizes it by the query's depth, as the kernels do).
+// Slots the interpreter does not reach are written -1 by it (run_line) or
+// were -1 before (PackedLevels).
 void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t lines,
                     const uint64_t* str, const uint64_t* lvl, int nq, const uint8_t* const* irs,
                     int slots, int64_t* out, const uint64_t* colon, int packed) {
@@ -204,11 +207,15 @@ void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t line
             const int64_t start = nl[i];
             const int64_t end = i + 1 < lines ? nl[i + 1] : n;
             int64_t* res = out + q * per_query + i * slots * 2;
-            if (packed) {
+            if (packed == 1) {
                 PackedLevels lv{ends, index, 1, kLevelSlots, start};
                 run_line_with(v, start, end, irs[q], res, lv);
+            } else if (packed == 0) {
+                for (int k = 0; k < slots * 2; k++) res[k] = 7;  // written again by run_line
+                run_line_depth(bytecode_depth(irs[q]), v, start, end, irs[q], res, slots * 2);
             } else {
-                run_line(v, start, end, irs[q], res, slots * 2, packed == 2 ? 64 : kRelLimit);
+                for (int k = 0; k < slots * 2; k++) res[k] = 7;
+                run_line<kLevelSlots>(v, start, end, irs[q], res, slots * 2, packed == 2 ? 64 : kRelLimit);
             }
         }
     }

@@ -133,11 +133,14 @@ def test_interpreter_matches_oracle(hostsim):
         b'  {"k\\"ey": 1, "key": [ ], "x":{"y":[[],[1]]}}  ',
         b'{"a":' + b" " * 100 + b'1, "b": [' + b" " * 70 + b'2]}',
         b'{"a": \n' + b" " * 90 + b'1}',  # a value's whitespace runs on into the next line
+        # deep enough for every size of the interpreter's register state
+        b'{"p":{"q":[[{"r":{"s":[0,{"t":{"u":[1,2,{"v":{"w":"deep"}}]}}]}}]]}}',
     ]
     paths = [
         "$.user.lang", "$.user.values[2]", "$.user.values[0:3]", "$.a.a", "$.a[1][0]", "$.a[2].b",
         "$.c.d[0]", "$.c.d[0:2]", "$.user.lang[?(@ == 'nl')]", "$[0]", "$.b.a", "$.a[0].b[2].c",
         "$.key[0]", "$.x.y[1][0]", "$.x.y[0:2]", "$['k\\\"ey']", "$.d", "$.a", "$.b[0]",
+        "$.p.q[0][0].r.s[1].t.u[2].v.w", "$.p.q[0][0].r.s[0:2]", "$.p.q[0][0].r.s[1].t.u[0:3]",
     ]
     for trial in range(40):
         lines = [rng.choice(base) for _ in range(rng.randint(1, 20))]
@@ -154,7 +157,8 @@ def test_interpreter_matches_oracle(hostsim):
             colon = colon_bitmap(f, idx.strings)
             # plain, with the fused kernel's colon jumps, with its packed level
             # state, and with the 32-bit interpreter's 64-bit fallbacks forced
-            for colon_ptr, packed in ((None, 0), (colon.ctypes.data, 0), (colon.ctypes.data, 1), (None, 2)):
+            for colon_ptr, packed in ((None, 0), (colon.ctypes.data, 0), (colon.ctypes.data, 1), (None, 2),
+                                      (colon.ctypes.data, 3)):
                 got = np.empty_like(want)
                 hostsim.hs_find_values(f.ctypes.data, f.size, idx.newlines.ctypes.data, len(idx.newlines),
                                        idx.strings.ctypes.data, idx.levels.ctypes.data, 1, ptrs, slots,
