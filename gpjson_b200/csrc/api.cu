@@ -291,7 +291,7 @@ struct TileScratch {
 };
 
 int alloc_tile_scratch(gpj_ctx* ctx, int64_t n, TileScratch* ts) {
-    const int64_t ntiles = (n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+    const int64_t ntiles = (n + gpj::kStandaloneTileBytes - 1) / gpj::kStandaloneTileBytes;
     int rc = device_alloc(ctx, &ts->bits, static_cast<size_t>((n + 63) / 64), "cudaMalloc(newline bitmap)");
     if (!rc) rc = device_alloc(ctx, &ts->counts, static_cast<size_t>(ntiles), "cudaMalloc(tile counts)");
     if (!rc)
@@ -324,7 +324,7 @@ int launch_tiles(gpj_ctx* ctx, const gpj::IndexParams& p) {
 // The newline index from the tiles' bitmap and counts; on return h_status
 // holds the status words (line count, error bits).
 int finish_tiles(gpj_ctx* ctx, const gpj::IndexParams& p, const TileScratch& ts) {
-    const int64_t ntiles = (p.n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+    const int64_t ntiles = (p.n + gpj::kStandaloneTileBytes - 1) / gpj::kStandaloneTileBytes;
     const int64_t grid = std::min<int64_t>((ntiles + 7) / 8, static_cast<int64_t>(ctx->sms) * 8);
     GPJ_CUDA(ctx, gpj::launch_newline_index(p, ts.offsets, static_cast<int>(grid), ctx->stream));
     ctx->launches += 2;
@@ -390,6 +390,8 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
             if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemsetAsync(status)");
         }
         if (!rc) {
+            fused.ntiles = (n + gpj::kStandaloneTileBytes - 1) / gpj::kStandaloneTileBytes;  // its own tile size
+            fused.tile_end = fused.ntiles;
             fused.newline_bits = ts.bits;
             fused.tile_newlines = ts.counts;
             fused.colon = d_colon;
@@ -577,10 +579,10 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
     return GPJ_OK;
 }
 
-// Bytes copied per step of load_and_index: 4096 line-kernel tiles (56 MiB),
-// a whole number of the newline scan's 1024-tile blocks.
-constexpr int64_t kLoadTiles = 4096;
-constexpr int64_t kLoadChunk = gpj::kLineTileBytes * kLoadTiles;
+// Bytes copied per step of load_and_index: 2048 standalone-kernel tiles
+// (60 MiB), a whole number of the newline scan's 1024-tile blocks.
+constexpr int64_t kLoadTiles = 2048;
+constexpr int64_t kLoadChunk = gpj::kStandaloneTileBytes * kLoadTiles;
 
 // Queries load_and_index evaluates on each chunk's lines as soon as their
 // index is complete (bytecode uploaded; results strided by out_lines).
@@ -628,7 +630,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         gpj::IndexParams p{};
         p.file = f->d_data;
         p.n = n;
-        p.ntiles = (n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+        p.ntiles = (n + gpj::kStandaloneTileBytes - 1) / gpj::kStandaloneTileBytes;
         p.string_index = f->d_str;
         p.leveled = f->d_lvl;
         p.level_size = f->words;
@@ -1633,7 +1635,7 @@ int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
         f->colon_valid = false;
         if (f->n == 0) continue;  // indexed alone below
         batched.push_back(f);
-        total_tiles += (f->n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+        total_tiles += (f->n + gpj::kStandaloneTileBytes - 1) / gpj::kStandaloneTileBytes;
         total_words += f->words;
     }
     const int nb = static_cast<int>(batched.size());
@@ -1657,7 +1659,7 @@ int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
             int64_t tile = 0, word = 0;
             for (int i = 0; i < nb; i++) {
                 gpj_file* f = batched[i];
-                const int64_t ntiles = (f->n + gpj::kLineTileBytes - 1) / gpj::kLineTileBytes;
+                const int64_t ntiles = (f->n + gpj::kStandaloneTileBytes - 1) / gpj::kStandaloneTileBytes;
                 tf.push_back(gpj::TileFile{f->d_data, f->n, f->n, f->d_str, f->d_lvl, f->words, bits + word,
                                            status + 2 * i, tile, f->d_colon});
                 lf.push_back(gpj::LineFile{bits + word, f->words, f->d_nl, f->nl_cap, status + 2 * i, tile, ntiles});

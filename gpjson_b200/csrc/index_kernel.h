@@ -11,6 +11,9 @@ constexpr int64_t kIndexTileBytes = 16384;  // exact kernel
 // The line-parallel kernel owns 14 KiB per tile and reads 2 KiB past it, so
 // that a tile and its look-ahead are one 64-byte word per index thread.
 constexpr int64_t kLineTileBytes = 14336;
+// The standalone index kernel owns 30 KiB per tile and reads 2 KiB past it:
+// four consecutive 64-byte words per thread of a 128-thread CTA.
+constexpr int64_t kStandaloneTileBytes = 30720;
 // The escape state at a tile start is found by scanning back over the bytes
 // before it; a backslash run longer than this crossing a tile start is
 // reported as an error (kErrEscapeRun) instead of being resolved.
@@ -102,7 +105,7 @@ cudaError_t launch_tile_index_kernel(const IndexParams& p, int grid, cudaStream_
 int tile_index_max_ctas_per_sm(int num_levels);
 
 // Newline index from newline_bits and tile_newlines (tiles of
-// kLineTileBytes): offsets of the tile counts within blocks of 1024 tiles
+// kStandaloneTileBytes): offsets of the tile counts within blocks of 1024 tiles
 // and the block sums into `offsets` (newline_offsets_words(ntiles)
 // entries), then every tile's '\n' positions; writes status[0] =
 // newlines + 1 and at most newline_cap entries.  Two launches, one stream.

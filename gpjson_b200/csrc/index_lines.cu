@@ -237,26 +237,8 @@ struct FShared {
     int64_t nl_before;
 };
 
-// Shared memory of the standalone index kernel (no line warps, no queries).
-template <int LV>
-struct TShared {
-    // nothing reads a tile's bytes after its last barrier, so the copy of
-    // tile k+1 can go into the slot of tile k-1: two byte slots (and room for
-    // five CTAs per SM); the file descriptors, read after that barrier, keep three
-    static constexpr int kByteSlots = 2;
-    uint8_t bytes[kByteSlots][kSlotBytes];
-    TileFile desc[kRing];
-    uint64_t lvacc[kTileWarps][LV][32];
-    uint64_t full[kByteSlots];
-    Span span_scratch[kTileWarps];
-    WarpSum rscan[2][kTileWarps];
-    int carry_esc;
-    int64_t first_line;
-    int64_t ext_b;
-    int64_t long_b;
-};
-
-// Exclusive compose-scan / sum-min over the 256 index threads (named barrier).
+// Exclusive compose-scan over the NW * 32 index threads (named barrier).
+template <int NW = kTileWarps>
 __device__ __forceinline__ Span index_scan_span(Span mine, Span* scratch, Span* total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Span incl = mine;
@@ -268,25 +250,29 @@ __device__ __forceinline__ Span index_scan_span(Span mine, Span* scratch, Span* 
     if (lane == 31) scratch[warp] = incl;
     Span excl = shfl_span_up(incl, 1);
     if (lane == 0) excl = span_identity();
-    group_sync(kBarIndex, kIndexThreads);
+    group_sync(kBarIndex, NW * 32);
     Span prefix = span_identity(), all = span_identity();
 #pragma unroll
-    for (int w = 0; w < kTileWarps; w++) {
+    for (int w = 0; w < NW; w++) {
         if (w == warp) prefix = all;
         all = span_compose(all, scratch[w]);
     }
     *total = all;
-    group_sync(kBarIndex, kIndexThreads);  // scratch may be reused after this
+    group_sync(kBarIndex, NW * 32);  // scratch may be reused after this
     return span_compose(prefix, excl);
 }
 
-// The tile scan over the 256 index threads in word order (see WarpSum);
-// one named barrier.  Per word: reset_w (a tile line starts in it), q (its
+// The tile scan over the NW * 32 index threads in word order (see WarpSum;
+// a thread's entry may also stand for several consecutive words); one named
+// barrier.  Per word: reset_w (a tile line starts in it), q (its
 // string state after the reset, else its quote parity), d_abs (reset: level
 // after it), d_out / d_in (no reset: level change entered outside / inside a
 // string), nl (as WarpSum::nl).  `sums` (kTileWarps entries) must not be
 // reused by the next tile (the caller alternates two).  `start_reset`: a
 // line starts at the slot's first byte (the file's first tile).
+// kBias: the largest level change of one entry (64 per word it stands for),
+// so that every biased entry is >= 0 and 32 of them fit in 16 bits.
+template <int NW = kTileWarps, int kBias = 64>
 __device__ __forceinline__ TileScan tile_scan(bool reset_w, int q, int d_abs, int d_out, int d_in, int nl,
                                               bool start_reset, WarpSum* sums) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -303,7 +289,7 @@ __device__ __forceinline__ TileScan tile_scan(bool reset_w, int q, int d_abs, in
         da = s_loc ? d_in : d_out;
         db = before ? da : (s_loc ? d_out : d_in);
     }
-    const uint32_t mine = static_cast<uint32_t>(da + 64) | (static_cast<uint32_t>(db + 64) << 16);
+    const uint32_t mine = static_cast<uint32_t>(da + kBias) | (static_cast<uint32_t>(db + kBias) << 16);
     uint32_t incl = mine;
     int nl_incl = nl;
 #pragma unroll
@@ -316,15 +302,15 @@ __device__ __forceinline__ TileScan tile_scan(bool reset_w, int q, int d_abs, in
         }
     }
     const uint32_t excl = incl - mine;
-    const int ea = static_cast<int>(excl & 0xFFFF) - 64 * lane;
-    const int eb = static_cast<int>(excl >> 16) - 64 * lane;
+    const int ea = static_cast<int>(excl & 0xFFFF) - kBias * lane;
+    const int eb = static_cast<int>(excl >> 16) - kBias * lane;
     const int a_r = __shfl_sync(~0u, d_abs, r);
-    const int pa_r = static_cast<int>(__shfl_sync(~0u, incl, r) & 0xFFFF) - 64 * (r + 1);
+    const int pa_r = static_cast<int>(__shfl_sync(~0u, incl, r) & 0xFFFF) - kBias * (r + 1);
     // the warp's summary
     const uint32_t all = __shfl_sync(~0u, incl, 31);
     const int last = b_reset ? 31 - __clz(b_reset) : 0;
     const int a_last = __shfl_sync(~0u, d_abs, last);
-    const int pa_last = static_cast<int>(__shfl_sync(~0u, incl, last) & 0xFFFF) - 64 * (last + 1);
+    const int pa_last = static_cast<int>(__shfl_sync(~0u, incl, last) & 0xFFFF) - kBias * (last + 1);
     const int nl_warp = __shfl_sync(~0u, nl_incl, 31);
     if (lane == 0) {
         WarpSum w;
@@ -332,19 +318,19 @@ __device__ __forceinline__ TileScan tile_scan(bool reset_w, int q, int d_abs, in
         w.nl = nl_warp;
         if (b_reset) {
             w.s = __popc(b_q & ~((1u << last) - 1)) & 1;
-            w.d_out = a_last + (static_cast<int>(all & 0xFFFF) - 64 * 32) - pa_last;
+            w.d_out = a_last + (static_cast<int>(all & 0xFFFF) - kBias * 32) - pa_last;
             w.d_in = w.d_out;
         } else {
             w.s = __popc(b_q) & 1;
-            w.d_out = static_cast<int>(all & 0xFFFF) - 64 * 32;
-            w.d_in = static_cast<int>(all >> 16) - 64 * 32;
+            w.d_out = static_cast<int>(all & 0xFFFF) - kBias * 32;
+            w.d_in = static_cast<int>(all >> 16) - kBias * 32;
         }
         sums[warp] = w;
     }
-    group_sync(kBarIndex, kIndexThreads);
-    // ---- across the warps: lane w < 8 holds warp w's summary, lane 8 an empty one
+    group_sync(kBarIndex, NW * 32);
+    // ---- across the warps: lane w < NW holds warp w's summary, lane NW an empty one
     WarpSum w{0, 0, 0, 0, 0};
-    if (lane < kTileWarps) w = sums[lane];
+    if (lane < NW) w = sums[lane];
     const unsigned c_reset = __ballot_sync(~0u, w.reset != 0);
     const unsigned c_q = __ballot_sync(~0u, w.s != 0);
     const unsigned cb = c_reset & lt;
@@ -354,7 +340,7 @@ __device__ __forceinline__ TileScan tile_scan(bool reset_w, int q, int d_abs, in
     const int cdelta = w.reset ? 0 : (cs ? w.d_in : w.d_out);
     int cincl = cdelta, cnl = w.nl;
 #pragma unroll
-    for (int off = 1; off <= kTileWarps; off <<= 1) {
+    for (int off = 1; off <= NW; off <<= 1) {
         const int o = __shfl_up_sync(~0u, cincl, off);
         const int on = __shfl_up_sync(~0u, cnl, off);
         if (lane >= off) {
@@ -382,10 +368,10 @@ __device__ __forceinline__ TileScan tile_scan(bool reset_w, int q, int d_abs, in
         out.d = in_d + (in_s ? eb : ea);
     }
     out.nl_before = in_nl + (nl_incl - nl);
-    out.lines_here = __shfl_sync(~0u, c_has, kTileWarps);
-    out.s_end = __shfl_sync(~0u, cs, kTileWarps);
-    out.d_end = __shfl_sync(~0u, cd, kTileWarps);
-    out.nl_total = __shfl_sync(~0u, cnl_excl, kTileWarps);
+    out.lines_here = __shfl_sync(~0u, c_has, NW);
+    out.s_end = __shfl_sync(~0u, cs, NW);
+    out.d_end = __shfl_sync(~0u, cd, NW);
+    out.nl_total = __shfl_sync(~0u, cnl_excl, NW);
     return out;
 }
 
@@ -977,21 +963,417 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
         line_warps<LV>(p, sh);
 }
 
-// Index only: the index warps alone, five CTAs per SM at up to 4 levels (48
-// registers), four at up to 8 and three at 16 (the level slots of deeper
-// indexes take more shared memory, so registers need no tighter cap); no
-// tile waits for another, since the newline index is built afterwards from
-// the counts.
+// ---- standalone index kernel ---------------------------------------------
+// Index builds without in-kernel queries (the default): 128 threads, each
+// owning four consecutive 64-byte words (256 bytes) of a 32 KiB slot, which
+// holds a 30 KiB tile and its 2 KiB look-ahead.  A thread classifies its
+// words one after another and composes their effect on the scan state
+// (string state, level, newline count) itself, so the warp scan, the
+// cross-warp scan and the tile's bookkeeping are paid once per four words.
+// What a word's classification leaves for the second pass (its masks and
+// level changes) is kept in shared memory where the word's bytes were, so
+// the slot holds bytes, then masks, then the level split's inputs, and four
+// CTAs fit per SM.  The level split deals the bracket cuts of a warp's 128
+// words over its lanes (deal_levels).  Writes the string index, the ':'
+// bitmap, the leveled bitmaps and the '\n' bitmap with one 32-byte store per
+// thread and bitmap where all four words are its own, and every tile's
+// newline count; no tile waits for another.  Ownership of words and lines
+// is the line kernel's (see the top of this file), with tiles of
+// kStandaloneTileBytes.
+constexpr int kWThreads = 128;
+constexpr int kWWarps = kWThreads / 32;
+constexpr int kWK = 4;                                     // consecutive words per thread
+constexpr int kWLaneBytes = 64 * kWK;                      // 256
+constexpr int64_t kWSlot = kWThreads * kWLaneBytes;        // 32 KiB
+constexpr int64_t kWTile = kStandaloneTileBytes;           // 30 KiB
+constexpr int kWTileLanes = static_cast<int>(kWTile / kWLaneBytes);  // threads 0..119: the tile
+constexpr int kWSlotWords = static_cast<int>(kWSlot / 64);           // 512
+constexpr int64_t kWRound = kWThreads * 64;                // extension rounds: one word per thread
+static_assert(kWTile % kWLaneBytes == 0 && kWSlot - kWTile == kExtBytes, "tile + 2 KiB look-ahead per slot");
+
 template <int LV>
-__global__ void __launch_bounds__(kIndexThreads, LV <= 4 ? 5 : (LV <= 8 ? 4 : 3)) tile_index_kernel(IndexParams p) {
+struct WShared {
+    // the tile's bytes (TMA destination); after a word is classified, its
+    // 64 bytes hold eight 8-byte cells of its state (word_cell)
+    uint8_t bytes[kWSlot];
+    union {
+        uint64_t acc[LV][kWSlotWords];    // level masks, at i * kWThreads + thread (deal_levels)
+        uint64_t lvacc[kWWarps][LV][32];  // split_levels_warp in the extension rounds
+    };
+    TileFile desc[2];  // the file of tile k in desc[k & 1]
+    uint64_t full;     // the slot's TMA barrier (phase k & 1 for tile k)
+    Span span_scratch[kWWarps];
+    WarpSum rscan[2][kWWarps];
+    int carry_esc;
+    int64_t long_b;
+};
+
+// Cell c (0..7) of word i of thread g, in the bytes the word was loaded
+// into.  Cells are rotated by the thread so that the threads of a warp
+// spread over the banks.  First pass: 0 quote prefix XOR, 1 '{['
+// (outside strings or not), 2 '}]', 3 structural, 4 ':', 5 '\n', 6 level
+// changes entered outside / inside a string, 7 quote parity or the string
+// state after a reset.  Second pass: 0 brackets opening, 1 brackets closing
+// (shifted to the byte after), 2 structural bytes, 3 level at the word's
+// first byte, all of the word's own and outside strings; 4 string mask,
+// 5 '\n' as before, 6 ':' outside strings.
+__device__ __forceinline__ uint64_t* word_cell(uint8_t* slot, int g, int i, int c) {
+    return reinterpret_cast<uint64_t*>(slot + kWLaneBytes * g + 64 * i + 8 * ((c + g) & 7));
+}
+
+// One 32-byte store of four words where all four are to be written and the
+// destination is 32-byte aligned, else one store per word of `mask`.
+__device__ __forceinline__ void store_words4(uint64_t* dst, const uint64_t (&v)[4], unsigned mask) {
+    if (mask == 0xFu && (reinterpret_cast<uintptr_t>(dst) & 31) == 0) {
+        asm volatile("st.global.v4.b64 [%0], {%1, %2, %3, %4};" ::"l"(dst), "l"(v[0]), "l"(v[1]), "l"(v[2]),
+                     "l"(v[3])
+                     : "memory");
+    } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+            if ((mask >> i) & 1u) dst[i] = v[i];
+    }
+}
+
+// Starts the TMA copy of tile t into the slot (one thread); its file goes
+// into desc[dslot] before the copy's arrive.
+template <int LV>
+__device__ __forceinline__ void start_wide_tile(const IndexParams& p, WShared<LV>& sh, int64_t t, int dslot) {
+    TileFile& F = sh.desc[dslot];
+    fetch_tile_file(p, t, &F);
+    const int64_t start = (t - F.tile_begin) * kWTile;
+    load_slot(F.file, start, F.avail - start < kWSlot ? F.avail - start : kWSlot, sh.bytes, &sh.full);
+}
+
+// The level split of the warp's 128 words (inputs in cells 0-3 of each
+// word, each word's first segment already in sh.acc): the segments that
+// start at a bracket cut are dealt out over the 32 lanes, one per lane per
+// pass, and OR-ed into the level slot of their word.  Cuts are few in most
+// words and many in some (tweets: 0.87 per word on average, three quarters
+// of the words have none), so dealing them over the warp takes about a
+// quarter of the passes of a per-thread loop, which runs as long as the
+// warp's densest thread.  `packed`: the cut counts of the thread's four
+// words, a byte each.
+template <int LV>
+__device__ __forceinline__ void deal_levels(WShared<LV>& sh, uint32_t packed) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int m = static_cast<int>((packed & 0xFF) + ((packed >> 8) & 0xFF) + ((packed >> 16) & 0xFF) + (packed >> 24));
+    int incl = m;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int o = __shfl_up_sync(~0u, incl, off);
+        if (lane >= off) incl += o;
+    }
+    const int base = incl - m;
+    const int total = __shfl_sync(~0u, incl, 31);
+    __syncwarp();
+    for (int r = 0; r < total; r += 32) {
+        const int g = r + lane;  // this lane's cut, numbered across the warp
+        int o = 0;               // its thread: the last lane whose first cut number is <= g
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1)
+            if (__shfl_sync(~0u, base, o + s) <= g) o += s;
+        const uint32_t pk = __shfl_sync(~0u, packed, o);
+        const int gi = g - __shfl_sync(~0u, base, o);  // cut number within thread o
+        const int p1 = static_cast<int>(pk & 0xFF);
+        const int p2 = p1 + static_cast<int>((pk >> 8) & 0xFF);
+        const int p3 = p2 + static_cast<int>((pk >> 16) & 0xFF);
+        const int wi = (gi >= p1 ? 1 : 0) + (gi >= p2 ? 1 : 0) + (gi >= p3 ? 1 : 0);  // its word
+        const int j = gi - (wi == 0 ? 0 : (wi == 1 ? p1 : (wi == 2 ? p2 : p3)));  // cut number within the word
+        if (g < total) {
+            const int og = 32 * warp + o;
+            const uint64_t op = *word_cell(sh.bytes, og, wi, 0), ca = *word_cell(sh.bytes, og, wi, 1);
+            const uint64_t st = *word_cell(sh.bytes, og, wi, 2);
+            const int dd = static_cast<int>(static_cast<int64_t>(*word_cell(sh.bytes, og, wi, 3)));
+            const uint64_t k = op | ca;
+            const int x = select_bit(k, j);
+            const uint64_t upto = bits_upto(x);
+            const uint64_t later = k & ~upto;
+            // bytes from the cut up to the next one (or the word end)
+            const uint64_t seg = st & ~(upto >> 1) & ((later & (~later + 1)) - 1);
+            const int level = dd + popc64(op & upto) - popc64(ca & upto);
+            if (seg && level >= 0 && level < LV)
+                atomicOr(reinterpret_cast<unsigned long long*>(&sh.acc[level][wi * kWThreads + og]),
+                         static_cast<unsigned long long>(seg));
+        }
+    }
+    __syncwarp();
+}
+
+// A line that runs past the slot: the rest of it, up to its '\n', from
+// device memory, one word per thread per round (the line kernel's long-line
+// path with 128 threads).  s_in / d_in: the scan state after the slot.
+template <int LV>
+__device__ void extend_long_line(const IndexParams& p, const TileFile& F, WShared<LV>& sh, int64_t loaded_end,
+                                 int64_t tile_end, int s_in, int64_t d_in) {
+    const int tid = threadIdx.x;
+    if (tid < 32) {
+        const int64_t e2 = find_line_end(F, loaded_end, tile_end);
+        if (tid == 0) {
+            sh.long_b = e2;
+            // the escape state at loaded_end: the backslash run before it
+            // lies in the line, which starts in this tile with a '\n'
+            int run = 0;
+            for (int64_t j = loaded_end - 1; j >= 0 && F.file[j] == '\\'; --j) ++run;
+            sh.carry_esc = run & 1;
+        }
+    }
+    group_sync(kBarIndex, kWThreads);
+    const int64_t b_t = sh.long_b;
+    const int64_t own_end = (b_t + 63) & ~static_cast<int64_t>(63);
+    int s = s_in, esc = sh.carry_esc;
+    int64_t d = d_in;
+    for (int64_t cs = loaded_end; cs < own_end && cs < F.n; cs += kWRound) {
+        const int64_t cw = cs + 64 * tid;
+        const uint64_t cvalid = cw < own_end ? bits_between(0, F.n - cw) : 0ull;
+        ClassMasks c{0, 0, 0, 0, 0, 0, 0};
+        if (cvalid) {
+            c = classify_global(F.file, F.n, cw);
+            restrict_masks(c, cvalid);
+        }
+        // escape carry: previous word's trailing run, else the bytes before
+        const bool all_bs = c.backslash == ~0ull;
+        const int trail_par = all_bs ? 0 : (clz64(~c.backslash) & 1);
+        const int prev_par = __shfl_up_sync(~0u, trail_par, 1);
+        const int prev_all = __shfl_up_sync(~0u, all_bs ? 1 : 0, 1);
+        uint32_t ccin;
+        if ((tid & 31) > 0 && !prev_all) {
+            ccin = static_cast<uint32_t>(prev_par);
+        } else if (!cvalid) {
+            ccin = 0;  // a word past the line's end: never scan bytes past the file
+        } else {
+            int run = 0;
+            int64_t j = cw - 1;
+            while (j >= cs && __ldg(F.file + j) == '\\') {
+                ++run;
+                --j;
+            }
+            ccin = static_cast<uint32_t>((run & 1) ^ (j < cs ? esc : 0));
+        }
+        uint32_t ccout;
+        const uint64_t cesc = escaped_mask(c.backslash, ccin, &ccout);
+        const uint64_t cq = c.quote & ~cesc;
+        const uint64_t cp0 = prefix_xor(cq);
+        const Span csp{popc64(cq) & 1, popc64(c.open & ~cp0) - popc64(c.close & ~cp0), popc64(c.open) - popc64(c.close),
+                       0};
+        Span ctotal;
+        const Span cex = index_scan_span<kWWarps>(csp, sh.span_scratch, &ctotal);
+        const uint64_t ccheck = (b_t >= cw && b_t < cw + 64) ? (c.newline & (1ull << (b_t - cw))) : 0ull;
+        finish_word<LV, false>(p, F, sh, 0, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0), cw >> 6, true,
+                               -1, cvalid, ccheck, cvalid != 0);
+        if (tid == kWThreads - 1) sh.carry_esc = static_cast<int>(ccout);
+        group_sync(kBarIndex, kWThreads);
+        esc = sh.carry_esc;
+        d += s ? (ctotal.ddt - ctotal.dd0) : ctotal.dd0;
+        s ^= ctotal.q;
+        group_sync(kBarIndex, kWThreads);
+    }
+}
+
+template <int LV>
+__global__ void __launch_bounds__(kWThreads, LV <= 4 ? 4 : (LV <= 8 ? 3 : 2)) tile_index_kernel(IndexParams p) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
-    TShared<LV>& sh = *reinterpret_cast<TShared<LV>*>(smem_raw);
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < TShared<LV>::kByteSlots; i++) mbar_init(&sh.full[i], 1);
+    WShared<LV>& sh = *reinterpret_cast<WShared<LV>*>(smem_raw);
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&sh.full, 1);
         fence_mbar_init();
     }
     __syncthreads();
-    index_warps<LV, false>(p, sh);
+    const int64_t first_tile = p.tile_begin + blockIdx.x, stride = gridDim.x;
+    if (tid == 0 && first_tile < p.tile_end) start_wide_tile(p, sh, first_tile, 0);
+    int64_t k = 0;
+    for (int64_t t = first_tile; t < p.tile_end; t += stride, ++k) {
+        if (!mbar_wait_bounded(&sh.full, static_cast<uint32_t>(k & 1)) && tid == 0)
+            atomicOr(p.status + 1, kErrCopyTimeout);
+        uint8_t* slot = sh.bytes;
+        const TileFile& F = sh.desc[k & 1];
+        const int64_t lt = t - F.tile_begin;  // the tile's index in its file
+        const int64_t tile_start = lt * kWTile;
+        const int64_t tile_end = F.n - tile_start < kWTile ? F.n : tile_start + kWTile;
+        const int64_t loaded_end = F.avail - tile_start < kWSlot ? F.avail : tile_start + kWSlot;
+        const bool ahead = tid >= kWTileLanes;  // the thread's words lie in the look-ahead
+        const int64_t lane_start = tile_start + kWLaneBytes * tid;
+        const int64_t vend = ahead ? loaded_end : tile_end;
+
+        // ---- first pass: classify the thread's four words, compose their scan effect
+        // The escape state entering the thread's bytes: a backslash run never
+        // crosses a '\n', so inside the slot the run before them is the whole
+        // run.  Read before any thread overwrites its bytes.
+        uint32_t cin = escape_scan_back(slot, kWK * tid, 0, 0);
+        group_sync(kBarIndex, kWThreads);
+        int l_reset = 0, l_s = 0, l_dout = 0, l_din = 0, l_nl = 0;
+#pragma unroll 1
+        for (int i = 0; i < kWK; i++) {
+            const int64_t ws = lane_start + 64 * i;
+            const uint64_t valid = bits_between(0, vend - ws);
+            ClassMasks m = load_classify(slot, kWK * tid + i);
+            if (valid != ~0ull) restrict_masks(m, valid);
+            uint32_t cout = 0;
+            const uint64_t esc = (m.backslash | cin) ? escaped_mask(m.backslash, cin, &cout) : 0ull;
+            cin = cout;
+            const uint64_t p0 = prefix_xor(m.quote & ~esc);
+            const bool has_nl = m.newline != 0;
+            const int f = has_nl ? ctz64(m.newline) : 0;
+            const int par_all = static_cast<int>(p0 >> 63);
+            int wq, wa, wb;
+            if (has_nl && !ahead) {
+                // a line starts after the word's first '\n': the state after the word is absolute
+                const uint64_t after = f == 63 ? 0ull : (~0ull << (f + 1));
+                const uint64_t pa = (p0 ^ (((p0 >> f) & 1ull) ? ~0ull : 0ull)) & after;
+                wq = par_all ^ static_cast<int>((p0 >> f) & 1ull);
+                wa = -1 + popc64(m.open & after & ~pa) - popc64(m.close & after & ~pa);
+                wb = 0;
+                l_reset = 1;
+                l_s = wq;
+                l_dout = wa;
+            } else {
+                wq = par_all;
+                wa = popc64(m.open & ~p0) - popc64(m.close & ~p0);  // entered outside a string
+                wb = popc64(m.open) - popc64(m.close) - wa;        // entered inside
+                if (l_reset) {
+                    l_dout += l_s ? wb : wa;
+                } else {
+                    const int a = l_dout + (l_s ? wb : wa);
+                    l_din += l_s ? wa : wb;
+                    l_dout = a;
+                }
+                l_s ^= wq;
+            }
+            l_nl += ahead ? (popc64(m.newline) << 16) : popc64(m.newline);
+            *word_cell(slot, tid, i, 0) = p0;
+            *word_cell(slot, tid, i, 1) = m.open;
+            *word_cell(slot, tid, i, 2) = m.close;
+            *word_cell(slot, tid, i, 3) = m.structural;
+            *word_cell(slot, tid, i, 4) = m.colon;
+            *word_cell(slot, tid, i, 5) = m.newline;
+            *word_cell(slot, tid, i, 6) = static_cast<uint32_t>(wa) | (static_cast<uint64_t>(static_cast<uint32_t>(wb)) << 32);
+            *word_cell(slot, tid, i, 7) = static_cast<uint64_t>(wq);
+        }
+        const TileScan sc = tile_scan<kWWarps, 64 * kWK>(l_reset != 0, l_s, l_dout, l_dout, l_din, l_nl, lt == 0,
+                                                         sh.rscan[k & 1]);
+        if (tid == 0) p.tile_newlines[t] = sc.nl_total & 0xFFFF;
+        const int ahead_nl = sc.nl_total >> 16;
+        const bool lines_here = sc.lines_here != 0;  // a line starts in this tile
+
+        // ---- second pass: final masks of the four words from the state at each one's first byte
+        int rb = sc.reset, s = sc.s, d = sc.d, nlb = sc.nl_before;
+        unsigned wmask = 0, packed = 0;
+#pragma unroll 1
+        for (int i = 0; i < kWK; i++) {
+            const int64_t ws = lane_start + 64 * i;
+            const uint64_t valid = bits_between(0, vend - ws);
+            const uint64_t p0 = *word_cell(slot, tid, i, 0), wopen = *word_cell(slot, tid, i, 1);
+            const uint64_t wclose = *word_cell(slot, tid, i, 2), wst = *word_cell(slot, tid, i, 3);
+            const uint64_t wcolon = *word_cell(slot, tid, i, 4), nl = *word_cell(slot, tid, i, 5);
+            const uint64_t ab = *word_cell(slot, tid, i, 6);
+            const int wq = static_cast<int>(*word_cell(slot, tid, i, 7));
+            const int wa = static_cast<int32_t>(static_cast<uint32_t>(ab)), wb = static_cast<int32_t>(ab >> 32);
+            const bool has_nl = nl != 0;
+            const int f = has_nl ? ctz64(nl) : 0;
+            const uint64_t after = has_nl ? (f == 63 ? 0ull : (~0ull << (f + 1))) : ~0ull;
+            // what this CTA finishes of the word, from which state
+            bool act = false, own = true;
+            uint64_t keep = ~0ull, wp0 = p0, check = 0;
+            int s_in = s, d_in = d;
+            if (!ahead) {
+                if (rb) {
+                    // every byte of the word belongs to lines that start in this tile
+                    act = ws < tile_end;
+                    check = nl;
+                } else if (has_nl) {
+                    // the tile's first line starts after byte f of this word
+                    keep = after;
+                    act = true;
+                    own = f == 0;
+                    wp0 = (p0 ^ (((p0 >> f) & 1ull) ? ~0ull : 0ull)) & after;
+                    s_in = 0;
+                    d_in = -1;
+                    check = nl & after;
+                }
+            } else if (lines_here && (nlb >> 16) == 0 && valid) {
+                // no '\n' between the tile end and this word: the tile's last
+                // line runs into it and ends at its first '\n' (the only one checked)
+                act = !(has_nl && f == 0);
+                check = has_nl ? (1ull << f) : 0ull;
+            }
+            const uint64_t in_str = (wp0 ^ (s_in ? ~0ull : 0ull)) & valid;
+            const uint64_t open = wopen & keep & ~in_str, close = wclose & keep & ~in_str;
+            if (act && check) {
+                // every checked '\n' must be outside strings at level -1
+                if (check & in_str) atomicOr(F.status + 1, kErrIrregular);
+                for (uint64_t c = check; c; c &= c - 1) {
+                    const uint64_t below = (1ull << ctz64(c)) - 1;
+                    if (d_in + popc64(open & below) - popc64(close & below) != -1) atomicOr(F.status + 1, kErrIrregular);
+                }
+            }
+            const bool split = act && own;
+            const uint64_t sk = split ? ~0ull : 0ull;
+            const uint64_t op = open & sk, ca = (close << 1) & sk, st = wst & keep & ~in_str & sk;
+            const int dd = d_in > 128 ? 128 : (d_in < -128 ? -128 : d_in);
+            *word_cell(slot, tid, i, 0) = op;
+            *word_cell(slot, tid, i, 1) = ca;
+            *word_cell(slot, tid, i, 2) = st;
+            *word_cell(slot, tid, i, 3) = static_cast<uint64_t>(static_cast<int64_t>(dd));
+            *word_cell(slot, tid, i, 4) = in_str;
+            *word_cell(slot, tid, i, 6) = wcolon & keep & ~in_str;
+            // the word's first segment (all of it without cuts) at its first level
+            const uint64_t cuts = op | ca;
+            const uint64_t seg0 = st & ((cuts & (~cuts + 1)) - 1);
+#pragma unroll
+            for (int l = 0; l < LV; l++) sh.acc[l][i * kWThreads + tid] = dd == l ? seg0 : 0ull;
+            packed |= static_cast<uint32_t>(popc64(cuts)) << (8 * i);
+            wmask |= split ? (1u << i) : 0u;
+            // the state at the next word's first byte
+            if (has_nl && !ahead) {
+                rb = 1;
+                s = wq;
+                d = wa;
+            } else {
+                d += s ? wb : wa;
+                s ^= wq;
+            }
+            nlb += ahead ? (popc64(nl) << 16) : popc64(nl);
+        }
+        deal_levels<LV>(sh, packed);
+        // ---- the thread's words to the index
+        if (!ahead) {  // the '\n' bitmap of the tile's words
+            const unsigned own_nl =
+                lane_start + kWLaneBytes <= tile_end
+                    ? 0xFu
+                    : (lane_start < tile_end ? ((1u << ((tile_end - lane_start + 63) >> 6)) - 1u) : 0u);
+            if (own_nl) {
+                uint64_t v[kWK];
+#pragma unroll
+                for (int i = 0; i < kWK; i++) v[i] = *word_cell(slot, tid, i, 5);
+                store_words4(F.newline_bits + (lane_start >> 6), v, own_nl);
+            }
+        }
+        if (p.materialize && wmask) {
+            const int64_t w0 = lane_start >> 6;
+            uint64_t v[kWK];
+#pragma unroll
+            for (int i = 0; i < kWK; i++) v[i] = *word_cell(slot, tid, i, 4);
+            store_words4(F.string_index + w0, v, wmask);
+            if (F.colon) {
+#pragma unroll
+                for (int i = 0; i < kWK; i++) v[i] = *word_cell(slot, tid, i, 6);
+                store_words4(F.colon + w0, v, wmask);
+            }
+#pragma unroll
+            for (int l = 0; l < LV; l++) {
+                if (l < p.num_levels) {
+#pragma unroll
+                    for (int i = 0; i < kWK; i++) v[i] = sh.acc[l][i * kWThreads + tid];
+                    store_words4(F.leveled + F.level_size * l + w0, v, wmask);
+                }
+            }
+        }
+        group_sync(kBarIndex, kWThreads);  // the slot and sh.acc are read: the next tile's copy may start
+        if (tid == 0 && t + stride < p.tile_end) start_wide_tile(p, sh, t + stride, static_cast<int>((k + 1) & 1));
+        if (lines_here && tile_end < F.n && ahead_nl == 0 && loaded_end < F.n)
+            extend_long_line<LV>(p, F, sh, loaded_end, tile_end, sc.s_end, sc.d_end);
+    }
 }
 
 // Raises a kernel's dynamic shared memory limit, once per device (the
@@ -1013,8 +1395,8 @@ struct KernelOf {
     static void* fn() {
         return kLines ? reinterpret_cast<void*>(line_index_kernel<LV>) : reinterpret_cast<void*>(tile_index_kernel<LV>);
     }
-    static size_t smem() { return kLines ? sizeof(FShared<LV>) : sizeof(TShared<LV>); }
-    static int threads() { return kLines ? kThreads : kIndexThreads; }
+    static size_t smem() { return kLines ? sizeof(FShared<LV>) : sizeof(WShared<LV>); }
+    static int threads() { return kLines ? kThreads : kWThreads; }
     static std::atomic<unsigned long long>& done() {
         static std::atomic<unsigned long long> d{0};
         return d;
@@ -1039,7 +1421,7 @@ cudaError_t launch(const IndexParams& p, int grid, cudaStream_t stream) {
     if (kLines)
         line_index_kernel<LV><<<grid, kThreads, sizeof(FShared<LV>), stream>>>(p);
     else
-        tile_index_kernel<LV><<<grid, kIndexThreads, sizeof(TShared<LV>), stream>>>(p);
+        tile_index_kernel<LV><<<grid, kWThreads, sizeof(WShared<LV>), stream>>>(p);
     return cudaGetLastError();
 }
 

@@ -18,8 +18,8 @@ namespace gpj {
 namespace {
 
 constexpr int kScanThreads = 1024;
-constexpr int kTileWordsL = static_cast<int>(kLineTileBytes / 64);  // 224
-constexpr int kWordsPerLane = kTileWordsL / 32;                      // 7
+constexpr int kTileWordsL = static_cast<int>(kStandaloneTileBytes / 64);  // 480
+constexpr int kWordsPerLane = kTileWordsL / 32;                            // 15
 static_assert(kWordsPerLane * 32 == kTileWordsL, "a tile's words split evenly over a warp");
 
 // Offsets of the tile counts within blocks of 1024 tiles (coalesced, one
@@ -138,7 +138,7 @@ cudaError_t launch_newline_index_batch(const int32_t* tile_newlines, int64_t tot
 
 cudaError_t launch_newline_index_range(const IndexParams& p, int64_t* offsets, int64_t t0, int64_t t1,
                                        int64_t* lines_done, int grid, cudaStream_t stream) {
-    const int64_t ntiles = (p.n + kLineTileBytes - 1) / kLineTileBytes;
+    const int64_t ntiles = (p.n + kStandaloneTileBytes - 1) / kStandaloneTileBytes;
     if (t0 % kScanThreads != 0 || t1 <= t0 || t1 > ntiles || (t1 != ntiles && t1 % kScanThreads != 0))
         return cudaErrorInvalidValue;
     const int64_t blk0 = t0 / kScanThreads;
@@ -154,7 +154,7 @@ cudaError_t launch_newline_index_range(const IndexParams& p, int64_t* offsets, i
 }
 
 cudaError_t launch_newline_index(const IndexParams& p, int64_t* offsets, int grid, cudaStream_t stream) {
-    const int64_t ntiles = (p.n + kLineTileBytes - 1) / kLineTileBytes;
+    const int64_t ntiles = (p.n + kStandaloneTileBytes - 1) / kStandaloneTileBytes;
     return launch_newline_index_range(p, offsets, 0, ntiles, nullptr, grid, stream);
 }
 
