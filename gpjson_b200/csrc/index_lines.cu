@@ -973,8 +973,8 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
 // What a word's classification leaves for the second pass (its masks and
 // level changes) is kept in shared memory where the word's bytes were, so
 // the slot holds bytes, then masks, then the level split's inputs, and four
-// CTAs fit per SM.  The level split deals the bracket cuts of a warp's 128
-// words over its lanes (deal_levels).  Writes the string index, the ':'
+// CTAs fit per SM.  The level split deals the warp's words that hold
+// bracket cuts over its lanes (deal_levels).  Writes the string index, the ':'
 // bitmap, the leveled bitmaps and the '\n' bitmap with one 32-byte store per
 // thread and bitmap where all four words are its own, and every tile's
 // newline count; no tile waits for another.  Ownership of words and lines
@@ -1013,10 +1013,10 @@ struct WShared {
 // spread over the banks.  First pass: 0 quote prefix XOR, 1 '{['
 // (outside strings or not), 2 '}]', 3 structural, 4 ':', 5 '\n', 6 level
 // changes entered outside / inside a string, 7 quote parity or the string
-// state after a reset.  Second pass: 0 brackets opening, 1 brackets closing
-// (shifted to the byte after), 2 structural bytes, 3 level at the word's
-// first byte, all of the word's own and outside strings; 4 string mask,
-// 5 '\n' as before, 6 ':' outside strings.
+// state after a reset.  Second pass: 0 opening brackets, 1 closing
+// brackets, 2 structural bytes, 3 level at the word's first byte, all of
+// the word's own and outside strings; 4 string mask, 5 '\n' as before,
+// 6 ':' outside strings.
 __device__ __forceinline__ uint64_t* word_cell(uint8_t* slot, int g, int i, int c) {
     return reinterpret_cast<uint64_t*>(slot + kWLaneBytes * g + 64 * i + 8 * ((c + g) & 7));
 }
@@ -1045,19 +1045,19 @@ __device__ __forceinline__ void start_wide_tile(const IndexParams& p, WShared<LV
     load_slot(F.file, start, F.avail - start < kWSlot ? F.avail - start : kWSlot, sh.bytes, &sh.full);
 }
 
-// The level split of the warp's 128 words (inputs in cells 0-3 of each
-// word, each word's first segment already in sh.acc): the segments that
-// start at a bracket cut are dealt out over the 32 lanes, one per lane per
-// pass, and OR-ed into the level slot of their word.  Cuts are few in most
-// words and many in some (tweets: 0.87 per word on average, three quarters
-// of the words have none), so dealing them over the warp takes about a
-// quarter of the passes of a per-thread loop, which runs as long as the
-// warp's densest thread.  `packed`: the cut counts of the thread's four
-// words, a byte each.
+// The level split of the warp's words that hold bracket cuts (inputs in
+// cells 0-3 of each word; sh.acc already holds every word's masks as if it
+// had none): such words are dealt out over the 32 lanes, one per lane per
+// pass, and each is split by split_levels, which walks its cuts.  A
+// quarter of the words have cuts and their counts differ a lot (tweets: 0.87
+// per word on average, many with eight or more), so dealing them over the
+// warp keeps most lanes busy, where a loop per thread would run as long as
+// the warp's densest thread.  `cmask`: which of the thread's four words have
+// cuts.
 template <int LV>
-__device__ __forceinline__ void deal_levels(WShared<LV>& sh, uint32_t packed) {
+__device__ __forceinline__ void deal_levels(WShared<LV>& sh, unsigned cmask) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int m = static_cast<int>((packed & 0xFF) + ((packed >> 8) & 0xFF) + ((packed >> 16) & 0xFF) + (packed >> 24));
+    const int m = __popc(cmask);
     int incl = m;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -1068,33 +1068,29 @@ __device__ __forceinline__ void deal_levels(WShared<LV>& sh, uint32_t packed) {
     const int total = __shfl_sync(~0u, incl, 31);
     __syncwarp();
     for (int r = 0; r < total; r += 32) {
-        const int g = r + lane;  // this lane's cut, numbered across the warp
-        int o = 0;               // its thread: the last lane whose first cut number is <= g
+        const int g = r + lane;  // this lane's word with cuts, numbered across the warp
+        int o = 0;               // its thread: the last lane whose first number is <= g
 #pragma unroll
         for (int s = 16; s > 0; s >>= 1)
             if (__shfl_sync(~0u, base, o + s) <= g) o += s;
-        const uint32_t pk = __shfl_sync(~0u, packed, o);
-        const int gi = g - __shfl_sync(~0u, base, o);  // cut number within thread o
-        const int p1 = static_cast<int>(pk & 0xFF);
-        const int p2 = p1 + static_cast<int>((pk >> 8) & 0xFF);
-        const int p3 = p2 + static_cast<int>((pk >> 16) & 0xFF);
-        const int wi = (gi >= p1 ? 1 : 0) + (gi >= p2 ? 1 : 0) + (gi >= p3 ? 1 : 0);  // its word
-        const int j = gi - (wi == 0 ? 0 : (wi == 1 ? p1 : (wi == 2 ? p2 : p3)));  // cut number within the word
+        const unsigned cm = __shfl_sync(~0u, cmask, o);
+        int c = g - __shfl_sync(~0u, base, o);  // number within thread o
+        int wi = 0;                              // its word: the c-th set bit of cm
+#pragma unroll
+        for (int b = 0; b < kWK; b++) {
+            const int has = (cm >> b) & 1u;
+            if (has && c == 0) wi = b;
+            c -= has;
+        }
         if (g < total) {
             const int og = 32 * warp + o;
-            const uint64_t op = *word_cell(sh.bytes, og, wi, 0), ca = *word_cell(sh.bytes, og, wi, 1);
+            const uint64_t op = *word_cell(sh.bytes, og, wi, 0), cl = *word_cell(sh.bytes, og, wi, 1);
             const uint64_t st = *word_cell(sh.bytes, og, wi, 2);
             const int dd = static_cast<int>(static_cast<int64_t>(*word_cell(sh.bytes, og, wi, 3)));
-            const uint64_t k = op | ca;
-            const int x = select_bit(k, j);
-            const uint64_t upto = bits_upto(x);
-            const uint64_t later = k & ~upto;
-            // bytes from the cut up to the next one (or the word end)
-            const uint64_t seg = st & ~(upto >> 1) & ((later & (~later + 1)) - 1);
-            const int level = dd + popc64(op & upto) - popc64(ca & upto);
-            if (seg && level >= 0 && level < LV)
-                atomicOr(reinterpret_cast<unsigned long long*>(&sh.acc[level][wi * kWThreads + og]),
-                         static_cast<unsigned long long>(seg));
+            uint64_t lv[LV];
+            split_levels<LV>(op, cl, st, dd, lv);
+#pragma unroll
+            for (int l = 0; l < LV; l++) sh.acc[l][wi * kWThreads + og] = lv[l];
         }
     }
     __syncwarp();
@@ -1258,7 +1254,7 @@ __global__ void __launch_bounds__(kWThreads, LV <= 4 ? 4 : (LV <= 8 ? 3 : 2)) ti
 
         // ---- second pass: final masks of the four words from the state at each one's first byte
         int rb = sc.reset, s = sc.s, d = sc.d, nlb = sc.nl_before;
-        unsigned wmask = 0, packed = 0;
+        unsigned wmask = 0, cmask = 0;
 #pragma unroll 1
         for (int i = 0; i < kWK; i++) {
             const int64_t ws = lane_start + 64 * i;
@@ -1309,20 +1305,19 @@ __global__ void __launch_bounds__(kWThreads, LV <= 4 ? 4 : (LV <= 8 ? 3 : 2)) ti
             }
             const bool split = act && own;
             const uint64_t sk = split ? ~0ull : 0ull;
-            const uint64_t op = open & sk, ca = (close << 1) & sk, st = wst & keep & ~in_str & sk;
+            const uint64_t op = open & sk, cl = close & sk, st = wst & keep & ~in_str & sk;
             const int dd = d_in > 128 ? 128 : (d_in < -128 ? -128 : d_in);
             *word_cell(slot, tid, i, 0) = op;
-            *word_cell(slot, tid, i, 1) = ca;
+            *word_cell(slot, tid, i, 1) = cl;
             *word_cell(slot, tid, i, 2) = st;
             *word_cell(slot, tid, i, 3) = static_cast<uint64_t>(static_cast<int64_t>(dd));
             *word_cell(slot, tid, i, 4) = in_str;
             *word_cell(slot, tid, i, 6) = wcolon & keep & ~in_str;
-            // the word's first segment (all of it without cuts) at its first level
-            const uint64_t cuts = op | ca;
-            const uint64_t seg0 = st & ((cuts & (~cuts + 1)) - 1);
+            // a word without bracket cuts is all at its first level (words
+            // with cuts are split by deal_levels)
 #pragma unroll
-            for (int l = 0; l < LV; l++) sh.acc[l][i * kWThreads + tid] = dd == l ? seg0 : 0ull;
-            packed |= static_cast<uint32_t>(popc64(cuts)) << (8 * i);
+            for (int l = 0; l < LV; l++) sh.acc[l][i * kWThreads + tid] = dd == l ? st : 0ull;
+            cmask |= (op | (cl << 1)) ? (1u << i) : 0u;
             wmask |= split ? (1u << i) : 0u;
             // the state at the next word's first byte
             if (has_nl && !ahead) {
@@ -1335,7 +1330,7 @@ __global__ void __launch_bounds__(kWThreads, LV <= 4 ? 4 : (LV <= 8 ? 3 : 2)) ti
             }
             nlb += ahead ? (popc64(nl) << 16) : popc64(nl);
         }
-        deal_levels<LV>(sh, packed);
+        deal_levels<LV>(sh, cmask);
         // ---- the thread's words to the index
         if (!ahead) {  // the '\n' bitmap of the tile's words
             const unsigned own_nl =
