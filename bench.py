@@ -34,8 +34,35 @@ sys.path.insert(0, str(ROOT))
 QUERIES = ["$.user.lang", "$.id", "$.user.followers_count", "$.entities.hashtags[0].text"]
 FILE_BYTES = 1 << 31
 LEVELS = 4
-TILE = 16384
 PROFILE_TRAFFIC = ROOT / "profiles" / "dram_traffic_tweets_256MiB.json"
+
+
+class Workload:
+    """One NDJSON file of a configuration's shape and its queries."""
+
+    def __init__(self, name: str, nbytes: int, levels: int, queries: list[str], kind: str, seed: int):
+        self.name, self.bytes, self.levels, self.queries, self.kind, self.seed = name, nbytes, levels, queries, kind, seed
+
+    def generate(self, n: int, rank: int = 0, out=None):
+        from gpjson_b200 import datagen
+
+        if self.kind == "tweets":
+            return datagen.tweets(n, seed=self.seed + rank, p_empty_hashtags=0.3, out=out)
+        return datagen.adversarial(n, seed=self.seed + rank, out=out)
+
+    def describe(self, n: int, lines: int) -> str:
+        what = ("tweet-like NDJSON" if self.kind == "tweets" else
+                "adversarial NDJSON (lines 100 B-1 MiB log-uniform, nesting 1-16, arrays of 0-1000 numbers, "
+                "backslash runs)")
+        return (f"{what}, {n} B per GPU ({lines} lines), one index build ({self.levels} levels) + "
+                f"{len(self.queries)} queries fused in one pass over it")
+
+
+# the 2 GiB tweet-like file with its four queries (the headline), and the
+# 4 GiB adversarial file with its three queries
+TWEETS = Workload("tweets", FILE_BYTES, LEVELS, QUERIES, "tweets", 0x67706A73 + 1)
+ADVERSARIAL = Workload("adversarial", 4 << 30, 5, ["$.a.b.c.d", "$.arr[5]", "$.x[0].y[2].z"], "adversarial",
+                       0x67706A73 + 2)
 
 
 def parse_args(argv=None):
@@ -44,7 +71,8 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--bytes", type=int, default=FILE_BYTES, help="input file size (default 2 GiB)")
+    ap.add_argument("--bytes", type=int, default=None,
+                    help="input file size (default: 2 GiB tweet-like, 4 GiB adversarial)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample", type=int, default=512 << 20, help="bytes of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -52,8 +80,9 @@ def parse_args(argv=None):
                     help="default: gpj_index_query_device as shipped (index kernel, then one find_value "
                          "launch for all queries); fused: the queries evaluated inside the index kernel; "
                          "index: index only (diagnostic)")
-    ap.add_argument("--workload", choices=["tweets", "batched", "serving"], default="tweets",
-                    help="tweets: the 2 GiB single-file headline; batched: 512 files of 4 KiB-64 MiB, 1-8 "
+    ap.add_argument("--workload", choices=["tweets", "adversarial", "batched", "serving"], default="tweets",
+                    help="tweets: the 2 GiB single-file headline; adversarial: the 4 GiB adversarial file with "
+                         "its three queries; batched: 512 files of 4 KiB-64 MiB, 1-8 "
                          "queries each, one batch vs per-file calls; serving: 64 resident corpora, Poisson "
                          "requests, continuous batching vs per-request")
     ap.add_argument("--requests", type=int, default=20000, help="serving: number of requests")
@@ -170,7 +199,7 @@ def ncu_traffic(key: str):
         return None
 
 
-def cpu_baseline(data_np, n_sample: int, threads_all: bool):
+def cpu_baseline(data_np, n_sample: int, threads_all: bool, w: Workload = TWEETS):
     """The oracle port of the reference's sequential path on a sample."""
     from oracle import oracle
 
@@ -181,39 +210,35 @@ def cpu_baseline(data_np, n_sample: int, threads_all: bool):
         cut -= 1
     sample = sample[:cut]
     t0 = time.perf_counter()
-    idx = oracle.Index(sample, LEVELS, mt=threads_all)
-    oracle.query(sample, QUERIES, mt=threads_all, index=idx)
+    idx = oracle.Index(sample, w.levels, mt=threads_all)
+    oracle.query(sample, w.queries, mt=threads_all, index=idx)
     dt = time.perf_counter() - t0
     return cut / dt / 1e9, cut, dt, (oracle.num_threads() if threads_all else 1)
 
 
 def run_reference(args, rank: int, world: int) -> None:
-    """CPU reference arm: the oracle restatement of Sequential, all threads."""
+    """CPU reference arm: the oracle restatement of Sequential on all host
+    threads, over the same whole file as our arm (same generator, seed, size
+    and queries)."""
     if rank != 0:
         return
-    import numpy as np
-
-    from gpjson_b200 import datagen
-
     from oracle import oracle
 
-    n = min(args.cpu_sample, args.bytes)
-    data = datagen.tweets(n, seed=datagen.SEED_BASE + 1, p_empty_hashtags=0.3)
-    cut = n
-    while cut > 0 and data[cut - 1] != 10:
-        cut -= 1
-    sample = data[:cut]
+    w = ADVERSARIAL if args.workload == "adversarial" else TWEETS
+    n = args.bytes or w.bytes
+    data = w.generate(n)
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        idx = oracle.Index(sample, LEVELS, mt=True)
-        oracle.query(sample, QUERIES, mt=True, index=idx)
+        idx = oracle.Index(data, w.levels, mt=True)
+        oracle.query(data, w.queries, mt=True, index=idx)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             times.append(dt)
     ms = 1000 * statistics.mean(times)
-    value = cut / (ms / 1000) / 1e9
+    value = n / (ms / 1000) / 1e9
     cores = oracle.num_threads()
+    lines = len(idx.newlines)
     line = {
         "impl": "reference",
         "metric": "input GB/s (index+query)",
@@ -229,17 +254,18 @@ def run_reference(args, rank: int, world: int) -> None:
         "dtype": "u8",
         "data": "synthetic",
         "config": {
-            "workload": f"tweet-like NDJSON sample of {cut} B (the 2 GiB workload's generator), index "
-                        f"({LEVELS} levels) + 4 queries",
-            "queries": QUERIES,
-            "bytes_per_step": cut,
+            "workload": w.describe(n, lines),
+            "queries": w.queries,
+            "bytes_per_gpu": n,
+            "lines_per_gpu": lines,
         },
         "cpu_baseline": {
             "value": round(value, 4),
             "unit": "GB/s",
             "cores": cores,
             "kind": "port",
-            "sample": f"{cut} B prefix of the seeded 2 GiB tweet-like file, whole lines",
+            "sample": f"the whole {n} B file of the GPU arm's workload, index ({w.levels} levels) + "
+                      f"{len(w.queries)} queries per step",
         },
         "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -247,13 +273,7 @@ def run_reference(args, rank: int, world: int) -> None:
 
 
 def run_ours(args, rank: int, world: int, local: int) -> None:
-    import ctypes
-
-    import numpy as np
     import torch
-
-    import gpjson_b200 as gj
-    from gpjson_b200 import datagen
 
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
@@ -263,11 +283,32 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+    w = ADVERSARIAL if args.workload == "adversarial" else TWEETS
+    result = measure_file(args, w, rank, world, local, device)
+    if world > 1:
+        import torch.distributed as dist
 
-    n = args.bytes
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def measure_file(args, w: Workload, rank: int, world: int, local: int, device) -> dict:
+    """The single-file workload `w`: device-resident passes (value), the end
+    to end passes through the C ABI (e2e), the roofline of the index kernel
+    and the CPU baseline; returns the JSON line's fields."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import gpjson_b200 as gj
+
+    QUERIES, LEVELS = w.queries, w.levels
+    n = args.bytes or w.bytes
     host = torch.empty(n, dtype=torch.uint8, pin_memory=True)
     host_np = host.numpy()
-    datagen.tweets(n, seed=datagen.SEED_BASE + 1 + rank, p_empty_hashtags=0.3, out=host_np)
+    w.generate(n, rank, out=host_np)
     dev = host.to(device, non_blocking=False)
     torch.cuda.synchronize()
 
@@ -292,7 +333,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
     g.set_query_fusion(args.mode == "fused")
 
     def step(ev=None):
-        """One pass: index (4 levels) + the 4 queries in one pass over it, input in HBM."""
+        """One pass: index + the queries in one pass over it, input in HBM."""
         if ev:
             ev[0].record(stream)
         if args.mode == "index":
@@ -432,8 +473,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         "dtype": "u8",
         "data": "synthetic",
         "config": {
-            "workload": f"tweet-like NDJSON, {n} B per GPU ({lines} lines), one index build ({LEVELS} levels) "
-                        "+ 4 queries fused in one pass over it",
+            "workload": w.describe(n, lines),
             "mode": args.mode,
             "queries": QUERIES,
             "bytes_per_gpu": n,
@@ -446,7 +486,7 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         "kernels_ms": {k: round(v, 4) for k, v in kernel_ms.items()},
         "roofline": {
             "bound": "hbm",
-            "kernel": ("line_index_kernel (with the 4 queries)" if dom == "index_and_query"
+            "kernel": ("line_index_kernel (with the queries)" if dom == "index_and_query"
                        else "tile_index_kernel (+ the two newline index kernels)"),
             "achieved": round(achieved, 1),
             "peak": peak,
@@ -474,22 +514,19 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         "clocks": clock_info,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cut, dt, cores = cpu_baseline(host_np, min(args.cpu_sample, n), threads_all=False)
+        v, cut, dt, cores = cpu_baseline(host_np, min(args.cpu_sample, n), threads_all=False, w=w)
         result["cpu_baseline"] = {
             "value": round(v, 4),
             "unit": "GB/s",
             "cores": cores,
             "kind": "port",
-            "sample": f"{cut} B prefix (whole lines) of the same file, index + 4 queries, {dt:.1f} s",
+            "sample": f"{cut} B prefix (whole lines) of the same file, index + {len(QUERIES)} queries, {dt:.1f} s",
         }
     f.release()
     g.close()
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
-    if rank == 0:
-        print(json.dumps(result), flush=True)
+    del dev, out, host
+    torch.cuda.empty_cache()
+    return result
 
 
 def batched_corpus(seed: int = 0x67706A73 + 3, files: int = 512):

@@ -29,6 +29,13 @@ GPJ_ESTATE = -9
 GPJ_MAX_QUERIES = 255
 GPJ_MAX_LEVELS = 16
 
+class Tuning(ctypes.Structure):
+    """gpj_tuning: launch shapes of a context's kernels."""
+
+    _fields_ = [("long_line_bytes", c_int64), ("query_ctas_per_sm", ctypes.c_int32),
+                ("index_ctas_per_sm", ctypes.c_int32)]
+
+
 # name -> (restype, argtypes); the full list of exported entry points.
 SIGNATURES: dict[str, tuple] = {
     "gpj_create": (c_int, [c_int, POINTER(c_void_p)]),
@@ -59,6 +66,8 @@ SIGNATURES: dict[str, tuple] = {
         [c_void_p, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_void_p, c_int64, POINTER(c_int64)],
     ),
     "gpj_set_query_fusion": (c_int, [c_void_p, c_int]),
+    "gpj_set_tuning": (c_int, [c_void_p, POINTER(Tuning)]),
+    "gpj_get_tuning": (c_int, [c_void_p, POINTER(Tuning)]),
     "gpj_set_path_extensions": (c_int, [c_void_p, c_uint]),
     "gpj_compile_ex": (
         c_int,

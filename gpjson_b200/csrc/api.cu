@@ -39,6 +39,17 @@ struct Phase {
 
 }  // namespace
 
+// Entries of a context's list of long lines handed to a warp each.
+static constexpr int64_t kLongItems = 1 << 16;
+
+static gpj_tuning default_tuning() {
+    gpj_tuning t{};
+    t.long_line_bytes = 65536;
+    t.query_ctas_per_sm = 0;
+    t.index_ctas_per_sm = 0;
+    return t;
+}
+
 struct gpj_ctx {
     int device = 0;
     int sms = 0;
@@ -66,6 +77,10 @@ struct gpj_ctx {
     bool fuse_queries = false;           // evaluate queries inside the index kernel
     unsigned path_extensions = 0;        // GPJ_PATH_* flags for calls that compile paths
     int query_occupancy[3] = {0, 0, 0};  // find_value CTAs per SM, by register-state size (depth <= 4, <= 8, more)
+    // lines find_value hands to a warp each (gpj_tuning); the hand-over list
+    gpj_tuning tuning{};
+    gpj::LongItem* d_long = nullptr;
+    unsigned long long* d_long_count = nullptr;
 
     // pinned staging for file reads
     uint8_t* h_stage = nullptr;
@@ -91,6 +106,7 @@ struct gpj_file {
     int64_t* d_nl = nullptr;
     int64_t nl_cap = 0;
     bool indexed = false;
+    bool exact_only = false;  // the line kernels flagged this input: index it with the exact kernel
     int num_levels = 0;
     int64_t num_lines = 0;
 
@@ -313,8 +329,16 @@ void set_tile_range(gpj::IndexParams* p, int64_t tile_begin, int64_t tile_end, i
     p->avail = avail;
 }
 
+// Standalone index kernel CTAs per SM (the tuning's choice when it sets one
+// below the maximum).
+int tile_ctas_per_sm(const gpj_ctx* ctx, int num_levels) {
+    const int occ = ctx->tile_occupancy[occupancy_slot(num_levels)];
+    const int want = ctx->tuning.index_ctas_per_sm;
+    return want > 0 && want < occ ? want : occ;
+}
+
 int launch_tiles(gpj_ctx* ctx, const gpj::IndexParams& p) {
-    const int occ = ctx->tile_occupancy[occupancy_slot(p.num_levels)];
+    const int occ = tile_ctas_per_sm(ctx, p.num_levels);
     const int64_t grid = std::min<int64_t>(p.tile_end - p.tile_begin, static_cast<int64_t>(ctx->sms) * occ);
     GPJ_CUDA(ctx, gpj::launch_tile_index_kernel(p, static_cast<int>(grid), ctx->stream));
     ctx->launches++;
@@ -340,9 +364,13 @@ int finish_tiles(gpj_ctx* ctx, const gpj::IndexParams& p, const TileScratch& ts)
 // tells whether every line's query results were written.
 // d_colon (optional) receives the ':' bitmap when the standalone kernel
 // builds the index; *colon_valid (optional) tells whether it did.
+// *exact_only (optional, in and out): the input needs the exact kernel (a
+// line kernel flagged it before, so later builds of the same input skip
+// straight to the exact kernel).
 int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, uint64_t* d_str,
               uint64_t* d_lvl, int64_t* d_nl, int64_t nl_cap, int64_t* lines, const FusedQueries* fq = nullptr,
-              bool* queries_done = nullptr, uint64_t* d_colon = nullptr, bool* colon_valid = nullptr) {
+              bool* queries_done = nullptr, uint64_t* d_colon = nullptr, bool* colon_valid = nullptr,
+              bool* exact_only = nullptr) {
     if (queries_done) *queries_done = false;
     if (colon_valid) *colon_valid = false;
     if (n == 0) {
@@ -378,6 +406,15 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
         fused.out_lines = fq->out_lines;
     }
     int rc;
+    if (exact_only && *exact_only) {
+        // known from an earlier build: the line kernels would flag this input
+        ctx->exact_fallbacks++;
+        rc = launch_index(ctx, true, p);
+        if (rc) return rc;
+        if ((rc = status_error(ctx, ctx->h_status[1]))) return rc;
+        *lines = static_cast<int64_t>(ctx->h_status[0]);
+        return GPJ_OK;
+    }
     if (fq && fq->nq > 0) {
         rc = launch_index(ctx, false, fused);
         if (rc) return rc;
@@ -407,6 +444,7 @@ int run_index(gpj_ctx* ctx, const uint8_t* d_file, int64_t n, int num_levels, ui
     if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) {
         ctx->exact_fallbacks++;
         exact = true;
+        if (exact_only) *exact_only = true;
         rc = launch_index(ctx, true, p);
         if (rc) return rc;
         errs = ctx->h_status[1];
@@ -479,9 +517,18 @@ int upload_queries(gpj_ctx* ctx, gpj_file* f, int nq, const uint8_t* const* bc, 
     return GPJ_OK;
 }
 
-// find_value CTAs per SM for queries no deeper than `depth`.
+// find_value CTAs per SM for queries no deeper than `depth` (the tuning's
+// choice when it sets one below the maximum).
 int query_occupancy(const gpj_ctx* ctx, int depth) {
-    return ctx->query_occupancy[depth <= 4 ? 0 : (depth <= 8 ? 1 : 2)];
+    const int occ = ctx->query_occupancy[depth <= 4 ? 0 : (depth <= 8 ? 1 : 2)];
+    const int want = ctx->tuning.query_ctas_per_sm;
+    return want > 0 && want < occ ? want : occ;
+}
+
+// The hand-over of long lines to a warp each, or none (tuning.long_line_bytes < 0).
+gpj::LongLines long_lines(const gpj_ctx* ctx) {
+    if (ctx->tuning.long_line_bytes < 0 || !ctx->d_long) return gpj::LongLines{nullptr, nullptr, 0, 0};
+    return gpj::LongLines{ctx->d_long, ctx->d_long_count, kLongItems, ctx->tuning.long_line_bytes};
 }
 
 // find_value over the file's lines, or (d_range given) over lines
@@ -509,11 +556,14 @@ int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, i
     p.newline_cap = f->nl_cap;
     p.colon = f->colon_valid ? f->d_colon : nullptr;
     p.depth = f->ir_depth;
+    p.long_lines = long_lines(ctx);
+    if (p.long_lines.items)
+        GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_long_count, 0, sizeof(unsigned long long), ctx->stream));
     const int64_t want = d_range ? INT64_MAX : (gpj::query_items(f->num_lines, nq) + 255) / 256;
     const int64_t grid = std::max<int64_t>(
         1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * query_occupancy(ctx, f->ir_depth)));
-    GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->stream));
-    ctx->launches++;
+    GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->sms * 2, ctx->stream));
+    ctx->launches += p.long_lines.items ? 2 : 1;
     return GPJ_OK;
 }
 
@@ -560,7 +610,7 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
     GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
     int64_t lines = 0;
     rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, fq,
-                   queries_done, f->d_colon, &f->colon_valid);
+                   queries_done, f->d_colon, &f->colon_valid, &f->exact_only);
     if (rc) return rc;
     if (lines > f->nl_cap) {  // more lines than the first guess: size exactly and rebuild
         device_free(ctx, f->d_nl);
@@ -568,7 +618,7 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
         rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(lines), "cudaMalloc(newline index)");
         if (rc) return rc;
         rc = run_index(ctx, f->d_data, f->n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, fq,
-                       queries_done, f->d_colon, &f->colon_valid);
+                       queries_done, f->d_colon, &f->colon_valid, &f->exact_only);
         if (rc) return rc;
     }
     rc = end_phase(ctx, fq && fq->nq ? "index_and_query" : "build_index", t0);
@@ -619,7 +669,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
             GPJ_CUDA(ctx, cudaMemcpyAsync(f->d_owned, host, static_cast<size_t>(n), cudaMemcpyHostToDevice,
                                           ctx->stream));
         rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, nullptr,
-                           nullptr, f->d_colon, &f->colon_valid);
+                           nullptr, f->d_colon, &f->colon_valid, &f->exact_only);
         if (rc) return rc;
     } else {
         while (static_cast<int64_t>(ctx->chunk_events.size()) < nchunks) {
@@ -705,7 +755,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) {
             // the whole input is on the device now: index it in one launch (exact fallback inside)
             rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, nullptr,
-                           nullptr, f->d_colon, &f->colon_valid);
+                           nullptr, f->d_colon, &f->colon_valid, &f->exact_only);
             if (rc) return rc;
         } else if ((rc = status_error(ctx, errs))) {
             f->colon_valid = false;
@@ -720,7 +770,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         rc = device_alloc(ctx, &f->d_nl, static_cast<size_t>(lines), "cudaMalloc(newline index)");
         if (rc) return rc;
         rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, nullptr,
-                           nullptr, f->d_colon, &f->colon_valid);
+                           nullptr, f->d_colon, &f->colon_valid, &f->exact_only);
         if (rc) return rc;
     }
     rc = end_phase(ctx, "load_and_index", t0);
@@ -913,6 +963,11 @@ int gpj_create(int device, gpj_ctx** out) {
             return bail(e, "cudaMemPoolSetAttribute");
     }
     if ((e = cudaMalloc(&ctx->d_counter, 16)) != cudaSuccess) return bail(e, "cudaMalloc(counter)");
+    if ((e = cudaMalloc(&ctx->d_long, sizeof(gpj::LongItem) * kLongItems)) != cudaSuccess)
+        return bail(e, "cudaMalloc(long lines)");
+    if ((e = cudaMalloc(&ctx->d_long_count, sizeof(unsigned long long))) != cudaSuccess)
+        return bail(e, "cudaMalloc(long line count)");
+    ctx->tuning = default_tuning();
     if ((e = cudaMalloc(&ctx->d_status, 16)) != cudaSuccess) return bail(e, "cudaMalloc(status)");
     if ((e = cudaMallocHost(&ctx->h_status, 16)) != cudaSuccess) return bail(e, "cudaMallocHost(status)");
     if ((e = cudaEventCreate(&ctx->ev0)) != cudaSuccess) return bail(e, "cudaEventCreate");
@@ -944,6 +999,8 @@ void gpj_destroy(gpj_ctx* ctx) {
         cudaStreamSynchronize(ctx->own_stream);
     }
     if (ctx->d_counter) cudaFree(ctx->d_counter);
+    if (ctx->d_long) cudaFree(ctx->d_long);
+    if (ctx->d_long_count) cudaFree(ctx->d_long_count);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->copy_stream) {
         cudaStreamSynchronize(ctx->copy_stream);
@@ -961,6 +1018,23 @@ void gpj_destroy(gpj_ctx* ctx) {
 }
 
 const char* gpj_last_error(const gpj_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+int gpj_set_tuning(gpj_ctx* ctx, const gpj_tuning* tuning) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (!tuning) return fail(ctx, GPJ_EINVAL, "tuning is null");
+    if (tuning->query_ctas_per_sm < 0 || tuning->index_ctas_per_sm < 0)
+        return fail(ctx, GPJ_EINVAL, "CTAs per SM must be >= 0");
+    ctx->tuning = *tuning;
+    if (ctx->tuning.long_line_bytes == 0) ctx->tuning.long_line_bytes = default_tuning().long_line_bytes;
+    return GPJ_OK;
+}
+
+int gpj_get_tuning(const gpj_ctx* ctx, gpj_tuning* out) {
+    if (!ctx || !out) return GPJ_EINVAL;
+    *out = ctx->tuning;
+    return GPJ_OK;
+}
 
 int gpj_set_query_fusion(gpj_ctx* ctx, int enabled) {
     int rc = check_ctx(ctx);
@@ -1682,7 +1756,7 @@ int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
                 p.batch_files = nb;
                 p.status = ctx->d_status;
                 p.tile_newlines = counts;
-                const int occ = ctx->tile_occupancy[occupancy_slot(levels)];
+                const int occ = tile_ctas_per_sm(ctx, levels);
                 const int64_t grid = std::min<int64_t>(total_tiles, static_cast<int64_t>(ctx->sms) * occ);
                 e = gpj::launch_tile_index_kernel(p, static_cast<int>(grid), ctx->stream);
                 ctx->launches++;
@@ -1851,11 +1925,14 @@ int gpj_batch_run(gpj_batch* b) {
         if (e == cudaSuccess && total_items > 0) {
             int depth = 0;
             for (auto& fr : b->files) depth = std::max(depth, fr.depth);
-            const int64_t grid =
-                std::max<int64_t>(1, std::min<int64_t>((total_items + 255) / 256, static_cast<int64_t>(ctx->sms) * 8));
-            e = gpj::launch_find_value_batch(d_qf, static_cast<int>(qf.size()), total_items, depth,
-                                             static_cast<int>(grid), ctx->stream);
-            ctx->launches++;
+            const int64_t grid = std::max<int64_t>(
+                1, std::min<int64_t>((total_items + 255) / 256, static_cast<int64_t>(ctx->sms) * query_occupancy(ctx, depth)));
+            const gpj::LongLines ll = long_lines(ctx);
+            if (ll.items) e = cudaMemsetAsync(ctx->d_long_count, 0, sizeof(unsigned long long), ctx->stream);
+            if (e == cudaSuccess)
+                e = gpj::launch_find_value_batch(d_qf, static_cast<int>(qf.size()), total_items, depth, ll,
+                                                 static_cast<int>(grid), ctx->sms * 2, ctx->stream);
+            ctx->launches += ll.items ? 2 : 1;
         }
         if (e == cudaSuccess && total_out > b->results_cap) {
             // wait for the copy that may still read the old buffer, then grow (doubling)

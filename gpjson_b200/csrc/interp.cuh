@@ -308,6 +308,26 @@ struct PackedLevels {
     GPJ_HD void set_idx(int k, int64_t v) { index[k * stride] = static_cast<int32_t>(v); }
 };
 
+// How the interpreter scans: one thread alone (SeqScan), or the 32 lanes of
+// a warp together on one line (WarpScan, query_kernel.cu), every lane
+// holding the same interpreter state.
+struct SeqScan {
+    template <typename P>
+    GPJ_HD static P next(const uint64_t* bm, P from, P limit, P& cw, uint64_t& cv) {
+        return next_bit<P>(bm, from, limit, cw, cv);
+    }
+    template <typename P>
+    GPJ_HD static P next_filtered(const uint64_t* bm, const uint64_t* filt, bool invert, P from, P limit, P& cw,
+                                  uint64_t& cv) {
+        return next_bit_filtered<P>(bm, filt, invert, from, limit, cw, cv);
+    }
+    template <typename P>
+    GPJ_HD static P skip(const uint8_t* file, P j, P hi) {
+        return skip_ws<P>(file, j, hi);
+    }
+    GPJ_HD static void store(int64_t* res, int64_t k, int64_t v) { res[k] = v; }
+};
+
 // Runs validated bytecode `ir` on the line [line_start, line_end) and writes
 // (start, end) pairs to res[2*k], res[2*k+1] for the k-th STORE_RESULT.
 // res must hold -1 on entry.  Returns kLineDeferred when the view ends
@@ -315,7 +335,7 @@ struct PackedLevels {
 // reaches `hi` returns).  Positions are of type P and relative to `base`
 // (added to the stored results); `file`, `string_index`, `levels` and
 // `colon` are rebased to match.  `lv` holds the per-level state.
-template <typename P, typename Levels>
+template <typename P, typename Levels, typename Scan = SeqScan>
 GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uint64_t* string_index,
                          const uint64_t* levels, int64_t level_size, const uint64_t* colon, P line_start,
                          P line_end, const uint8_t* ir, int64_t* res, int64_t base, Levels& lv, int& stored) {
@@ -345,11 +365,11 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
                 case 0:  // END
                     return kLineDone;
                 case 1: {  // STORE_RESULT (find_value.cu:59-82)
-                    j = skip_ws<P>(file, j, hi);  // [bounded] stops at end of file
+                    j = Scan::template skip<P>(file, j, hi);  // [bounded] stops at end of file
                     if (j >= hi && skip_end) return kLineDeferred;
                     const P e = lv.end(cur);
-                    res[2 * result_index] = base + j;
-                    res[2 * result_index + 1] = e < 0 ? -1 : base + e;
+                    Scan::store(res, 2 * result_index, base + j);
+                    Scan::store(res, 2 * result_index + 1, e < 0 ? -1 : base + e);
                     stored = ++result_index;
                     break;
                 }
@@ -363,7 +383,9 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
                     ++cur;
                     if (lv.end(cur) == -1) {
                         const P lim = lv.end(cur - 1);
-                        const P m = next_bit<P>(levels + level_size * (cur - 1), j + 1, lim);
+                        P mw = -1;
+                        uint64_t mv = 0;
+                        const P m = Scan::template next<P>(levels + level_size * (cur - 1), j + 1, lim, mw, mv);
                         if (m < lim) lv.set_end(cur, m);
                     }
                     break;
@@ -398,7 +420,7 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
                     want_len = static_cast<P>(read_varint(ir, pc));
                     want = ir + pc;
                     pc += static_cast<int>(want_len);
-                    j = skip_ws<P>(file, j, hi);  // [bounded]
+                    j = Scan::template skip<P>(file, j, hi);  // [bounded]
                     if (j >= hi && skip_end) return kLineDeferred;
                     if (lv.end(cur) - j != want_len) return kLineDone;
                     for (P k = 0; k < want_len; k++)
@@ -456,9 +478,9 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
             const P lim = cend < n ? cend : n;
             if (j < lim) {
                 if (colon)
-                    j = next_bit_filtered<P>(levels + level_size * cur, colon, type != 4, j, lim, cw, cv);
+                    j = Scan::template next_filtered<P>(levels + level_size * cur, colon, type != 4, j, lim, cw, cv);
                 else
-                    j = next_bit<P>(levels + level_size * cur, j, lim, cw, cv);
+                    j = Scan::template next<P>(levels + level_size * cur, j, lim, cw, cv);
                 found = j < lim;
             }
         } else {

@@ -9,6 +9,25 @@
 
 namespace gpj {
 
+// A (line, query) item handed from the thread-per-line kernels to the
+// warp-per-line kernel (line of file `file` of the launch).
+struct LongItem {
+    int64_t line;
+    int32_t file;
+    int32_t query;
+};
+
+// Where the thread-per-line kernels put lines longer than `bytes`, which a
+// whole warp then evaluates (find_value_long): `items` holds `cap` entries,
+// `count` (zeroed before the launch) counts them; items past `cap` are
+// evaluated by their thread.  items == nullptr: no line is handed over.
+struct LongLines {
+    LongItem* items;
+    unsigned long long* count;
+    int64_t cap;
+    int64_t bytes;
+};
+
 struct QueryParams {
     const uint8_t* file;
     int64_t n;
@@ -39,9 +58,12 @@ struct QueryParams {
     // deepest level of the launch's queries (sizes the interpreter's
     // register state)
     int depth;
+    LongLines long_lines;
 };
 
-cudaError_t launch_find_value(const QueryParams& p, int grid, cudaStream_t stream);
+// find_value over the launch's lines, then (when p.long_lines.items is set)
+// the long lines a warp each, with `long_grid` CTAs.
+cudaError_t launch_find_value(const QueryParams& p, int grid, int long_grid, cudaStream_t stream);
 // Resident CTAs per SM of the find_value kernel for queries of that depth.
 int find_value_max_ctas_per_sm(int depth);
 
@@ -73,7 +95,7 @@ struct QueryFile {
 // level of any of their queries), one per thread:
 // a warp's lanes run one query on 32 lines of one file, and the warps of a
 // block of lines run its queries side by side.
-cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_items, int depth, int grid,
-                                    cudaStream_t stream);
+cudaError_t launch_find_value_batch(const QueryFile* files, int nfiles, int64_t total_items, int depth,
+                                    const LongLines& long_lines, int grid, int long_grid, cudaStream_t stream);
 
 }  // namespace gpj

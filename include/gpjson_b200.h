@@ -81,6 +81,25 @@ const char *gpj_last_error(const gpj_ctx *ctx);
  * the legacy default stream (CUDARuntime.java:388). */
 int gpj_set_stream(gpj_ctx *ctx, void *stream);
 
+/* Launch shapes of a context's kernels (no counterpart in the reference,
+ * whose launch shapes are fixed: 8x1024 threads for the index kernels and
+ * 512x1024 for find_value, stages/CombinedIndex.java:28-56,
+ * functions/QueryFunction.java:201-241).  Results do not depend on them.
+ *  - long_line_bytes: find_value evaluates lines longer than this with a
+ *    whole warp each instead of one thread (0 = the default, 65536; -1 = never);
+ *  - query_ctas_per_sm, index_ctas_per_sm: resident CTAs per SM of
+ *    find_value and of the standalone index kernel (0 = the occupancy
+ *    maximum; larger values are capped at it).
+ * gpjson_b200.tune (Python) measures and persists them per device. */
+typedef struct gpj_tuning {
+    int64_t long_line_bytes;
+    int32_t query_ctas_per_sm;
+    int32_t index_ctas_per_sm;
+} gpj_tuning;
+
+int gpj_set_tuning(gpj_ctx *ctx, const gpj_tuning *tuning);
+int gpj_get_tuning(const gpj_ctx *ctx, gpj_tuning *out);
+
 /* How gpj_index_query_device and gpj_query_paths evaluate queries: 0 (the
  * default) builds the index with one kernel and then evaluates all queries
  * with one find_value launch; 1 evaluates them inside the index kernel, on

@@ -57,9 +57,10 @@ def test_batch_matches_single_file_path_and_oracle(gpjson):
         b.run()
         got = [b.result(it) for it in items]
         # a second run reuses the resident indexes: one find_value launch
+        # (and the one for lines handed to a warp each)
         before = gpjson.kernel_launches()
         b.run()
-        assert gpjson.kernel_launches() - before == 1
+        assert gpjson.kernel_launches() - before == (2 if gpjson.tuning()["long_line_bytes"] >= 0 else 1)
         again = [b.result(it) for it in items]
     finally:
         b.release()

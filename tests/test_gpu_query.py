@@ -126,6 +126,65 @@ def test_random_documents_many_paths(gpjson):
     assert np.array_equal(got, want)
 
 
+def random_documents(count: int, seed: int = 11) -> bytes:
+    rng = random.Random(seed)
+    base = [
+        fixture_bytes(SIMPLE),
+        b'{"a": {"b": "a"},"b": {"a": "c" }}',
+        b'{"a":[1,[2,3],{"b":4}],"c":{"d":[]}}',
+        b'{"a" :[ {"b":[0,1,{"c":"x"}]} , 7 ], "d": "\\"a\\":1"}',
+        b'  {"k\\"ey": 1, "key": [ ], "x":{"y":[[],[1]]}}  ',
+        b'{"a":' + b" " * 1500 + b'1, "b": [' + b" " * 700 + b'2]}',
+    ]
+    lines = []
+    for _ in range(count):
+        if rng.random() < 0.9:
+            lines.append(rng.choice(base))
+        else:
+            lines.append(bytes(rng.choice(b'{}[]:,"\\ ab') for _ in range(rng.randint(0, 80))))
+    return b"\n".join(lines)
+
+
+@pytest.mark.gpu
+def test_long_lines_on_a_warp_equal_oracle(gpjson):
+    """Lines longer than the tuning's long_line_bytes are evaluated by a
+    whole warp (the warp-wide bitmap searches and whitespace skips); with
+    the threshold at 64 bytes almost every line takes that path (more than
+    the hand-over list holds, so its overflow is evaluated per thread too),
+    with -1 none does.  Results equal the oracle's either way, for the
+    single-file and the batched launch."""
+    paths = ["$.user.lang", "$.a[1][0]", "$.a[2].b", "$.c.d[0:2]", "$.user.lang[?(@ == 'nl')]", "$.b",
+             "$.x.y[1][0]", "$['k\\\"ey']", "$.d", "$.a[0].b[2].c"]
+    cases = [(random_documents(3000), paths), (adversarial_bytes(24 << 20), ADV_PATHS),
+             (datagen.tweets(4 << 20, seed=datagen.SEED_BASE + 9).tobytes(), TWEET_PATHS)]
+    try:
+        for threshold in (64, -1, 0):
+            gpjson.set_tuning(long_line_bytes=threshold)
+            for data, ps in cases:
+                want = oracle.query(data, ps, mt=True)
+                f = gpjson.load_bytes(data)
+                try:
+                    assert np.array_equal(f.query_paths(ps), want), (threshold, ps)
+                finally:
+                    f.release()
+            b = gpjson.batch()
+            files = [gpjson.load_bytes(data) for data, _ in cases]
+            try:
+                items = [b.add(f, ps) for f, (_, ps) in zip(files, cases)]
+                b.run()
+                for it, (data, ps) in zip(items, cases):
+                    want = oracle.query(data, ps, mt=True)
+                    got = b.result(it)
+                    assert np.array_equal(got[:, :, : want.shape[2]], want), (threshold, "batch", ps)
+            finally:
+                b.release()
+                for f in files:
+                    f.release()
+    finally:
+        gpjson.set_tuning(long_line_bytes=0)
+    assert gpjson.tuning()["long_line_bytes"] == 65536
+
+
 @pytest.mark.gpu
 def test_empty_and_tiny_files(gpjson, tmp_path):
     for data in [b"", b"\n", b"{}", b'{"a":1}\n{"a":2}\n', b"\n\n\n"]:
