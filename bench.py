@@ -86,6 +86,8 @@ def parse_args(argv=None):
                          "queries each, one batch vs per-file calls; serving: 64 resident corpora, Poisson "
                          "requests, continuous batching vs per-request")
     ap.add_argument("--requests", type=int, default=20000, help="serving: number of requests")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default run: skip the adversarial, batched and serving measurements added to its line")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: arrivals per second")
     return ap.parse_args(argv)
 
@@ -285,6 +287,28 @@ def run_ours(args, rank: int, world: int, local: int) -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
     w = ADVERSARIAL if args.workload == "adversarial" else TWEETS
     result = measure_file(args, w, rank, world, local, device)
+    if rank == 0 and world == 1 and w is TWEETS and not args.no_extras and args.bytes is None:
+        # the other configurations on the same GPU in the same run, bounded
+        # so the default run stays within minutes
+        sub = argparse.Namespace(**vars(args))
+        sub.steps, sub.warmup, sub.e2e_steps = min(args.steps, 5), 3, 1
+        sub.cpu_sample = 128 << 20
+        adv = measure_file(sub, ADVERSARIAL, rank, world, local, device)
+        result["adversarial"] = {k: adv[k] for k in ("value", "ms_per_step", "config", "kernels_ms", "roofline",
+                                                     "e2e", "cpu_baseline") if k in adv}
+        sub.steps, sub.warmup = min(args.steps, 3), 1
+        bat = measure_batched(sub)
+        result["batched"] = {k: bat[k] for k in ("metric", "value", "unit", "ms_per_step", "config", "input_gbs",
+                                                 "per_file_calls", "batched_vs_per_file")}
+        sub.requests = min(args.requests, 4000)
+        srv = measure_serving(sub)
+        result["serving"] = {k: srv[k] for k in ("metric", "value", "unit", "config", "latency_ms", "live",
+                                                 "cold_start", "saturated_batched", "saturated_per_request",
+                                                 "batched_vs_per_request_qps")}
+        result["batched_vs_per_file"] = bat["batched_vs_per_file"]
+        result["batched_vs_per_request_qps"] = srv["batched_vs_per_request_qps"]
+        result["served_p50_ms"] = srv["latency_ms"]["p50"]
+        result["served_p99_ms"] = srv["latency_ms"]["p99"]
     if world > 1:
         import torch.distributed as dist
 
@@ -546,6 +570,10 @@ def batched_corpus(seed: int = 0x67706A73 + 3, files: int = 512):
 
 
 def run_batched(args) -> None:
+    print(json.dumps(measure_batched(args)), flush=True)
+
+
+def measure_batched(args) -> dict:
     """Batched workload: every step indexes all 512 files and evaluates their
     queries, once as one gpj_batch_run, once as 512 gpj_query_paths calls."""
     import torch
@@ -622,10 +650,16 @@ def run_batched(args) -> None:
     }
     b.release()
     g.close()
-    print(json.dumps(line), flush=True)
+    del dev
+    torch.cuda.empty_cache()
+    return line
 
 
 def run_serving(args) -> None:
+    print(json.dumps(measure_serving(args)), flush=True)
+
+
+def measure_serving(args) -> dict:
     """Serving workload: 64 corpora of 1 MiB-1 GiB (log-uniform), requests
     arriving Poisson with Zipf(1.1) corpus popularity, a 120 GiB budget;
     continuous batching, then the per-request form on a saturated sample."""
@@ -683,7 +717,7 @@ def run_serving(args) -> None:
         "saturated_per_request": solo,
         "batched_vs_per_request_qps": round(batched["queries_per_s"] / max(solo["queries_per_s"], 1e-9), 2),
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main(argv=None) -> None:

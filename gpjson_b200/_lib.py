@@ -25,6 +25,7 @@ GPJ_EIO = -6
 GPJ_ELIMIT = -7
 GPJ_EDEVICE = -8
 GPJ_ESTATE = -9
+GPJ_EAGAIN = -10
 
 GPJ_MAX_QUERIES = 255
 GPJ_MAX_LEVELS = 16
@@ -34,6 +35,13 @@ class Tuning(ctypes.Structure):
 
     _fields_ = [("long_line_bytes", c_int64), ("query_ctas_per_sm", ctypes.c_int32),
                 ("index_ctas_per_sm", ctypes.c_int32)]
+
+
+class ServerConfig(ctypes.Structure):
+    """gpj_server_config."""
+
+    _fields_ = [("device", ctypes.c_int32), ("num_levels", ctypes.c_int32), ("budget_bytes", c_int64),
+                ("max_batch", ctypes.c_int32), ("workers", ctypes.c_int32)]
 
 
 # name -> (restype, argtypes); the full list of exported entry points.
@@ -84,6 +92,17 @@ SIGNATURES: dict[str, tuple] = {
     "gpj_batch_add": (c_int, [c_void_p, c_void_p, c_int, POINTER(c_char_p), POINTER(c_int)]),
     "gpj_batch_run": (c_int, [c_void_p]),
     "gpj_batch_result": (c_int, [c_void_p, c_int, POINTER(c_void_p)]),
+    "gpj_batch_result_ex": (c_int, [c_void_p, c_int, c_int, POINTER(c_void_p)]),
+    "gpj_serve_create": (c_int, [POINTER(ServerConfig), POINTER(c_void_p)]),
+    "gpj_serve_add_corpus": (c_int, [c_void_p, c_void_p, c_int64, POINTER(c_int)]),
+    "gpj_serve_set_batching": (c_int, [c_void_p, c_int, c_int]),
+    "gpj_serve_submit": (c_int, [c_void_p, c_int, c_int, POINTER(c_char_p), POINTER(c_uint64)]),
+    "gpj_serve_poll": (
+        c_int, [c_void_p, c_uint64, c_int, POINTER(c_void_p), POINTER(c_int64), POINTER(c_int64)]
+    ),
+    "gpj_serve_now_ns": (c_int64, [c_void_p]),
+    "gpj_serve_stats": (c_int, [c_void_p, c_char_p, c_size_t, POINTER(c_size_t)]),
+    "gpj_serve_destroy": (None, [c_void_p]),
     "gpj_batch_size": (c_int, [c_void_p]),
     "gpj_batch_clear": (None, [c_void_p]),
     "gpj_batch_release": (None, [c_void_p]),

@@ -11,6 +11,7 @@
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -38,6 +39,9 @@ struct Phase {
 };
 
 }  // namespace
+
+// Longest run past a tile the batched index launch follows to finish a line.
+static constexpr int64_t kBatchMaxExtension = 8ll << 20;
 
 // Entries of a context's list of long lines handed to a warp each.
 static constexpr int64_t kLongItems = 1 << 16;
@@ -120,17 +124,39 @@ struct gpj_file {
     size_t d_out_cap = 0;  // elements
 };
 
+// The page-locked results of one batch run, shared by the batch and the
+// gpj_result views handed out for it (gpj_batch_result_ex); the last owner
+// frees it.
+struct PinnedResults {
+    int64_t* p = nullptr;
+    size_t cap = 0;  // elements
+    std::atomic<int> refs{1};
+};
+
+static void unref(PinnedResults* r) {
+    if (r && r->refs.fetch_sub(1) == 1) {
+        cudaFreeHost(r->p);
+        delete r;
+    }
+}
+
 struct gpj_result {
     int64_t nq = 0, lines = 0;
     int slots = 0;
-    // [nq][lines][slots][2], every element copied in
+    // [nq][lines][slots][2], copied in, or inside `backing`
     int64_t* offsets = nullptr;
-    size_t cap = 0;  // elements of `offsets`
+    size_t cap = 0;  // elements of `offsets` (when not a view)
+    PinnedResults* backing = nullptr;
 
     gpj_result() = default;
     gpj_result(const gpj_result&) = delete;
     gpj_result& operator=(const gpj_result&) = delete;
-    ~gpj_result() { gpj::result_buffers().give(offsets, cap); }
+    ~gpj_result() {
+        if (backing)
+            unref(backing);
+        else
+            gpj::result_buffers().give(offsets, cap);
+    }
 
     bool allocate(size_t count) {
         offsets = gpj::result_buffers().take(std::max<size_t>(count, 1), &cap);
@@ -166,12 +192,12 @@ struct gpj_batch {
     std::vector<Item> items;
     std::vector<FileRun> files;
     // results of the last run, page-locked (one copy from the device at full
-    // speed), kept and grown across runs
-    int64_t* results = nullptr;
-    size_t results_cap = 0;  // elements
+    // speed); buffers no result refers to any more are used again
+    std::vector<PinnedResults*> pool;
+    PinnedResults* cur = nullptr;
     bool ran = false;
     ~gpj_batch() {
-        if (results) cudaFreeHost(results);
+        for (PinnedResults* r : pool) unref(r);
     }
 };
 
@@ -1704,6 +1730,9 @@ int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
     int64_t total_tiles = 0, total_words = 0;
     int rc = GPJ_OK;
     for (gpj_file* f : need) {
+        // a file of another context may still be in use on that context's
+        // stream: wait for it before its index buffers are reallocated here
+        if (f->ctx != ctx) GPJ_CUDA(ctx, cudaStreamSynchronize(f->ctx->stream));
         if ((rc = ensure_index_buffers(ctx, f, levels))) return rc;
         f->indexed = false;
         f->colon_valid = false;
@@ -1754,6 +1783,10 @@ int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
                 p.tile_end = total_tiles;
                 p.batch = d_tf;
                 p.batch_files = nb;
+                // a file of a batch is small (its long lines cost one CTA
+                // little) and its re-indexing alone would cost a launch
+                // and a wait: lines up to 8 MiB past a tile stay in the launch
+                p.max_extension = kBatchMaxExtension;
                 p.status = ctx->d_status;
                 p.tile_newlines = counts;
                 const int occ = tile_ctas_per_sm(ctx, levels);
@@ -1934,20 +1967,39 @@ int gpj_batch_run(gpj_batch* b) {
                                                  static_cast<int>(grid), ctx->sms * 2, ctx->stream);
             ctx->launches += ll.items ? 2 : 1;
         }
-        if (e == cudaSuccess && total_out > b->results_cap) {
-            // wait for the copy that may still read the old buffer, then grow (doubling)
-            const size_t cap = std::max(total_out, 2 * b->results_cap);
-            e = cudaStreamSynchronize(ctx->stream);
-            if (e == cudaSuccess && b->results) cudaFreeHost(b->results);
-            b->results = nullptr;
-            b->results_cap = 0;
-            if (e == cudaSuccess) {
-                e = cudaMallocHost(&b->results, cap * 8);
-                if (e == cudaSuccess) b->results_cap = cap;
+        // a page-locked buffer no result of an earlier run refers to (every
+        // earlier run's copy has completed: each run ends synchronised)
+        PinnedResults* pick = nullptr;
+        for (PinnedResults* r : b->pool)
+            if (!pick && r->refs.load() == 1 && r->cap >= std::max<size_t>(total_out, 1)) pick = r;
+        if (e == cudaSuccess && !pick) {
+            // drop the idle buffers (too small), then allocate with a quarter to spare
+            std::vector<PinnedResults*> keep;
+            for (PinnedResults* r : b->pool) {
+                if (r->refs.load() == 1)
+                    unref(r);
+                else
+                    keep.push_back(r);
+            }
+            b->pool.swap(keep);
+            PinnedResults* r = new (std::nothrow) PinnedResults;
+            if (!r) {
+                e = cudaErrorMemoryAllocation;
+            } else {
+                const size_t cap = std::max<size_t>(total_out + total_out / 4, 1 << 16);
+                e = cudaMallocHost(&r->p, cap * 8);
+                if (e == cudaSuccess) {
+                    r->cap = cap;
+                    b->pool.push_back(r);
+                    pick = r;
+                } else {
+                    delete r;
+                }
             }
         }
+        if (pick) b->cur = pick;
         if (e == cudaSuccess && total_out > 0)
-            e = cudaMemcpyAsync(b->results, d_out, total_out * 8, cudaMemcpyDeviceToHost, ctx->stream);
+            e = cudaMemcpyAsync(pick->p, d_out, total_out * 8, cudaMemcpyDeviceToHost, ctx->stream);
         if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "batch query");
     }
@@ -1961,25 +2013,42 @@ int gpj_batch_run(gpj_batch* b) {
     return GPJ_OK;
 }
 
-int gpj_batch_result(gpj_batch* b, int item, gpj_result** out) {
+int gpj_batch_result(gpj_batch* b, int item, gpj_result** out) { return gpj_batch_result_ex(b, item, 0, out); }
+
+int gpj_batch_result_ex(gpj_batch* b, int item, int slots, gpj_result** out) {
     if (!b) return GPJ_EINVAL;
     gpj_ctx* ctx = b->ctx;
-    if (!out || item < 0 || item >= static_cast<int>(b->items.size())) return fail(ctx, GPJ_EINVAL, "bad arguments");
+    if (!out || item < 0 || item >= static_cast<int>(b->items.size()) || slots < 0)
+        return fail(ctx, GPJ_EINVAL, "bad arguments");
     if (!b->ran) return fail(ctx, GPJ_ESTATE, "batch has not run since its last change");
     const auto& it = b->items[item];
     const auto& fr = b->files[it.file_slot];
+    if (slots > fr.slots) return fail(ctx, GPJ_EINVAL, "more slots than the batch has for the file");
+    if (slots == 0) slots = fr.slots;
     gpj_result* r = new (std::nothrow) gpj_result;
     if (!r) return fail(ctx, GPJ_ENOMEM, "out of host memory");
     r->nq = static_cast<int64_t>(it.queries.size());
     r->lines = fr.lines;
-    r->slots = fr.slots;
+    r->slots = slots;
     const size_t per_query = static_cast<size_t>(fr.lines) * fr.slots * 2;
-    const int64_t* src = b->results + fr.out_offset + it.q0 * per_query;
-    if (!r->allocate(static_cast<size_t>(r->nq) * per_query)) {
+    int64_t* src = b->cur->p + fr.out_offset + it.q0 * per_query;
+    if (slots == fr.slots) {
+        // a view of the run's page-locked results, kept alive by the view
+        b->cur->refs.fetch_add(1);
+        r->backing = b->cur;
+        r->offsets = src;
+        *out = r;
+        return GPJ_OK;
+    }
+    if (!r->allocate(static_cast<size_t>(r->nq) * fr.lines * slots * 2)) {
         delete r;
         return fail(ctx, GPJ_ENOMEM, "out of host memory for results");
     }
-    std::memcpy(r->offsets, src, static_cast<size_t>(r->nq) * per_query * sizeof(int64_t));
+    {  // each line's first `slots` pairs
+        const size_t lines = static_cast<size_t>(r->nq) * fr.lines;
+        for (size_t l = 0; l < lines; l++)
+            std::memcpy(r->offsets + l * slots * 2, src + l * fr.slots * 2, static_cast<size_t>(slots) * 2 * 8);
+    }
     *out = r;
     return GPJ_OK;
 }

@@ -74,6 +74,9 @@ struct IndexParams {
     // single file (wait timeouts).
     const TileFile* batch;
     int batch_files;
+    // Longest run past its tile a CTA follows to finish a line before it
+    // flags kErrLongLine (0: the kernels' default, 64 KiB).
+    int64_t max_extension;
 
     // Queries evaluated in the same pass (line-parallel kernel only; 0 = none).
     int num_queries;

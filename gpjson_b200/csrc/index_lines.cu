@@ -551,11 +551,11 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, const TileFile
 }
 
 // The long tail of a line that runs past the slot: first '\n' from `from`
-// (warp 0 of the index group); flags lines beyond kMaxExtension.
-__device__ int64_t find_line_end(const TileFile& p, int64_t from, int64_t tile_end) {
+// (warp 0 of the index group); flags lines beyond max_ext past the tile.
+__device__ int64_t find_line_end(const TileFile& p, int64_t from, int64_t tile_end, int64_t max_ext) {
     const int lane = threadIdx.x & 31;
     int64_t found = kNone;
-    int64_t limit = p.n - tile_end > kMaxExtension ? tile_end + kMaxExtension : p.n;
+    int64_t limit = p.n - tile_end > max_ext ? tile_end + max_ext : p.n;
     if (limit > p.avail) limit = p.avail;
     for (int64_t base = from; base < limit && found == kNone; base += 512) {
         const int64_t q = base + 16 * lane;
@@ -777,7 +777,8 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                 const int64_t d_in = sc.d_end;
                 const int esc_in = sh.carry_esc;
                 if (tid < 32) {
-                    const int64_t e2 = find_line_end(F, loaded_end, tile_end);
+                    const int64_t e2 =
+                        find_line_end(F, loaded_end, tile_end, p.max_extension > 0 ? p.max_extension : kMaxExtension);
                     if (tid == 0) sh.long_b = e2;
                 }
                 group_sync(kBarIndex, kIndexThreads);
@@ -1108,7 +1109,8 @@ __device__ void extend_long_line(const IndexParams& p, const TileFile& F, WShare
                                  int64_t tile_end, int s_in, int64_t d_in) {
     const int tid = threadIdx.x;
     if (tid < 32) {
-        const int64_t e2 = find_line_end(F, loaded_end, tile_end);
+        const int64_t e2 =
+            find_line_end(F, loaded_end, tile_end, p.max_extension > 0 ? p.max_extension : kMaxExtension);
         if (tid == 0) {
             sh.long_b = e2;
             // the escape state at loaded_end: the backslash run before it

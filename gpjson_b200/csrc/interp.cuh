@@ -41,7 +41,9 @@ struct LineView {
     const uint64_t* colon;
 };
 
-enum LineStatus : int { kLineDone = 0, kLineDeferred = 1 };
+// kLineLong: run_line gave up on a whitespace skip longer than its skip
+// bound (the caller evaluates the line again another way).
+enum LineStatus : int { kLineDone = 0, kLineDeferred = 1, kLineLong = 2 };
 
 GPJ_HD bool is_ws(uint8_t c) { return c == '\n' || c == '\r' || c == '\t' || c == ' '; }
 
@@ -399,13 +401,9 @@ GPJ_HD int run_line_core(const uint8_t* file, P n, P hi, int skip_end, const uin
                 case 5:  // MOVE_TO_INDEX (:131-169)
                     want_index = read_varint(ir, pc);
                     if (lv.idx(cur) == -1) {
-                        for (;;) {  // [bounded] only whitespace may precede '['
-                            if (j >= hi) return skip_end;
-                            const uint8_t c = file[j];
-                            if (c == '[') break;
-                            if (!is_ws(c)) return kLineDone;
-                            ++j;
-                        }
+                        j = Scan::template skip<P>(file, j, hi);  // [bounded] only whitespace may precede '['
+                        if (j >= hi) return skip_end;
+                        if (file[j] != '[') return kLineDone;
                         lv.set_idx(cur, 0);
                     }
                     if (want_index == 0) {
@@ -532,15 +530,20 @@ int run_line_wide(const LineView& v, int64_t line_start, int64_t line_end, const
 // initialised).  Lines whose end lies more than rel_limit (<= kRelLimit)
 // bytes past that word run in 64 bits; a whitespace skip that reaches
 // rel_limit (bytes past it exist) stops there and the line is evaluated
-// again in 64 bits.
+// again in 64 bits.  With a skip_bound, a whitespace skip that runs more
+// than skip_bound bytes past the line's end (into the blank lines after it)
+// stops there too and run_line returns kLineLong, with res partly written,
+// for the caller to evaluate the line again (a warp each, query_kernel.cu).
 template <int D = kLevelSlots>
 GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir, int64_t* res,
-                    int64_t res_len, int64_t rel_limit = kRelLimit) {
+                    int64_t res_len, int64_t rel_limit = kRelLimit, int64_t skip_bound = -1) {
     const int64_t base = line_start & ~static_cast<int64_t>(63);
     int stored = 0;
     if (line_end - base <= rel_limit) {
-        const bool clamped = v.hi - base > rel_limit;
-        const int32_t hi = static_cast<int32_t>(clamped ? rel_limit : v.hi - base);
+        const int64_t lim =
+            skip_bound >= 0 && line_end - base + skip_bound < rel_limit ? line_end - base + skip_bound : rel_limit;
+        const bool clamped = v.hi - base > lim;
+        const int32_t hi = static_cast<int32_t>(clamped ? lim : v.hi - base);
         const int32_t n = static_cast<int32_t>(v.n - base > rel_limit ? rel_limit : v.n - base);
         const int skip_end = clamped || v.hi < v.n ? kLineDeferred : kLineDone;
         const int64_t w = base >> 6;
@@ -553,6 +556,7 @@ GPJ_HD int run_line(const LineView& v, int64_t line_start, int64_t line_end, con
             for (int64_t k = 2 * static_cast<int64_t>(stored); k < res_len; k++) res[k] = -1;
             return r;
         }
+        if (skip_bound >= 0) return kLineLong;
     }
     return run_line_wide(v, line_start, line_end, ir, res, res_len);
 }
@@ -576,14 +580,14 @@ GPJ_HD int bytecode_depth(const uint8_t* ir) {
 // run_line with the register state sized for queries no deeper than `depth`
 // (the sizes the kernels are instantiated for).
 GPJ_HD int run_line_depth(int depth, const LineView& v, int64_t line_start, int64_t line_end, const uint8_t* ir,
-                          int64_t* res, int64_t res_len, int64_t rel_limit = kRelLimit) {
+                          int64_t* res, int64_t res_len, int64_t rel_limit = kRelLimit, int64_t skip_bound = -1) {
     switch (level_slots_for_depth(depth)) {
         case 5:
-            return run_line<5>(v, line_start, line_end, ir, res, res_len, rel_limit);
+            return run_line<5>(v, line_start, line_end, ir, res, res_len, rel_limit, skip_bound);
         case 9:
-            return run_line<9>(v, line_start, line_end, ir, res, res_len, rel_limit);
+            return run_line<9>(v, line_start, line_end, ir, res, res_len, rel_limit, skip_bound);
         default:
-            return run_line<kLevelSlots>(v, line_start, line_end, ir, res, res_len, rel_limit);
+            return run_line<kLevelSlots>(v, line_start, line_end, ir, res, res_len, rel_limit, skip_bound);
     }
 }
 

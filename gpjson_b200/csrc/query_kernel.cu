@@ -154,7 +154,13 @@ __global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
         const int64_t end = to_eof ? p.n : p.newlines[i + 1];
         if (p.long_lines.items && end - start > p.long_lines.bytes && hand_over(p.long_lines, i, 0, q)) continue;
         int64_t* res = p.out + (static_cast<int64_t>(q) * p.out_lines + i) * per_line;
-        run_line<D>(view, start, end, p.bytecode + p.offsets[q], res, per_line);  // writes every slot once
+        const uint8_t* ir = p.bytecode + p.offsets[q];
+        // writes every slot once, unless a whitespace skip runs far past the
+        // line (then a warp evaluates it again)
+        if (run_line<D>(view, start, end, ir, res, per_line, kRelLimit,
+                        p.long_lines.items ? p.long_lines.bytes : -1) == kLineLong &&
+            !hand_over(p.long_lines, i, 0, q))
+            run_line_wide(view, start, end, ir, res, per_line);
     }
 }
 
@@ -201,7 +207,11 @@ __global__ void __launch_bounds__(256) find_value_batch_kernel(const QueryFile* 
         if (long_lines.items && end - start > long_lines.bytes && hand_over(long_lines, i, lo, q)) continue;
         const int64_t per_line = 2 * static_cast<int64_t>(F.slots);
         int64_t* res = F.out + (q * F.out_lines + i) * per_line;
-        run_line<D>(view, start, end, F.bytecode + F.offsets[q], res, per_line);
+        const uint8_t* ir = F.bytecode + F.offsets[q];
+        if (run_line<D>(view, start, end, ir, res, per_line, kRelLimit, long_lines.items ? long_lines.bytes : -1) ==
+                kLineLong &&
+            !hand_over(long_lines, i, lo, q))
+            run_line_wide(view, start, end, ir, res, per_line);
     }
 }
 

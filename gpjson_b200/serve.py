@@ -1,18 +1,16 @@
-"""Serving loop: (corpus, JSONPath) requests against resident corpora.
+"""Serving: (corpus, JSONPath) requests against resident corpora, over the
+native request server (gpj_serve_*, include/gpjson_b200.h).
 
-Each corpus is loaded once (pipelined host copy + index build,
-gpj_file_from_host_indexed) and kept in device memory with its structural
-index under a byte budget; when a new corpus does not fit, the least
-recently used ones not needed by the current requests are released.  Loads
-run on a context of their own in a loader thread, so they overlap the
-queries running on the serving context.
-
-Continuous batching: every iteration takes all requests that have arrived
-and whose corpus is resident and evaluates them in one gpj_batch_run (one
-find_value launch over every line of every corpus involved, one copy of the
-results); requests arriving meanwhile, or waiting for their corpus to load,
-join a later iteration.  The per-request form (one request per run) is the
-baseline the batched form is measured against.
+The server keeps corpora resident in device memory with their structural
+indexes under a byte budget (least recently used out, an evicted corpus's
+bytes counting until its memory is released), loads cold ones from
+page-locked host memory on a loader thread, and batches continuously:
+each of its serving threads takes every arrived request whose corpus is
+resident and evaluates them in one batch on its own stream, so iterations
+overlap on the device.  This module paces requests by their arrival times,
+collects the results and computes latency statistics.  The per-request form
+(one request at a time) is the baseline the batched form is measured
+against.
 
 The reference has no serving mode; its query() reads, indexes and queries
 the file on every call (functions/QueryFunction.java:48-265).
@@ -20,16 +18,16 @@ the file on every call (functions/QueryFunction.java:48-265).
 
 from __future__ import annotations
 
-import collections
-import queue
+import ctypes
+import json
 import statistics
-import threading
 import time
+from ctypes import byref, c_char_p, c_int, c_int64, c_size_t, c_uint64, c_void_p
 from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import GPJSON, File
+from . import _lib, _result_array
 
 # 32 paths of depth 1-6 over the two synthetic schemas (tweet-like objects;
 # the adversarial generator's a/b/c/d chains, arrays and x/y/z nesting),
@@ -98,151 +96,118 @@ class ServeStats:
         }
 
 
+class ServerError(RuntimeError):
+    def __init__(self, message: str, code: int):
+        super().__init__(message)
+        self.code = code
+
+
 class Server:
-    """Resident corpora under `budget_bytes` and a continuous-batching loop."""
+    """Resident corpora under `budget_bytes` and continuous batching, on the
+    native server (`workers` serving threads, each its own stream)."""
 
     def __init__(self, corpora: dict[str, np.ndarray], budget_bytes: int, device: int = 0,
-                 levels: int = POOL_LEVELS, max_batch: int = 512):
-        self.corpora = corpora
-        self.budget = budget_bytes
-        self.levels = levels
+                 levels: int = POOL_LEVELS, max_batch: int = 512, workers: int = 2):
+        self.lib = _lib.load()
         self.max_batch = max_batch
-        self.gpj = GPJSON(device)          # batches (this thread)
-        self._load_gpj = GPJSON(device)    # loads and releases (loader thread)
-        self.resident: collections.OrderedDict[str, File] = collections.OrderedDict()
-        self.loading: set[str] = set()
-        self.used = 0
-        self.loads = 0
-        self.evictions = 0
-        self._cv = threading.Condition()
-        self._jobs: queue.Queue = queue.Queue()
-        self._error: BaseException | None = None
-        self._loader = threading.Thread(target=self._loader_loop, name="gpjson-loader", daemon=True)
-        self._loader.start()
-        # one batch for the server's life: its page-locked result buffer is
-        # allocated once and reused by every iteration
-        self._batch = self.gpj.batch()
+        self.workers = workers
+        cfg = _lib.ServerConfig(device, levels, int(budget_bytes), max_batch, workers)
+        self._h = c_void_p()
+        self._check(self.lib.gpj_serve_create(byref(cfg), byref(self._h)), "gpj_serve_create")
+        self._arrays = {}
+        self._ids: dict[str, int] = {}
+        for name, arr in corpora.items():
+            a = np.ascontiguousarray(arr, dtype=np.uint8)
+            cid = c_int()
+            self._check(self.lib.gpj_serve_add_corpus(self._h, a.ctypes.data, a.size, byref(cid)),
+                        f"gpj_serve_add_corpus({name})")
+            self._arrays[name] = a  # must outlive the server
+            self._ids[name] = cid.value
 
-    # -- loader thread -------------------------------------------------------
-    def _loader_loop(self) -> None:
-        while True:
-            job = self._jobs.get()
-            if job is None:
-                return
-            kind, name, f = job
-            try:
-                if kind == "release":
-                    f.release()
-                    continue
-                f = self._load_gpj.load_bytes_indexed(self.corpora[name], self.levels)
-                with self._cv:
-                    self.resident[name] = f
-                    self.loading.discard(name)
-                    self.loads += 1
-                    self._cv.notify_all()
-            except BaseException as e:  # surfaced by serve()
-                with self._cv:
-                    self._error = e
-                    self.loading.discard(name)
-                    self._cv.notify_all()
+    @staticmethod
+    def _check(rc: int, what: str) -> None:
+        if rc != _lib.GPJ_OK:
+            raise ServerError(f"{what} failed ({rc})", rc)
 
-    # -- admission ------------------------------------------------------------
-    def _admit(self, name: str, needed: set[str]) -> bool:
-        """True when `name` is resident; otherwise starts its load (after
-        evicting least recently used corpora not in `needed`)."""
-        with self._cv:
-            if name in self.resident:
-                self.resident.move_to_end(name)
-                return True
-            if name in self.loading:
-                return False
-            cost = resident_bytes(self.corpora[name].size, self.levels)
-            while self.used + cost > self.budget:
-                victim = next((v for v in self.resident if v not in needed), None)
-                if victim is None:
-                    if not self.resident and not self.loading:
-                        raise MemoryError(f"corpus {name} ({cost} B resident) exceeds the {self.budget} B budget")
-                    return False  # wait for room
-                f = self.resident.pop(victim)
-                self.used -= resident_bytes(self.corpora[victim].size, self.levels)
-                self.evictions += 1
-                self._jobs.put(("release", victim, f))
-            self.used += cost
-            self.loading.add(name)
-        self._jobs.put(("load", name, None))
-        return False
+    def stats(self) -> dict:
+        n = c_size_t()
+        self.lib.gpj_serve_stats(self._h, None, 0, byref(n))
+        buf = ctypes.create_string_buffer(n.value + 1)
+        self._check(self.lib.gpj_serve_stats(self._h, buf, n.value + 1, byref(n)), "gpj_serve_stats")
+        return json.loads(buf.value.decode())
 
-    def preload(self, names) -> None:
-        for name in names:
-            self._admit(name, set(names))
-        with self._cv:
-            while any(n in self.loading for n in names):
-                if self._error:
-                    raise self._error
-                self._cv.wait(0.05)
-
-    # -- serving -------------------------------------------------------------
     def serve(self, requests: list[Request], per_request: bool = False, keep_results: bool = False) -> ServeStats:
-        """Runs `requests` (ascending arrival) in real time; per_request=True
-        runs each request alone (the baseline form)."""
+        """Submits `requests` at their arrival times (seconds from now) and
+        waits for all; per_request=True runs one request at a time (the
+        baseline form).  Latency = completion - arrival."""
+        lib = self.lib
         reqs = sorted(requests, key=lambda r: r.arrival)
-        batch = self._batch
-        pending: collections.deque[Request] = collections.deque()
-        nxt, finished, batches = 0, 0, 0
+        if per_request:
+            self._check(lib.gpj_serve_set_batching(self._h, 1, 1), "gpj_serve_set_batching")
+        else:
+            self._check(lib.gpj_serve_set_batching(self._h, self.max_batch, self.workers), "gpj_serve_set_batching")
+        before = self.stats()
+        ids: list[int] = []
+        t0_ns = lib.gpj_serve_now_ns(self._h)
         t0 = time.perf_counter()
-        try:
-            while finished < len(reqs):
-                if self._error:
-                    raise self._error
-                now = time.perf_counter() - t0
-                while nxt < len(reqs) and reqs[nxt].arrival <= now:
-                    pending.append(reqs[nxt])
-                    nxt += 1
-                needed = {r.corpus for r in pending}
-                ready = [r for r in pending if self._admit(r.corpus, needed)]
-                if not ready:
-                    wait = reqs[nxt].arrival - now if nxt < len(reqs) else 0.05
-                    with self._cv:
-                        self._cv.wait(max(0.0, min(wait, 0.05)))
+        collected = 0
+
+        def collect(timeout_ms: int) -> bool:
+            """Takes the oldest outstanding request's result if it is done
+            (results are handed back as they finish, so their memory is
+            released early)."""
+            nonlocal collected
+            r, rid = reqs[collected], ids[collected]
+            res, sub, done = c_void_p(), c_int64(), c_int64()
+            rc = lib.gpj_serve_poll(self._h, rid, timeout_ms, byref(res), byref(sub), byref(done))
+            if rc == _lib.GPJ_EAGAIN:
+                return False
+            if rc != _lib.GPJ_OK:
+                if res.value:
+                    lib.gpj_result_release(res)
+                raise ServerError(f"request for {r.corpus} {r.paths} failed ({rc})", rc)
+            r.done = (done.value - t0_ns) / 1e9
+            if keep_results:
+                r.result = _result_array(lib, res)
+            else:
+                lib.gpj_result_release(res)
+            collected += 1
+            return True
+
+        for r in reqs:
+            while True:
+                wait = r.arrival - (time.perf_counter() - t0)
+                if wait <= 0:
+                    break
+                if collected < len(ids) and collect(0):
                     continue
-                take = ready[:1] if per_request else ready[: self.max_batch]
-                batch.clear()
-                items = []
-                for r in take:
-                    with self._cv:
-                        f = self.resident[r.corpus]
-                    items.append(batch.add(f, r.paths))
-                batch.run()
-                batches += 1
-                done = time.perf_counter() - t0
-                taken = set(map(id, take))
-                for r, it in zip(take, items):
-                    r.done = done
-                    if keep_results:
-                        r.result = batch.result(it)
-                pending = collections.deque(r for r in pending if id(r) not in taken)
-                finished += len(take)
-        finally:
-            batch.clear()
+                time.sleep(min(wait, 0.0005))
+            arr = (c_char_p * len(r.paths))(*[p.encode("utf-8") for p in r.paths])
+            rid = c_uint64()
+            self._check(lib.gpj_serve_submit(self._h, self._ids[r.corpus], len(r.paths), arr, byref(rid)),
+                        "gpj_serve_submit")
+            ids.append(rid.value)
+        while collected < len(ids):
+            collect(-1)
+        after = self.stats()
         last = max(r.done for r in reqs) if reqs else 0.0
         first = min(r.arrival for r in reqs) if reqs else 0.0
         return ServeStats(
             requests=len(reqs), seconds=last - first,
             latencies_ms=[1000.0 * (r.done - r.arrival) for r in reqs],
-            batches=batches, loads=self.loads, evictions=self.evictions,
+            batches=after["batches"] - before["batches"], loads=after["loads"], evictions=after["evictions"],
         )
 
     def close(self) -> None:
-        with self._cv:
-            files = list(self.resident.values())
-            self.resident.clear()
-        for f in files:
-            self._jobs.put(("release", "", f))
-        self._jobs.put(None)
-        self._loader.join(timeout=60)
-        self._batch.release()
-        self.gpj.close()
-        self._load_gpj.close()
+        if self._h:
+            self.lib.gpj_serve_destroy(self._h)
+            self._h = c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def poisson_requests(corpora: list[str], count: int, rate: float, zipf_s: float = 1.1, paths_per_request: int = 1,

@@ -53,6 +53,7 @@ extern "C" {
 #define GPJ_ELIMIT (-7)       /* a documented limit was exceeded */
 #define GPJ_EDEVICE (-8)      /* a kernel reported an error word (bounded wait expired) */
 #define GPJ_ESTATE (-9)       /* object not in the state the call needs */
+#define GPJ_EAGAIN (-10)      /* not finished yet (gpj_serve_poll) */
 
 /* Limits kept from the reference. */
 #define GPJ_MAX_QUERIES 255   /* QueryFunction.java:74-77 */
@@ -361,10 +362,75 @@ int gpj_batch_run(gpj_batch *batch);
  * in the order added; slots = the largest num_results among the queries of
  * the request's file in this batch). */
 int gpj_batch_result(gpj_batch *batch, int item, gpj_result **out);
+/* The same with `slots` result slots per line (0: as gpj_batch_result):
+ * each line's first `slots` slots, which hold every result of the request's
+ * own queries when slots >= their largest num_results (GPJ_EINVAL when
+ * slots exceeds the batch's slots for that file). */
+int gpj_batch_result_ex(gpj_batch *batch, int item, int slots, gpj_result **out);
 int gpj_batch_size(const gpj_batch *batch);
 /* Removes all requests (the batch can be filled and run again). */
 void gpj_batch_clear(gpj_batch *batch);
 void gpj_batch_release(gpj_batch *batch);
+
+/* ---- serving ----------------------------------------------------------------- */
+
+/* A request server: (corpus, paths) requests against corpora kept resident
+ * in device memory with their structural indexes under a byte budget, with
+ * no counterpart in the reference (whose query() reads, indexes and queries
+ * the file on every call, QueryFunction.java:48-265; a server would call the
+ * interop object of GPJSONLibrary.java:48-54 once per request).
+ *  - `workers` serving threads, each with its own context and stream: a
+ *    free worker takes every pending request whose corpus is resident (up to
+ *    max_batch, in arrival order) and evaluates them as one batch
+ *    (gpj_batch_run); requests arriving meanwhile are taken by the next free
+ *    worker, so iterations overlap on the device (continuous batching).
+ *  - one loader thread: a corpus is loaded (copy from page-locked host
+ *    memory pipelined with its index build) when a request needs it and its
+ *    resident bytes fit the budget; least recently used corpora that no
+ *    pending or running request needs are evicted, their bytes counting
+ *    against the budget until their memory is released.
+ * Every function is thread-safe.  A request's result equals gpj_query_paths
+ * on its corpus alone (gpj_result layout; slots = the largest num_results of
+ * its own paths). */
+typedef struct gpj_server gpj_server;
+typedef struct gpj_server_config {
+    int32_t device;
+    int32_t num_levels;    /* every corpus is indexed with this many levels (1..16); deeper paths are refused */
+    int64_t budget_bytes;  /* device bytes for resident corpora with their indexes */
+    int32_t max_batch;     /* requests per iteration (>= 1) */
+    int32_t workers;       /* serving threads, iterations on the device at once (1..8) */
+} gpj_server_config;
+
+int gpj_serve_create(const gpj_server_config *cfg, gpj_server **out);
+/* Registers n bytes of NDJSON in host memory as a corpus (*corpus = its
+ * number).  The memory must stay valid and unchanged until
+ * gpj_serve_destroy; it is page-locked here (cudaHostRegister) unless it
+ * already is.  Nothing is loaded before a request needs it.  GPJ_ELIMIT when
+ * its resident bytes exceed the budget. */
+int gpj_serve_add_corpus(gpj_server *s, const void *host, int64_t n, int *corpus);
+/* Requests per iteration and iterations at once from now on (max_inflight
+ * is capped at the server's workers; 1, 1 = one request at a time). */
+int gpj_serve_set_batching(gpj_server *s, int max_batch, int max_inflight);
+/* Queues a request and returns at once; *request receives its id.  Paths
+ * are compiled here: GPJ_EPARSE / GPJ_EUNSUPPORTED as gpj_compile,
+ * GPJ_ELIMIT for a path deeper than the server's num_levels. */
+int gpj_serve_submit(gpj_server *s, int corpus, int nq, const char *const *paths, uint64_t *request);
+/* Waits up to timeout_ms (0: do not wait, -1: no limit) for request
+ * `request`.  When it has finished, hands over its result (*out, released
+ * with gpj_result_release) with its submit and completion times (ns since
+ * the server's creation, optional) and returns its status; GPJ_EAGAIN while
+ * it is not finished (call again). */
+int gpj_serve_poll(gpj_server *s, uint64_t request, int timeout_ms, gpj_result **out, int64_t *submit_ns,
+                   int64_t *done_ns);
+/* The server's clock (ns since creation), as used by gpj_serve_poll. */
+int64_t gpj_serve_now_ns(const gpj_server *s);
+/* Counters as JSON (served, batches, loads, evictions, resident corpora,
+ * budget bytes in use); writes at most cap bytes including the NUL, *len
+ * receives the full length. */
+int gpj_serve_stats(gpj_server *s, char *json, size_t cap, size_t *len);
+/* Stops the threads, releases the resident corpora and unregisters the host
+ * memory; requests not handed back are dropped. */
+void gpj_serve_destroy(gpj_server *s);
 
 /* ---- diagnostics ---------------------------------------------------------- */
 

@@ -192,7 +192,8 @@ int64_t hs_build_index_lines(const uint8_t* f, int64_t n, int num_levels, uint64
 // jump along; `packed` = 1 selects the 32-bit level state the fused kernel
 // keeps in shared memory, 2 the line-relative 32-bit interpreter with a
 // 64-byte limit (so that its 64-bit fallbacks run), 3 the register state of
-// the deepest size (0 sizes it by the query's depth, as the kernels do).
+// the deepest size (0 sizes it by the query's depth, as the kernels do),
+// 4 that with a whitespace-skip bound (the kernels' hand-over of long skips).
 // Slots the interpreter does not reach are written -1 by it (run_line) or
 // were -1 before (PackedLevels).
 void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t lines,
@@ -213,6 +214,14 @@ void hs_find_values(const uint8_t* f, int64_t n, const int64_t* nl, int64_t line
             } else if (packed == 0) {
                 for (int k = 0; k < slots * 2; k++) res[k] = 7;  // written again by run_line
                 run_line_depth(bytecode_depth(irs[q]), v, start, end, irs[q], res, slots * 2);
+            } else if (packed == 4) {
+                // a skip bound of 16 bytes past the line: lines that skip further
+                // are evaluated again by the 64-bit interpreter, as the kernels
+                // hand them to a warp
+                for (int k = 0; k < slots * 2; k++) res[k] = 7;
+                if (run_line_depth(bytecode_depth(irs[q]), v, start, end, irs[q], res, slots * 2, kRelLimit, 16) ==
+                    kLineLong)
+                    run_line_wide(v, start, end, irs[q], res, slots * 2);
             } else {
                 for (int k = 0; k < slots * 2; k++) res[k] = 7;
                 run_line<kLevelSlots>(v, start, end, irs[q], res, slots * 2, packed == 2 ? 64 : kRelLimit);

@@ -263,3 +263,18 @@ def test_values_arrays_are_views_that_own_the_native_values():
     del kept
     gc.collect()
     assert released == [0x77]
+
+
+def test_server_rejects_bad_configuration_without_gpu():
+    """gpj_serve_create checks its configuration before any device work."""
+    from ctypes import byref, c_void_p
+
+    lib = _lib.load()
+    h = c_void_p()
+    for cfg in [(0, 0, 1 << 20, 1, 1), (0, 17, 1 << 20, 1, 1), (0, 4, 0, 1, 1), (0, 4, 1 << 20, 0, 1),
+                (0, 4, 1 << 20, 1, 0), (0, 4, 1 << 20, 1, 9)]:
+        assert lib.gpj_serve_create(byref(_lib.ServerConfig(*cfg)), byref(h)) == _lib.GPJ_EINVAL, cfg
+    assert lib.gpj_serve_create(None, byref(h)) == _lib.GPJ_EINVAL
+    assert lib.gpj_serve_poll(None, 1, 0, byref(c_void_p()), None, None) == _lib.GPJ_EINVAL
+    assert lib.gpj_serve_now_ns(None) == -1
+    lib.gpj_serve_destroy(None)

@@ -58,3 +58,68 @@ def test_serving_mix_equals_alone_and_oracle():
     assert s["loads"] >= len(names) and s["evictions"] > 0
     assert 0 <= s["p50_ms"] <= s["p99_ms"]
     assert solo.summary()["batches"] == 40
+
+
+@pytest.mark.gpu
+def test_server_through_the_c_abi_from_two_threads():
+    """gpj_serve_* called directly: two client threads submit requests for
+    two corpora at once, each result (gpj_result, its own slots) equals the
+    oracle's; a path deeper than the server's levels and a bad corpus are
+    refused; GPJ_EAGAIN until a request is done."""
+    import ctypes
+    import threading
+    from ctypes import byref, c_char_p, c_int, c_int64, c_uint64, c_void_p
+
+    from gpjson_b200 import _lib, _result_array
+
+    lib = _lib.load()
+    data = {"t": datagen.tweets(2 << 20, seed=datagen.SEED_BASE + 60),
+            "a": datagen.adversarial(3 << 20, seed=datagen.SEED_BASE + 61)}
+    cfg = _lib.ServerConfig(0, 5, 1 << 30, 64, 2)
+    h = c_void_p()
+    assert lib.gpj_serve_create(byref(cfg), byref(h)) == _lib.GPJ_OK
+    try:
+        ids = {}
+        for name, arr in data.items():
+            cid = c_int()
+            assert lib.gpj_serve_add_corpus(h, arr.ctypes.data, arr.size, byref(cid)) == _lib.GPJ_OK
+            ids[name] = cid.value
+        jobs = [("t", ["$.user.lang", "$.entities.hashtags[0:2]"]), ("a", ["$.arr[5]"]), ("t", ["$.id"]),
+                ("a", ["$.a.b.c.d", "$.x[0].y[2].z"])] * 6
+        out = [None] * len(jobs)
+
+        def client(k0):
+            for k in range(k0, len(jobs), 2):
+                name, paths = jobs[k]
+                arr = (c_char_p * len(paths))(*[p.encode() for p in paths])
+                rid = c_uint64()
+                assert lib.gpj_serve_submit(h, ids[name], len(paths), arr, byref(rid)) == _lib.GPJ_OK
+                res, sub, done = c_void_p(), c_int64(), c_int64()
+                rc = lib.gpj_serve_poll(h, rid, 0, byref(res), byref(sub), byref(done))
+                while rc == _lib.GPJ_EAGAIN:
+                    rc = lib.gpj_serve_poll(h, rid, 50, byref(res), byref(sub), byref(done))
+                assert rc == _lib.GPJ_OK
+                assert 0 <= sub.value <= done.value
+                out[k] = _result_array(lib, res)
+
+        threads = [threading.Thread(target=client, args=(i,)) for i in range(2)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        for (name, paths), got in zip(jobs, out):
+            want = oracle.query(data[name].tobytes(), paths)
+            assert np.array_equal(got, want), (name, paths)
+        deep = (c_char_p * 1)(b"$.a.b.c.d.e.f")
+        rid = c_uint64()
+        assert lib.gpj_serve_submit(h, ids["a"], 1, deep, byref(rid)) == _lib.GPJ_ELIMIT
+        assert lib.gpj_serve_submit(h, 99, 1, deep, byref(rid)) in (_lib.GPJ_EINVAL, _lib.GPJ_ELIMIT)
+        n = ctypes.c_size_t()
+        buf = ctypes.create_string_buffer(4096)
+        assert lib.gpj_serve_stats(h, buf, 4096, byref(n)) == _lib.GPJ_OK
+        import json
+
+        st = json.loads(buf.value.decode())
+        assert st["served"] == len(jobs) and st["loads"] == 2 and st["batches"] <= len(jobs)
+    finally:
+        lib.gpj_serve_destroy(h)

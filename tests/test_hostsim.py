@@ -158,7 +158,7 @@ def test_interpreter_matches_oracle(hostsim):
             # plain, with the fused kernel's colon jumps, with its packed level
             # state, and with the 32-bit interpreter's 64-bit fallbacks forced
             for colon_ptr, packed in ((None, 0), (colon.ctypes.data, 0), (colon.ctypes.data, 1), (None, 2),
-                                      (colon.ctypes.data, 3)):
+                                      (colon.ctypes.data, 3), (colon.ctypes.data, 4)):
                 got = np.empty_like(want)
                 hostsim.hs_find_values(f.ctypes.data, f.size, idx.newlines.ctypes.data, len(idx.newlines),
                                        idx.strings.ctypes.data, idx.levels.ctypes.data, 1, ptrs, slots,
