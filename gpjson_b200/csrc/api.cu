@@ -196,8 +196,32 @@ struct gpj_batch {
     std::vector<PinnedResults*> pool;
     PinnedResults* cur = nullptr;
     bool ran = false;
+    // The query phase of the last run as a CUDA graph (find_value over every
+    // item, the long-line warps, the copy of the results), replayed by the
+    // next run when neither the requests nor the files' indexes nor the
+    // launch shapes changed and no result of the last run is still held.
+    struct Replay {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<uint64_t> sig;  // what the graph reads (files' buffers, line counts, tuning)
+        uint8_t* d_blob = nullptr;  // kept while the graph lives
+        int64_t* d_out = nullptr;
+        gpj::QueryFile* d_qf = nullptr;
+        PinnedResults* dst = nullptr;  // the copy's destination
+        cudaStream_t stream = nullptr;
+    } replay;
+    bool dirty = true;  // requests added or cleared since the graph was made
+    int64_t replays = 0;
     ~gpj_batch() {
+        drop_replay();
         for (PinnedResults* r : pool) unref(r);
+    }
+    void drop_replay() {
+        if (replay.exec) cudaGraphExecDestroy(replay.exec);
+        // pool allocations of the batch's context, freed in its stream order
+        if (replay.d_blob) cudaFreeAsync(replay.d_blob, replay.stream);
+        if (replay.d_out) cudaFreeAsync(replay.d_out, replay.stream);
+        if (replay.d_qf) cudaFreeAsync(replay.d_qf, replay.stream);
+        replay = Replay{};
     }
 };
 
@@ -1872,6 +1896,7 @@ int gpj_batch_add(gpj_batch* b, gpj_file* f, int nq, const char* const* paths, i
     }
     b->items.push_back(std::move(it));
     b->ran = false;
+    b->dirty = true;
     *item = static_cast<int>(b->items.size() - 1);
     return GPJ_OK;
 }
@@ -1930,12 +1955,48 @@ int gpj_batch_run(gpj_batch* b) {
         total_out += nq * static_cast<size_t>(fr.lines) * fr.slots * 2;
         total_items += gpj::query_items(fr.lines, static_cast<int>(nq));
     }
+    // what the query phase reads: replay its graph when nothing of it changed
+    int depth = 0;
+    for (auto& fr : b->files) depth = std::max(depth, fr.depth);
+    std::vector<uint64_t> sig{static_cast<uint64_t>(reinterpret_cast<uintptr_t>(ctx->stream)),
+                              static_cast<uint64_t>(ctx->tuning.long_line_bytes),
+                              static_cast<uint64_t>(query_occupancy(ctx, depth))};
+    for (auto& fr : b->files) {
+        gpj_file* f = fr.file;
+        for (uint64_t v : {static_cast<uint64_t>(reinterpret_cast<uintptr_t>(f)),
+                           static_cast<uint64_t>(reinterpret_cast<uintptr_t>(f->d_data)),
+                           static_cast<uint64_t>(reinterpret_cast<uintptr_t>(f->d_nl)),
+                           static_cast<uint64_t>(reinterpret_cast<uintptr_t>(f->d_str)),
+                           static_cast<uint64_t>(reinterpret_cast<uintptr_t>(f->d_lvl)),
+                           static_cast<uint64_t>(reinterpret_cast<uintptr_t>(f->colon_valid ? f->d_colon : nullptr)),
+                           static_cast<uint64_t>(f->num_lines), static_cast<uint64_t>(f->n)})
+            sig.push_back(v);
+    }
+    if (!b->dirty && b->replay.exec && b->replay.sig == sig && b->replay.dst->refs.load() == 1) {
+        cudaError_t e = cudaGraphLaunch(b->replay.exec, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "batch query (graph)");
+        ctx->launches += long_lines(ctx).items ? 2 : 1;
+        b->cur = b->replay.dst;
+        b->replays++;
+        rc = end_phase(ctx, "batch_query_replay", t0);
+        if (rc) return rc;
+        b->ran = true;
+        return GPJ_OK;
+    }
+    b->drop_replay();
+    // a graph pays off from the third identical run on: capture only when
+    // the requests did not change since the last run (a serving loop's
+    // batches, new every time, run directly)
+    const bool try_capture = !b->dirty;
+    b->dirty = false;
     uint8_t* d_blob = nullptr;
     int64_t* d_out = nullptr;
     gpj::QueryFile* d_qf = nullptr;
     rc = device_alloc(ctx, &d_blob, blob.size(), "cudaMalloc(batch bytecode)");
     if (!rc) rc = device_alloc(ctx, &d_out, std::max<size_t>(total_out, 1), "cudaMalloc(batch results)");
     if (!rc) rc = device_alloc(ctx, &d_qf, b->files.size(), "cudaMalloc(batch query files)");
+    bool captured = false;
     if (!rc) {
         std::vector<gpj::QueryFile> qf;
         int64_t item = 0;
@@ -1955,18 +2016,6 @@ int gpj_batch_run(gpj_batch* b) {
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(d_qf, qf.data(), sizeof(gpj::QueryFile) * qf.size(), cudaMemcpyHostToDevice,
                                 ctx->stream);
-        if (e == cudaSuccess && total_items > 0) {
-            int depth = 0;
-            for (auto& fr : b->files) depth = std::max(depth, fr.depth);
-            const int64_t grid = std::max<int64_t>(
-                1, std::min<int64_t>((total_items + 255) / 256, static_cast<int64_t>(ctx->sms) * query_occupancy(ctx, depth)));
-            const gpj::LongLines ll = long_lines(ctx);
-            if (ll.items) e = cudaMemsetAsync(ctx->d_long_count, 0, sizeof(unsigned long long), ctx->stream);
-            if (e == cudaSuccess)
-                e = gpj::launch_find_value_batch(d_qf, static_cast<int>(qf.size()), total_items, depth, ll,
-                                                 static_cast<int>(grid), ctx->sms * 2, ctx->stream);
-            ctx->launches += ll.items ? 2 : 1;
-        }
         // a page-locked buffer no result of an earlier run refers to (every
         // earlier run's copy has completed: each run ends synchronised)
         PinnedResults* pick = nullptr;
@@ -1998,14 +2047,65 @@ int gpj_batch_run(gpj_batch* b) {
             }
         }
         if (pick) b->cur = pick;
-        if (e == cudaSuccess && total_out > 0)
-            e = cudaMemcpyAsync(pick->p, d_out, total_out * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        // the query phase: captured as a graph (kept for the next run) when
+        // the stream allows it, else launched directly
+        const int64_t grid = std::max<int64_t>(
+            1, std::min<int64_t>((total_items + 255) / 256,
+                                 static_cast<int64_t>(ctx->sms) * query_occupancy(ctx, depth)));
+        const gpj::LongLines ll = long_lines(ctx);
+        auto query_phase = [&]() -> cudaError_t {
+            cudaError_t q = cudaSuccess;
+            if (total_items > 0) {
+                if (ll.items) q = cudaMemsetAsync(ctx->d_long_count, 0, sizeof(unsigned long long), ctx->stream);
+                if (q == cudaSuccess)
+                    q = gpj::launch_find_value_batch(d_qf, static_cast<int>(qf.size()), total_items, depth, ll,
+                                                     static_cast<int>(grid), ctx->sms * 2, ctx->stream);
+            }
+            if (q == cudaSuccess && total_out > 0)
+                q = cudaMemcpyAsync(pick->p, d_out, total_out * 8, cudaMemcpyDeviceToHost, ctx->stream);
+            return q;
+        };
+        cudaGraphExec_t exec = nullptr;
+        if (e == cudaSuccess) {
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            cudaError_t ce = cudaStreamIsCapturing(ctx->stream, &cs);
+            if (try_capture && ce == cudaSuccess && cs == cudaStreamCaptureStatusNone && ctx->stream != nullptr &&
+                cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                const cudaError_t qe = query_phase();
+                cudaGraph_t graph = nullptr;
+                const cudaError_t ee = cudaStreamEndCapture(ctx->stream, &graph);
+                if (qe == cudaSuccess && ee == cudaSuccess && graph &&
+                    cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+                    captured = true;
+                } else {
+                    exec = nullptr;
+                }
+                if (graph) cudaGraphDestroy(graph);
+                cudaGetLastError();
+            }
+            e = captured ? cudaGraphLaunch(exec, ctx->stream) : query_phase();
+        }
+        ctx->launches += ll.items ? 2 : 1;
         if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (!rc && e != cudaSuccess) rc = cuda_fail(ctx, e, "batch query");
+        if (captured && !rc) {
+            b->replay.exec = exec;
+            b->replay.sig = sig;
+            b->replay.d_blob = d_blob;
+            b->replay.d_out = d_out;
+            b->replay.d_qf = d_qf;
+            b->replay.dst = pick;  // a buffer of the pool: replayed only while no result refers to it
+            b->replay.stream = ctx->stream;
+        } else if (exec) {
+            cudaGraphExecDestroy(exec);
+            captured = false;
+        }
     }
-    device_free(ctx, d_blob);
-    device_free(ctx, d_out);
-    device_free(ctx, d_qf);
+    if (!captured) {
+        device_free(ctx, d_blob);
+        device_free(ctx, d_out);
+        device_free(ctx, d_qf);
+    }
     if (rc) return rc;
     rc = end_phase(ctx, "batch_query", t0);
     if (rc) return rc;
@@ -2060,6 +2160,7 @@ void gpj_batch_clear(gpj_batch* b) {
     b->items.clear();
     b->files.clear();
     b->ran = false;
+    b->dirty = true;
 }
 
 void gpj_batch_release(gpj_batch* b) { delete b; }

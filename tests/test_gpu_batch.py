@@ -101,3 +101,56 @@ def test_batch_errors(gpjson):
     finally:
         b.release()
         f.release()
+
+
+@pytest.mark.gpu
+def test_batch_replays_its_query_graph(gpjson):
+    """A batch run again with the same requests on the same resident indexes
+    replays the CUDA graph of its query phase (phase batch_query_replay);
+    results are the same; holding a result, adding a request or changing the
+    launch shapes makes the next run capture a new graph."""
+    rng = random.Random(9)
+    data, requests = corpus(rng)
+    files = [gpjson.load_bytes(d) for d in data]
+    b = gpjson.batch()
+
+    def phases():
+        return [p["name"] for p in gpjson.timings()["phases"]]
+
+    try:
+        items = [b.add(files[i], paths) for i, paths in requests]
+        b.run()  # indexes the files; queries launched directly
+        first = [b.result(it).copy() for it in items]
+        b.run()  # unchanged: the query phase is captured as a graph and launched
+        assert all(np.array_equal(b.result(it), x) for it, x in zip(items, first))
+        gpjson._native.lib.gpj_reset_timings(gpjson._native.h)
+        b.run()
+        assert "batch_query_replay" in phases()
+        again = [b.result(it) for it in items]
+        assert all(np.array_equal(x, y) for x, y in zip(first, again))
+        # a result of the last run is still held: no replay into its buffer
+        gpjson._native.lib.gpj_reset_timings(gpjson._native.h)
+        b.run()
+        assert "batch_query_replay" not in phases() and "batch_query" in phases()
+        b.run()  # captured again, into another buffer
+        held = [b.result(it) for it in items]
+        assert all(np.array_equal(x, y) for x, y in zip(first, held))
+        del again, held
+        gpjson._native.lib.gpj_reset_timings(gpjson._native.h)
+        b.run()
+        assert "batch_query_replay" in phases()
+        gpjson.set_tuning(query_ctas_per_sm=1)
+        gpjson._native.lib.gpj_reset_timings(gpjson._native.h)
+        b.run()
+        assert "batch_query_replay" not in phases()
+        gpjson.set_tuning(query_ctas_per_sm=0)
+        b.add(files[0], ["$.id"])
+        gpjson._native.lib.gpj_reset_timings(gpjson._native.h)
+        b.run()
+        assert "batch_query_replay" not in phases()
+        assert all(np.array_equal(b.result(it), x) for it, x in zip(items, first))
+    finally:
+        gpjson.set_tuning(query_ctas_per_sm=0)
+        b.release()
+        for f in files:
+            f.release()
