@@ -332,9 +332,8 @@ int status_error(gpj_ctx* ctx, unsigned long long errs) {
     std::string m = "index kernel reported:";
     if (errs & gpj::kErrLookbackTimeout) m += " look-back wait expired;";
     if (errs & gpj::kErrCopyTimeout) m += " TMA copy wait expired;";
-    if (errs & gpj::kErrEscapeRun) m += " a backslash run longer than 64 KiB crosses a 16 KiB tile boundary;";
     if (errs & (gpj::kErrIrregular | gpj::kErrLongLine)) m += " unexpected line check failure;";
-    return fail(ctx, (errs & gpj::kErrEscapeRun) ? GPJ_ELIMIT : GPJ_EDEVICE, m);
+    return fail(ctx, GPJ_EDEVICE, m);
 }
 
 // Queries evaluated by the index pass (packed bytecode already on device).

@@ -41,6 +41,9 @@ __device__ __align__(256) unsigned long long g_scratch[kScratchWords];
 constexpr int kMaxDevices = 64;
 
 struct DeviceSetup {
+    // held from set-up to the end of a call's device work: calls on one
+    // device never overlap on the GPU (they would race on the array)
+    std::mutex mu;
     bool ready = false;
     unsigned long long* scratch = nullptr;
     int sms = 0;
@@ -49,7 +52,6 @@ struct DeviceSetup {
     uint32_t epoch = 0;
 };
 
-std::mutex g_mu;
 DeviceSetup g_devices[kMaxDevices];
 
 int level_slot(int num_levels) { return num_levels <= 4 ? 0 : (num_levels <= 8 ? 1 : 2); }
@@ -120,11 +122,19 @@ extern "C" int gpj_build_index_device_noalloc(void* stream_handle, const void* d
     if (num_levels < 1 || num_levels > GPJ_MAX_LEVELS) return GPJ_ELIMIT;
     if (n > kMaxBytes) return GPJ_ELIMIT;
     cudaStream_t stream = static_cast<cudaStream_t>(stream_handle);
+    // every call reads its status back and waits for its stream, which a
+    // stream being captured into a graph does not allow
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &capturing) != cudaSuccess) {
+        cudaGetLastError();
+        return GPJ_EINVAL;
+    }
+    if (capturing != cudaStreamCaptureStatusNone) return GPJ_EINVAL;
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return GPJ_ECUDA;
 
-    std::lock_guard<std::mutex> lock(g_mu);
     DeviceSetup* d = &g_devices[device];
+    std::lock_guard<std::mutex> lock(d->mu);
     if (!d->ready) {
         const int rc = setup_device(device, d);
         if (rc) return rc;
@@ -158,12 +168,14 @@ extern "C" int gpj_build_index_device_noalloc(void* stream_handle, const void* d
     unsigned long long status[2] = {0, 0};
     int rc = launch(d, false, lp, stream, status);
     if (rc) return rc;
+    // a wait that expired in the line pass is reported even when the exact
+    // pass that replaces it succeeds
+    const unsigned long long line_waits = status[1] & (gpj::kErrLookbackTimeout | gpj::kErrCopyTimeout);
     if (status[1] & (gpj::kErrIrregular | gpj::kErrLongLine)) {
         rc = launch(d, true, p, stream, status);
         if (rc) return rc;
     }
-    const unsigned long long errs = status[1] & ~(gpj::kErrDeferred | gpj::kErrOutOverflow);
-    if (errs & gpj::kErrEscapeRun) return GPJ_ELIMIT;
+    const unsigned long long errs = (status[1] | line_waits) & ~(gpj::kErrDeferred | gpj::kErrOutOverflow);
     if (errs) return GPJ_EDEVICE;
     *num_lines = static_cast<int64_t>(status[0]);
     return *num_lines > newline_cap ? GPJ_ELIMIT : GPJ_OK;

@@ -11,7 +11,6 @@ namespace gpj {
 enum DeviceError : unsigned long long {
     kErrLookbackTimeout = 1ull << 0,  // a predecessor tile never published
     kErrCopyTimeout = 1ull << 1,      // a TMA copy never completed
-    kErrEscapeRun = 1ull << 2,        // backslash run longer than the scan bound
     kErrIrregular = 1ull << 3,        // a line does not end outside strings at level -1
     kErrLongLine = 1ull << 4,         // a line runs further past its tile than the bound
     kErrDeferred = 1ull << 5,         // some lines were not evaluated by the fused queries
@@ -20,7 +19,7 @@ enum DeviceError : unsigned long long {
 
 // Errors after which waiting for other tiles is pointless (the others are
 // notes for the host: take another path for part or all of the input).
-constexpr unsigned long long kFatalErrors = kErrLookbackTimeout | kErrCopyTimeout | kErrEscapeRun;
+constexpr unsigned long long kFatalErrors = kErrLookbackTimeout | kErrCopyTimeout;
 
 // Poll budgets of the bounded waits (each poll also sleeps briefly).
 constexpr unsigned kMaxPolls = 1u << 22;

@@ -102,23 +102,30 @@ __device__ __forceinline__ Span64 shfl_span64_down(const Span64& v, int off) {
 }
 
 // Parity of the backslash run that ends just before byte `pos` (the escape
-// state of byte `pos`).  `pos` is a tile start, a multiple of 16, so the
-// bytes before it are read as aligned 16-byte vectors; at most
-// kEscapeScanBytes are examined.
-__device__ int escape_parity_before(const uint8_t* file, int64_t pos, unsigned long long* status) {
+// state of byte `pos`), however long the run (Sequential.java:36-64 has no
+// bound either).  `pos` is a tile start, a multiple of 16, so the bytes
+// before it are read as aligned 16-byte vectors, four at a time.
+__device__ int escape_parity_before(const uint8_t* file, int64_t pos) {
     int64_t run = 0;
-    const int64_t floor = pos - kEscapeScanBytes > 0 ? pos - kEscapeScanBytes : 0;
-    for (int64_t k = pos; k > floor; k -= 16) {
-        const uint4 q = __ldg(reinterpret_cast<const uint4*>(file + k - 16));
-        const uint32_t w[4] = {q.w, q.z, q.y, q.x};  // highest bytes first
+    for (int64_t k = pos; k > 0; k -= 64) {
+        const int64_t lo = k - 64 > 0 ? k - 64 : 0;
+        uint4 q[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const uint32_t nb = ~eq_bytes(w[i], 0x5C5C5C5Cu) & 0x80808080u;  // non-backslash bytes
-            if (nb) return static_cast<int>((run + (__clz(nb) >> 3)) & 1);
-            run += 4;
+        for (int j = 0; j < 4; j++)  // the 16-byte vectors ending at k, k - 16, ...
+            q[j] = k - 16 * (j + 1) >= lo ? __ldg(reinterpret_cast<const uint4*>(file + k - 16 * (j + 1)))
+                                          : make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (k - 16 * (j + 1) < lo) return static_cast<int>(run & 1);  // the file's first byte
+            const uint32_t w[4] = {q[j].w, q[j].z, q[j].y, q[j].x};  // highest bytes first
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t nb = ~eq_bytes(w[i], 0x5C5C5C5Cu) & 0x80808080u;  // non-backslash bytes
+                if (nb) return static_cast<int>((run + (__clz(nb) >> 3)) & 1);
+                run += 4;
+            }
         }
     }
-    if (floor > 0) atomicOr(status + 1, kErrEscapeRun);
     return static_cast<int>(run & 1);
 }
 
@@ -233,7 +240,7 @@ __device__ int64_t claim_and_load(const IndexParams& p, Shared& sh, int b) {
             mbar_arrive(&sh.bar[b]);
         }
         for (int64_t i = bulk; i < bytes; i++) sh.buf[b][i] = p.file[start + i];  // < 16 tail bytes
-        sh.esc_parity[b] = start == 0 ? 0 : escape_parity_before(p.file, start, p.status);
+        sh.esc_parity[b] = start == 0 ? 0 : escape_parity_before(p.file, start);
     }
     return t;
 }

@@ -14,10 +14,6 @@ constexpr int64_t kLineTileBytes = 14336;
 // The standalone index kernel owns 30 KiB per tile and reads 2 KiB past it:
 // four consecutive 64-byte words per thread of a 128-thread CTA.
 constexpr int64_t kStandaloneTileBytes = 30720;
-// The escape state at a tile start is found by scanning back over the bytes
-// before it; a backslash run longer than this crossing a tile start is
-// reported as an error (kErrEscapeRun) instead of being resolved.
-constexpr int64_t kEscapeScanBytes = 1 << 16;
 
 // The file a tile of the standalone index kernel belongs to.  A build over
 // one file uses IndexParams' own fields; a batch passes one entry per file,

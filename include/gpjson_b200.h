@@ -239,14 +239,17 @@ int gpj_build_index_device(gpj_ctx *ctx, const void *d_file, int64_t n, int num_
  * cudaStream_t of that device; NULL = the legacy default stream), and
  * synchronizes that stream before returning (to read the line count).
  * The first call on a device looks the array up (cudaGetSymbolAddress) and
- * sets the kernels' shared-memory attributes; make it outside stream capture
- * and before any latency-critical call.  All calls on one device share the
- * array: calls that overlap in time, from two threads or on two streams,
- * race and give wrong results; the caller serializes them.
- * Returns GPJ_OK, GPJ_EINVAL, GPJ_ELIMIT (input too large, newline_cap too
- * small, or an escape run the kernel cannot resolve), GPJ_ECUDA (CUDA error or
- * a device that is not sm_100) or GPJ_EDEVICE (a kernel wait expired).  There
- * is no context to carry a message; the code is the whole report. */
+ * sets the kernels' shared-memory attributes; make it before any
+ * latency-critical call.  Every call reads its status back and waits for its
+ * stream, so no call may be made on a stream that is being captured into a
+ * graph (GPJ_EINVAL).  All calls on one device share the array, and calls
+ * that overlapped on the GPU would race on it: within a process the library
+ * serializes the calls on one device (a lock held until the call's device
+ * work has finished), so a second thread's call waits for the first.
+ * Returns GPJ_OK, GPJ_EINVAL, GPJ_ELIMIT (input too large or newline_cap too
+ * small), GPJ_ECUDA (CUDA error or a device that is not sm_100) or
+ * GPJ_EDEVICE (a kernel wait expired, in either pass).  There is no context
+ * to carry a message; the code is the whole report. */
 int gpj_build_index_device_noalloc(void *stream, const void *d_file, int64_t n, int num_levels,
                                    uint64_t *d_string_index, uint64_t *d_leveled,
                                    int64_t *d_newlines, int64_t newline_cap, int64_t *num_lines);

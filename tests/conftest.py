@@ -5,6 +5,7 @@ host-compiled device arithmetic)."""
 from __future__ import annotations
 
 import ctypes
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -31,10 +32,14 @@ def hostsim():
     csrc = ROOT / "gpjson_b200" / "csrc"
     deps = [HOSTSIM_SRC, csrc / "host_io.h"] + list(csrc.glob("*.cuh"))
     if not HOSTSIM_LIB.exists() or any(d.stat().st_mtime > HOSTSIM_LIB.stat().st_mtime for d in deps):
+        # built beside the target and renamed over it, so that a library
+        # mapped by another process is never rewritten in place
+        tmp = HOSTSIM_LIB.with_suffix(f".{os.getpid()}.tmp")
         subprocess.run(
-            ["g++", "-std=c++17", "-O2", "-shared", "-fPIC", "-pthread", "-o", str(HOSTSIM_LIB), str(HOSTSIM_SRC)],
+            ["g++", "-std=c++17", "-O2", "-shared", "-fPIC", "-pthread", "-o", str(tmp), str(HOSTSIM_SRC)],
             check=True,
         )
+        tmp.replace(HOSTSIM_LIB)
     L = ctypes.CDLL(str(HOSTSIM_LIB))
     P = ctypes.c_void_p
     L.hs_build_index.restype = ctypes.c_int64

@@ -74,6 +74,19 @@ def test_escape_runs_across_tiles(gpjson):
 
 
 @pytest.mark.gpu
+def test_backslash_runs_longer_than_many_tiles(gpjson):
+    """Backslash runs of 100 KB and more cross several tiles of the exact
+    kernel (which resolves the escape state at a tile start by scanning back
+    over the run, however long); even and odd lengths, in a line of a
+    well-formed file and in pretty-printed input."""
+    for run in (100_000, 100_001, 300_003):
+        for pre in (0, 5, 16384 - 7):
+            line = b'{"s":"' + b"a" * pre + b"\\" * run + b'"x", "t":[1,{"u":"\\\\"}]}'
+            assert_index_equal(gpjson, line + b"\n" + b'{"a":[1]}\n' + line, 4)
+            assert_index_equal(gpjson, b'{\n "x": [\n  ' + line + b"\n ]\n}\n", 4)
+
+
+@pytest.mark.gpu
 def test_long_string_over_many_tiles(gpjson):
     body = b'{"s":"' + (b"ab\\\"c{[:,]}" * 20000) + b'","t":[1,{"u":2}]}\n'
     assert_index_equal(gpjson, body * 3, 4)

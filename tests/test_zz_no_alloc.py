@@ -127,3 +127,29 @@ def test_noalloc_rejects_oversized_input(gpjson):
         None, d.data_ptr(), 4096, 17, d.data_ptr(), d.data_ptr(), d.data_ptr(), d.numel(), ctypes.byref(lines)
     )
     assert rc == _lib.GPJ_ELIMIT
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_a_capturing_stream(gpjson):
+    """A call on a stream that is being captured into a graph is refused
+    (GPJ_EINVAL) before it touches the stream: every call reads its status
+    back and waits for its stream, which capture does not allow."""
+    import torch
+
+    lib = gpjson._native.lib
+    data = datagen.tweets(1 << 20, seed=datagen.SEED_BASE + 31).tobytes()
+    n = len(data)
+    d_file = torch.frombuffer(bytearray(data), dtype=torch.uint8).cuda()
+    d_str, d_lvl, d_nl = device_buffers(torch, n, 4)
+    lines = ctypes.c_int64(-1)
+    side = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph, stream=side):
+        rc = lib.gpj_build_index_device_noalloc(
+            ctypes.c_void_p(side.cuda_stream), d_file.data_ptr(), n, 4, d_str.data_ptr(), d_lvl.data_ptr(),
+            d_nl.data_ptr(), d_nl.numel(), ctypes.byref(lines),
+        )
+        d_str.add_(0)  # some captured work
+    assert rc == _lib.GPJ_EINVAL and lines.value == -1
+    torch.cuda.synchronize()
