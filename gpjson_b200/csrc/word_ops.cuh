@@ -16,6 +16,8 @@
 
 namespace gpj {
 
+// Byte permute: result byte i is byte (s_i & 7) of the 8-byte pair (y:x)
+// for the selector nibbles s_i (bit 3 of each nibble ignored).
 GPJ_HD uint32_t byte_perm(uint32_t x, uint32_t y, uint32_t s) {
 #ifdef __CUDA_ARCH__
     return __byte_perm(x, y, s);
@@ -23,6 +25,27 @@ GPJ_HD uint32_t byte_perm(uint32_t x, uint32_t y, uint32_t s) {
     const uint64_t v = (static_cast<uint64_t>(y) << 32) | x;
     uint32_t r = 0;
     for (int i = 0; i < 4; i++) r |= static_cast<uint32_t>((v >> (8 * ((s >> (4 * i)) & 7))) & 0xFF) << (8 * i);
+    return r;
+#endif
+}
+
+// The same with bit 3 of a selector nibble honoured as PTX prmt's default
+// mode defines it: that result byte is the selected byte's bit 7 replicated
+// over all eight bits (a zero byte for a table byte below 0x80).
+GPJ_HD uint32_t byte_perm_sign(uint32_t x, uint32_t y, uint32_t s) {
+#ifdef __CUDA_ARCH__
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(y), "r"(s));
+    return r;
+#else
+    const uint64_t v = (static_cast<uint64_t>(y) << 32) | x;
+    uint32_t r = 0;
+    for (int i = 0; i < 4; i++) {
+        const uint32_t sel = (s >> (4 * i)) & 0xF;
+        uint32_t b = static_cast<uint32_t>((v >> (8 * (sel & 7))) & 0xFF);
+        if (sel & 8) b = (b & 0x80) ? 0xFF : 0x00;
+        r |= b << (8 * i);
+    }
     return r;
 #endif
 }
@@ -91,53 +114,77 @@ struct ClassMasks {
     uint64_t colon;       // ':'
 };
 
+// Class bits of each byte of 32 bytes: the byte's high nibble h and low
+// nibble l look up one table each (PRMT with 4-bit selectors) and the
+// results AND together, so a class bit survives only for the (h, l) pairs
+// of its characters: '\n' 0A, ',' 2C, ':' 3A, '\\' 5C, '[' 5B and '{' 7B
+// (open), ']' 5D and '}' 7D (close).  Lookups are by h (0-7; a non-ASCII
+// byte, h >= 8, reads a sign-replicated zero) and by l ^ 8 (the low nibbles
+// A-D of these characters become 2-5; every other value either selects a
+// zero entry or reads a sign-replicated zero; byte_perm_sign).  '"' is the one character
+// with a low nibble below 8 and is found by a byte compare (bit 7).
+constexpr uint32_t kClsNewline = 1u << 0, kClsComma = 1u << 1, kClsColon = 1u << 2, kClsBackslash = 1u << 3,
+                   kClsOpen = 1u << 4, kClsClose = 1u << 5, kClsQuote = 1u << 7;
+// table by high nibble: entries 0-3 and 4-7
+constexpr uint32_t kHiTab0 = kClsNewline | (0u << 8) | (kClsComma << 16) | (kClsColon << 24);
+constexpr uint32_t kHiTab1 = 0u | ((kClsBackslash | kClsOpen | kClsClose) << 8) | (0u << 16) |
+                             ((kClsOpen | kClsClose) << 24);
+// table by low nibble ^ 8: entries 0-3 (l = 8, 9, A, B) and 4-7 (l = C, D, E, F)
+constexpr uint32_t kLoTab0 = 0u | (0u << 8) | ((kClsNewline | kClsColon) << 16) | (kClsOpen << 24);
+constexpr uint32_t kLoTab1 = (kClsComma | kClsBackslash) | (kClsClose << 8) | (0u << 16) | (0u << 24);
+
+// The four nibbles at bits 0-3, 8-11, 16-19, 24-27 of x packed into a PRMT
+// selector (bits 0-15).
+GPJ_HD uint32_t nibble_selector(uint32_t x) {
+    const uint32_t c = (x | (x >> 4)) & 0x00FF00FFu;
+    return byte_perm(c, 0, 0x3320);
+}
+
+GPJ_HD uint32_t class_bytes(uint32_t x) {
+    const uint32_t hi = nibble_selector((x >> 4) & 0x0F0F0F0Fu);
+    const uint32_t lo = nibble_selector((x ^ 0x08080808u) & 0x0F0F0F0Fu);
+    const uint32_t c = byte_perm_sign(kHiTab0, kHiTab1, hi) & byte_perm_sign(kLoTab0, kLoTab1, lo);
+    return c | eq_bytes(x, 0x22222222u);  // '"' at bit 7
+}
+
+// One step of the bit-matrix transpose: swaps bit rows of a and b at
+// distance s (bits of mask m of b with the bits s higher of a).
+GPJ_HD void swap_bits(uint32_t& a, uint32_t& b, int s, uint32_t m) {
+    const uint32_t t = ((a >> s) ^ b) & m;
+    b ^= t;
+    a ^= t << s;
+}
+
 // Classifies 32 bytes given as 8 little-endian u32 (v[j] = bytes 4j..4j+3).
 // The bytes are first transposed so that t[w] holds bytes {w, w+8, w+16,
-// w+24}; the per-byte flag of byte 8k+w then sits at bit 8k+7 of the test
-// result for t[w], and shifting it right by 7-w drops it on bit 8k+w: the
-// eight shifted results OR (or add) into the 32-bit mask in byte order.
+// w+24}; their class bytes form, in each byte lane k, an 8x8 bit matrix
+// (row w = t[w]'s class byte, column = class bit), transposed in three
+// rounds of swaps so that row c afterwards holds class c with byte 8k+w at
+// bit 8k+w: the class masks in byte order.
 GPJ_HD void classify32(const uint32_t v[8], uint32_t& bs, uint32_t& qt, uint32_t& nl, uint32_t& op,
                        uint32_t& cl, uint32_t& st, uint32_t& cn) {
     uint32_t t[8];
     transpose4(v[0], v[2], v[4], v[6], t[0], t[1], t[2], t[3]);
     transpose4(v[1], v[3], v[5], v[7], t[4], t[5], t[6], t[7]);
-    bs = qt = nl = op = cl = st = cn = 0;
+    uint32_t r[8];
 #pragma unroll
-    for (int w = 0; w < 8; w++) {
-        const uint32_t x = t[w];
-        const uint32_t y = x | 0x20202020u;  // folds '['->'{', ']'->'}'
-        const uint32_t fb = eq_bytes(x, 0x5C5C5C5Cu);
-        const uint32_t fq = eq_bytes(x, 0x22222222u);
-        const uint32_t fn = eq_bytes(x, 0x0A0A0A0Au);
-        // a byte is structural when it equals any of the four patterns: the
-        // "differs" bits AND together (y has x's bit 7)
-        const uint32_t lo = low_differs(y, 0x7B7B7B7Bu), lc = low_differs(y, 0x7D7D7D7Du);
-        const uint32_t lk = low_differs(x, 0x3A3A3A3Au), lm = low_differs(x, 0x2C2C2C2Cu);
-        const uint32_t fo = ~(lo | x) & 0x80808080u;
-        const uint32_t fc = ~(lc | x) & 0x80808080u;
-        const uint32_t fk = ~(lk | x) & 0x80808080u;
-        const uint32_t fs = ~((lo & lc & lk & lm) | x) & 0x80808080u;
-        // flags of different w occupy different bits, so adding equals OR;
-        // the high half of f * 2^(25+w) is f >> (7-w) (one multiply-add)
-        if (w < 7) {
-            const uint32_t mul = 1u << (25 + w);
-            bs += mulhi32(fb, mul);
-            qt += mulhi32(fq, mul);
-            nl += mulhi32(fn, mul);
-            op += mulhi32(fo, mul);
-            cl += mulhi32(fc, mul);
-            st += mulhi32(fs, mul);
-            cn += mulhi32(fk, mul);
-        } else {
-            bs += fb;
-            qt += fq;
-            nl += fn;
-            op += fo;
-            cl += fc;
-            st += fs;
-            cn += fk;
-        }
+    for (int w = 0; w < 8; w++) r[w] = class_bytes(t[w]);
+#pragma unroll
+    for (int w = 0; w < 4; w++) swap_bits(r[w], r[w + 4], 4, 0x0F0F0F0Fu);
+#pragma unroll
+    for (int w = 0; w < 8; w += 4) {
+        swap_bits(r[w], r[w + 2], 2, 0x33333333u);
+        swap_bits(r[w + 1], r[w + 3], 2, 0x33333333u);
     }
+#pragma unroll
+    for (int w = 0; w < 8; w += 2) swap_bits(r[w], r[w + 1], 1, 0x55555555u);
+    nl = r[0];
+    cn = r[2];
+    bs = r[3];
+    op = r[4];
+    cl = r[5];
+    qt = r[7];
+    st = r[1] | r[2] | op | cl;  // ',' ':' and the brackets
 }
 
 GPJ_HD ClassMasks classify64(const uint32_t v[16]) {
