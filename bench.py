@@ -87,6 +87,9 @@ def parse_args(argv=None):
                          "requests, continuous batching vs per-request")
     ap.add_argument("--requests", type=int, default=20000, help="serving: number of requests")
     ap.add_argument("--no-tune", action="store_true", help="keep the library's default launch shapes")
+    ap.add_argument("--chunk-tiles", type=int, default=None,
+                    help="after tuning: index and query the resident file in chunks of this many 30 KiB tiles "
+                         "(a multiple of 1024; 0 = whole-file passes)")
     ap.add_argument("--no-extras", action="store_true",
                     help="default run: skip the adversarial, batched and serving measurements added to its line")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: arrivals per second")
@@ -357,6 +360,8 @@ def measure_file(args, w: Workload, rank: int, world: int, local: int, device) -
         while cut > 1 and host_np[cut - 1] != 10:
             cut -= 1
         tuned = tune.tune(g, dev[:cut], QUERIES, LEVELS, device=local, persist=False, workload=w.name)
+    if args.chunk_tiles is not None:
+        g.set_tuning(chunk_tiles=args.chunk_tiles)
     f = g.from_device(dev.data_ptr(), n, keepalive=dev)
 
     # first pass sizes the index and result buffers

@@ -601,16 +601,17 @@ class GPJSON:
         t = _lib.Tuning()
         self._native.check(self._native.lib.gpj_get_tuning(self._native.h, byref(t)))
         return {"long_line_bytes": t.long_line_bytes, "query_ctas_per_sm": t.query_ctas_per_sm,
-                "index_ctas_per_sm": t.index_ctas_per_sm}
+                "index_ctas_per_sm": t.index_ctas_per_sm, "chunk_tiles": t.chunk_tiles}
 
     def set_tuning(self, long_line_bytes: int | None = None, query_ctas_per_sm: int | None = None,
-                   index_ctas_per_sm: int | None = None) -> None:
+                   index_ctas_per_sm: int | None = None, chunk_tiles: int | None = None) -> None:
         """gpj_set_tuning: changes the given launch shapes (results do not
         depend on them)."""
         cur = self.tuning()
         t = _lib.Tuning(cur["long_line_bytes"] if long_line_bytes is None else long_line_bytes,
                         cur["query_ctas_per_sm"] if query_ctas_per_sm is None else query_ctas_per_sm,
-                        cur["index_ctas_per_sm"] if index_ctas_per_sm is None else index_ctas_per_sm)
+                        cur["index_ctas_per_sm"] if index_ctas_per_sm is None else index_ctas_per_sm,
+                        cur["chunk_tiles"] if chunk_tiles is None else chunk_tiles, 0)
         self._native.check(self._native.lib.gpj_set_tuning(self._native.h, byref(t)))
 
     def set_stream(self, stream_handle: int | None) -> None:

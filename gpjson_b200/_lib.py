@@ -34,7 +34,8 @@ class Tuning(ctypes.Structure):
     """gpj_tuning: launch shapes of a context's kernels."""
 
     _fields_ = [("long_line_bytes", c_int64), ("query_ctas_per_sm", ctypes.c_int32),
-                ("index_ctas_per_sm", ctypes.c_int32)]
+                ("index_ctas_per_sm", ctypes.c_int32), ("chunk_tiles", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
 
 
 class ServerConfig(ctypes.Structure):

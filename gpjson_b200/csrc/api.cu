@@ -51,6 +51,7 @@ static gpj_tuning default_tuning() {
     t.long_line_bytes = 65536;
     t.query_ctas_per_sm = 0;
     t.index_ctas_per_sm = 0;
+    t.chunk_tiles = 0;
     return t;
 }
 
@@ -585,6 +586,7 @@ gpj::LongLines long_lines(const gpj_ctx* ctx) {
 // (`last`: they include the file's last line).
 int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, int64_t out_lines,
                  const int64_t* d_range = nullptr, bool last = false) {
+    cudaStream_t stream = ctx->stream;
     const size_t header = ((static_cast<size_t>(nq) * 4 + 15) / 16) * 16;
     gpj::QueryParams p{};
     p.file = f->d_data;
@@ -607,11 +609,11 @@ int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, i
     p.depth = f->ir_depth;
     p.long_lines = long_lines(ctx);
     if (p.long_lines.items)
-        GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_long_count, 0, sizeof(unsigned long long), ctx->stream));
+        GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_long_count, 0, sizeof(unsigned long long), stream));
     const int64_t want = d_range ? INT64_MAX : (gpj::query_items(f->num_lines, nq) + 255) / 256;
     const int64_t grid = std::max<int64_t>(
         1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * query_occupancy(ctx, f->ir_depth)));
-    GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->sms * 2, ctx->stream));
+    GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->sms * 2, stream));
     ctx->launches += p.long_lines.items ? 2 : 1;
     return GPJ_OK;
 }
@@ -701,9 +703,15 @@ struct ChunkQueries {
 // tells whether they all ran that way).  Inputs the line kernel cannot
 // index this way (not NDJSON, or a line longer than a chunk) are indexed
 // again from the complete copy by run_index.
+//
+// host == nullptr: the input is already in f->d_data; chunks of
+// `chunk_tiles` tiles are indexed and queried in turn (index kernel, newline
+// index, find_value on the lines the chunk completes), so find_value reads a
+// chunk's index while it is still in L2.
 int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_levels, const ChunkQueries* cq = nullptr,
-                   bool* queries_done = nullptr) {
+                   bool* queries_done = nullptr, int64_t chunk_tiles = kLoadTiles) {
     const int64_t n = f->n;
+    const bool resident = host == nullptr;
     if (queries_done) *queries_done = false;
     int rc = ensure_index_buffers(ctx, f, num_levels);
     if (rc) return rc;
@@ -711,17 +719,18 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
     f->colon_valid = false;
     const double t0 = now_ms();
     GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    const int64_t nchunks = (n + kLoadChunk - 1) / kLoadChunk;
+    const int64_t chunk_bytes = gpj::kStandaloneTileBytes * chunk_tiles;
+    const int64_t nchunks = (n + chunk_bytes - 1) / chunk_bytes;
     int64_t lines = 0;
     if (nchunks <= 1) {
-        if (n > 0)
+        if (n > 0 && !resident)
             GPJ_CUDA(ctx, cudaMemcpyAsync(f->d_owned, host, static_cast<size_t>(n), cudaMemcpyHostToDevice,
                                           ctx->stream));
         rc = run_index(ctx, f->d_data, n, num_levels, f->d_str, f->d_lvl, f->d_nl, f->nl_cap, &lines, nullptr,
                            nullptr, f->d_colon, &f->colon_valid, &f->exact_only);
         if (rc) return rc;
     } else {
-        while (static_cast<int64_t>(ctx->chunk_events.size()) < nchunks) {
+        while (!resident && static_cast<int64_t>(ctx->chunk_events.size()) < nchunks) {
             cudaEvent_t e = nullptr;
             GPJ_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             ctx->chunk_events.push_back(e);
@@ -747,8 +756,8 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
             cudaError_t e = cq ? cudaMemsetAsync(d_lines, 0, sizeof(int64_t), ctx->stream) : cudaSuccess;
             if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_status, 0, 2 * sizeof(unsigned long long), ctx->stream);
             // the copies start once the buffers exist (pool allocations are ordered on ctx->stream)
-            if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_ready, ctx->stream);
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0);
+            if (e == cudaSuccess && !resident) e = cudaEventRecord(ctx->ev_ready, ctx->stream);
+            if (e == cudaSuccess && !resident) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_ready, 0);
             if (e != cudaSuccess) rc = cuda_fail(ctx, e, "chunked index setup");
         }
         if (rc) {
@@ -761,9 +770,10 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         p.newline_bits = ts.bits;
         p.tile_newlines = ts.counts;
         auto launch_chunk = [&](int64_t k) -> int {
-            const int64_t t0 = k * kLoadTiles, t1 = std::min(p.ntiles, (k + 1) * kLoadTiles);
-            set_tile_range(&p, t0, t1, std::min(n, (k + 2) * kLoadChunk));
-            GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->chunk_events[std::min(k + 1, nchunks - 1)], 0));
+            const int64_t t0 = k * chunk_tiles, t1 = std::min(p.ntiles, (k + 1) * chunk_tiles);
+            set_tile_range(&p, t0, t1, resident ? n : std::min(n, (k + 2) * chunk_bytes));
+            if (!resident)
+                GPJ_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->chunk_events[std::min(k + 1, nchunks - 1)], 0));
             int r = launch_tiles(ctx, p);
             if (r || !cq) return r;
             // the chunk's newline index, then the queries on the lines it completes
@@ -774,14 +784,18 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
             return launch_query(ctx, f, cq->nq, cq->slots, cq->d_out, cq->out_lines, d_lines + k, k == nchunks - 1);
         };
         for (int64_t k = 0; k < nchunks && !rc; k++) {
-            const int64_t pos = k * kLoadChunk;
-            const size_t len = static_cast<size_t>(std::min(kLoadChunk, n - pos));
+            if (resident) {
+                rc = launch_chunk(k);
+                continue;
+            }
+            const int64_t pos = k * chunk_bytes;
+            const size_t len = static_cast<size_t>(std::min(chunk_bytes, n - pos));
             cudaError_t e = cudaMemcpyAsync(f->d_owned + pos, host + pos, len, cudaMemcpyHostToDevice, ctx->copy_stream);
             if (e == cudaSuccess) e = cudaEventRecord(ctx->chunk_events[k], ctx->copy_stream);
             if (e != cudaSuccess) rc = cuda_fail(ctx, e, "cudaMemcpyAsync(file chunk)");
             if (!rc && k >= 1) rc = launch_chunk(k - 1);
         }
-        if (!rc) rc = launch_chunk(nchunks - 1);
+        if (!rc && !resident) rc = launch_chunk(nchunks - 1);
         if (!rc) {
             if (cq) {  // the newline index is complete: read the status words
                 cudaError_t e = cudaMemcpyAsync(ctx->h_status, ctx->d_status, 2 * sizeof(unsigned long long),
@@ -796,7 +810,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
         device_free(ctx, d_lines);
         if (rc) {
             f->colon_valid = false;
-            cudaStreamSynchronize(ctx->copy_stream);
+            if (!resident) cudaStreamSynchronize(ctx->copy_stream);
             return rc;
         }
         const unsigned long long errs = ctx->h_status[1];
@@ -822,7 +836,7 @@ int load_and_index(gpj_ctx* ctx, gpj_file* f, const uint8_t* host, int num_level
                            nullptr, f->d_colon, &f->colon_valid, &f->exact_only);
         if (rc) return rc;
     }
-    rc = end_phase(ctx, "load_and_index", t0);
+    rc = end_phase(ctx, resident ? "index_and_query" : "load_and_index", t0);
     if (rc) return rc;
     f->num_lines = lines;
     f->num_levels = num_levels;
@@ -842,6 +856,30 @@ int index_and_query(gpj_ctx* ctx, gpj_file* f, int num_levels, int nq, const uin
     if (depth > num_levels)
         return fail(ctx, GPJ_ELIMIT, "queries need " + std::to_string(depth) + " levels, the index is built with " +
                                          std::to_string(num_levels));
+    const int64_t chunk_tiles = ctx->tuning.chunk_tiles;
+    if (!ctx->fuse_queries && chunk_tiles > 0 && !f->exact_only &&
+        f->n > gpj::kStandaloneTileBytes * chunk_tiles) {
+        // chunk by chunk: index kernel, newline index, find_value on the
+        // lines the chunk completes
+        ChunkQueries cq;
+        cq.nq = nq;
+        cq.slots = slots;
+        cq.d_out = d_out;
+        cq.out_lines = out_lines;
+        bool done = false;
+        rc = load_and_index(ctx, f, nullptr, num_levels, &cq, &done, chunk_tiles);
+        if (rc) return rc;
+        if (lines_needed) *lines_needed = f->num_lines;
+        if (f->num_lines > out_lines)
+            return fail(ctx, GPJ_ELIMIT, "result buffer holds " + std::to_string(out_lines) +
+                                             " lines, the file has " + std::to_string(f->num_lines));
+        if (done) return GPJ_OK;
+        const double t1 = now_ms();
+        GPJ_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+        rc = launch_query(ctx, f, nq, slots, d_out, out_lines);
+        if (rc) return rc;
+        return end_phase(ctx, "find_value", t1);
+    }
     if (!ctx->fuse_queries) {
         // index kernel, then one find_value launch for all queries
         rc = index_pass(ctx, f, num_levels, nullptr, nullptr);
@@ -1074,6 +1112,8 @@ int gpj_set_tuning(gpj_ctx* ctx, const gpj_tuning* tuning) {
     if (!tuning) return fail(ctx, GPJ_EINVAL, "tuning is null");
     if (tuning->query_ctas_per_sm < 0 || tuning->index_ctas_per_sm < 0)
         return fail(ctx, GPJ_EINVAL, "CTAs per SM must be >= 0");
+    if (tuning->chunk_tiles < 0 || tuning->chunk_tiles % 1024 != 0)
+        return fail(ctx, GPJ_EINVAL, "chunk_tiles must be a multiple of 1024 (0 = whole-file passes)");
     ctx->tuning = *tuning;
     if (ctx->tuning.long_line_bytes == 0) ctx->tuning.long_line_bytes = default_tuning().long_line_bytes;
     return GPJ_OK;

@@ -6,13 +6,15 @@ functions/QueryFunction.java:201-241).  Here the resident CTAs per SM of
 the standalone index kernel and of find_value, and the line length above
 which find_value gives a line a whole warp, are searched on a sample of the
 caller's workload: one knob at a time, each candidate timed with the
-library's CUDA-event phase times (index build + one query pass), the best
+library's CUDA-event phase times of one gpj_index_query_device pass (index
+build + queries; whole-file or chunk by chunk, the fourth knob), the best
 kept.  Results do not depend on these shapes, only speed does.
 
 The choice is stored per device (name and SM count) in a JSON file under
 $GPJSON_TUNING_DIR (default ~/.cache/gpjson_b200) and applied by
 `apply()`; the environment variables GPJSON_LONG_LINE_BYTES,
-GPJSON_QUERY_CTAS_PER_SM and GPJSON_INDEX_CTAS_PER_SM override it.
+GPJSON_QUERY_CTAS_PER_SM, GPJSON_INDEX_CTAS_PER_SM and GPJSON_CHUNK_TILES
+override it.
 """
 
 from __future__ import annotations
@@ -23,14 +25,16 @@ import statistics
 from collections.abc import Callable
 from pathlib import Path
 
-KNOBS = ("index_ctas_per_sm", "query_ctas_per_sm", "long_line_bytes")
+KNOBS = ("index_ctas_per_sm", "query_ctas_per_sm", "long_line_bytes", "chunk_tiles")
 ENV = {"long_line_bytes": "GPJSON_LONG_LINE_BYTES", "query_ctas_per_sm": "GPJSON_QUERY_CTAS_PER_SM",
-       "index_ctas_per_sm": "GPJSON_INDEX_CTAS_PER_SM"}
-# candidates per knob (0 = the library's default: the occupancy maximum, or 64 KiB)
+       "index_ctas_per_sm": "GPJSON_INDEX_CTAS_PER_SM", "chunk_tiles": "GPJSON_CHUNK_TILES"}
+# candidates per knob (0 = the library's default: the occupancy maximum, 64 KiB,
+# or whole-file passes)
 CANDIDATES = {
     "index_ctas_per_sm": [0, 1, 2, 3],
     "query_ctas_per_sm": [0, 1, 2, 3],
     "long_line_bytes": [0, 16384, 262144, -1],
+    "chunk_tiles": [0, 2048],
 }
 
 
@@ -132,20 +136,23 @@ def tune(gpjson, data, queries: list[str], levels: int, device: int = 0, repeats
     f = gpjson.from_device(dev.data_ptr(), dev.numel(), keepalive=dev)
     compiled = [gj.compile_path(q) for q in queries]
     lib, h = gpjson._native.lib, gpjson._native.h
+    f.build_index(levels)
+    slots = max(c.num_results for c in compiled)
+    out = torch.empty((len(compiled), f.num_lines, slots, 2), dtype=torch.int64, device=dev.device)
 
     def measure(setting: dict) -> float:
         gpjson.set_tuning(**setting)
-        f.build_index(levels)
-        f.run(compiled)  # warm
+        f.index_and_query_device(compiled, levels, out.data_ptr(), f.num_lines, slots)  # warm
         lib.gpj_reset_timings(h)
         for _ in range(repeats):
-            f.build_index(levels)
-            f.run(compiled)
+            f.index_and_query_device(compiled, levels, out.data_ptr(), f.num_lines, slots)
         phases = gpjson.timings()["phases"]
         per = {}
         for ph in phases:
             per.setdefault(ph["name"], []).append(ph["device_ms"])
-        return sum(statistics.mean(v) for k, v in per.items() if k in ("build_index", "find_value"))
+        # one pass = the sum of its phases (whole-file: index build + find_value)
+        return sum(statistics.mean(v) for k, v in per.items()
+                   if k in ("build_index", "find_value", "index_and_query"))
 
     try:
         best, seen = search(measure)

@@ -90,12 +90,22 @@ int gpj_set_stream(gpj_ctx *ctx, void *stream);
  *    whole warp each instead of one thread (0 = the default, 65536; -1 = never);
  *  - query_ctas_per_sm, index_ctas_per_sm: resident CTAs per SM of
  *    find_value and of the standalone index kernel (0 = the occupancy
- *    maximum; larger values are capped at it).
+ *    maximum; larger values are capped at it);
+ *  - chunk_tiles: gpj_index_query_device and gpj_query_paths build the index
+ *    and evaluate the queries chunk by chunk, chunks of this many 30 KiB
+ *    tiles (a multiple of 1024), so that find_value reads each chunk's index
+ *    from L2 right after it is written (0, the default = one index pass over
+ *    the whole file, then one find_value pass; on tweet-like NDJSON the
+ *    whole-file passes are faster, since find_value needs more lines than a
+ *    chunk holds to hide its load latency);
+ *  - reserved: 0.
  * gpjson_b200.tune (Python) measures and persists them per device. */
 typedef struct gpj_tuning {
     int64_t long_line_bytes;
     int32_t query_ctas_per_sm;
     int32_t index_ctas_per_sm;
+    int32_t chunk_tiles;
+    int32_t reserved;
 } gpj_tuning;
 
 int gpj_set_tuning(gpj_ctx *ctx, const gpj_tuning *tuning);

@@ -369,6 +369,50 @@ def test_pipelined_query_equals_load_then_query(gpjson, case):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", ["ndjson", "long_line", "raw_newline", "small", "many_lines"])
+def test_chunked_resident_pass_equals_whole_file_pass(gpjson, case):
+    """gpj_index_query_device with tuning.chunk_tiles (index kernel, newline
+    index and find_value chunk by chunk over input already on the device)
+    equals the whole-file pass, including inputs the chunks cannot index (a
+    line longer than a chunk, a raw newline in a string: indexed again
+    whole) and more lines than the first estimate; a too-small result
+    buffer is refused."""
+    import torch
+
+    data, paths = _pipelined_case(case)
+    compiled = [gj.compile_path(p) for p in paths]
+    levels = max(c.max_depth for c in compiled)
+    dev = torch.from_numpy(data).cuda()
+    f = gpjson.from_device(dev.data_ptr(), dev.numel(), keepalive=dev)
+    try:
+        f.build_index(levels)
+        want = f.run(compiled)
+        lines = f.num_lines
+        out = torch.full((len(compiled), lines, want.shape[2], 2), 7, dtype=torch.int64, device="cuda")
+        for chunk in (1024, 2048):
+            gpjson.set_tuning(chunk_tiles=chunk)
+            try:
+                for _ in range(2):
+                    out.fill_(7)
+                    f.index_and_query_device(compiled, levels, out.data_ptr(), lines)
+                    assert f.num_lines == lines
+                    assert np.array_equal(out.cpu().numpy(), want), (case, chunk)
+                if lines > 1:
+                    small = torch.empty((len(compiled), lines - 1, want.shape[2], 2), dtype=torch.int64,
+                                        device="cuda")
+                    with pytest.raises(gj.GPJSONException):
+                        f.index_and_query_device(compiled, levels, small.data_ptr(), lines - 1)
+            finally:
+                gpjson.set_tuning(chunk_tiles=0)
+        with pytest.raises(gj.GPJSONException):
+            gpjson.set_tuning(chunk_tiles=1000)  # not a multiple of 1024
+    finally:
+        f.release()
+    if case == "small":
+        assert np.array_equal(want, oracle.query(data.tobytes(), paths))
+
+
+@pytest.mark.gpu
 def test_index_union_extension(gpjson):
     """`[i,j]` is rejected as the reference rejects it unless the context
     enables PATH_INDEX_UNIONS; then each index has its own result slot, equal

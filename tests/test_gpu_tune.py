@@ -33,4 +33,4 @@ def test_tuner_picks_applies_and_stores(gpjson, tmp_path, monkeypatch):
         finally:
             f.release()
     finally:
-        gpjson.set_tuning(long_line_bytes=0, query_ctas_per_sm=0, index_ctas_per_sm=0)
+        gpjson.set_tuning(long_line_bytes=0, query_ctas_per_sm=0, index_ctas_per_sm=0, chunk_tiles=0)

@@ -10,7 +10,7 @@ from gpjson_b200 import tune
 
 
 def test_search_finds_the_minimum_of_a_separable_cost():
-    best_of = {"index_ctas_per_sm": 3, "query_ctas_per_sm": 2, "long_line_bytes": 262144}
+    best_of = {"index_ctas_per_sm": 3, "query_ctas_per_sm": 2, "long_line_bytes": 262144, "chunk_tiles": 2048}
     calls = []
 
     def cost(setting):
