@@ -29,27 +29,6 @@ GPJ_HD uint32_t byte_perm(uint32_t x, uint32_t y, uint32_t s) {
 #endif
 }
 
-// The same with bit 3 of a selector nibble honoured as PTX prmt's default
-// mode defines it: that result byte is the selected byte's bit 7 replicated
-// over all eight bits (a zero byte for a table byte below 0x80).
-GPJ_HD uint32_t byte_perm_sign(uint32_t x, uint32_t y, uint32_t s) {
-#ifdef __CUDA_ARCH__
-    uint32_t r;
-    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(y), "r"(s));
-    return r;
-#else
-    const uint64_t v = (static_cast<uint64_t>(y) << 32) | x;
-    uint32_t r = 0;
-    for (int i = 0; i < 4; i++) {
-        const uint32_t sel = (s >> (4 * i)) & 0xF;
-        uint32_t b = static_cast<uint32_t>((v >> (8 * (sel & 7))) & 0xFF);
-        if (sel & 8) b = (b & 0x80) ? 0xFF : 0x00;
-        r |= b << (8 * i);
-    }
-    return r;
-#endif
-}
-
 GPJ_HD int popc64(uint64_t x) {
 #ifdef __CUDA_ARCH__
     return __popcll(x);
@@ -114,39 +93,6 @@ struct ClassMasks {
     uint64_t colon;       // ':'
 };
 
-// Class bits of each byte of 32 bytes: the byte's high nibble h and low
-// nibble l look up one table each (PRMT with 4-bit selectors) and the
-// results AND together, so a class bit survives only for the (h, l) pairs
-// of its characters: '\n' 0A, ',' 2C, ':' 3A, '\\' 5C, '[' 5B and '{' 7B
-// (open), ']' 5D and '}' 7D (close).  Lookups are by h (0-7; a non-ASCII
-// byte, h >= 8, reads a sign-replicated zero) and by l ^ 8 (the low nibbles
-// A-D of these characters become 2-5; every other value either selects a
-// zero entry or reads a sign-replicated zero; byte_perm_sign).  '"' is the one character
-// with a low nibble below 8 and is found by a byte compare (bit 7).
-constexpr uint32_t kClsNewline = 1u << 0, kClsComma = 1u << 1, kClsColon = 1u << 2, kClsBackslash = 1u << 3,
-                   kClsOpen = 1u << 4, kClsClose = 1u << 5, kClsQuote = 1u << 7;
-// table by high nibble: entries 0-3 and 4-7
-constexpr uint32_t kHiTab0 = kClsNewline | (0u << 8) | (kClsComma << 16) | (kClsColon << 24);
-constexpr uint32_t kHiTab1 = 0u | ((kClsBackslash | kClsOpen | kClsClose) << 8) | (0u << 16) |
-                             ((kClsOpen | kClsClose) << 24);
-// table by low nibble ^ 8: entries 0-3 (l = 8, 9, A, B) and 4-7 (l = C, D, E, F)
-constexpr uint32_t kLoTab0 = 0u | (0u << 8) | ((kClsNewline | kClsColon) << 16) | (kClsOpen << 24);
-constexpr uint32_t kLoTab1 = (kClsComma | kClsBackslash) | (kClsClose << 8) | (0u << 16) | (0u << 24);
-
-// The four nibbles at bits 0-3, 8-11, 16-19, 24-27 of x packed into a PRMT
-// selector (bits 0-15).
-GPJ_HD uint32_t nibble_selector(uint32_t x) {
-    const uint32_t c = (x | (x >> 4)) & 0x00FF00FFu;
-    return byte_perm(c, 0, 0x3320);
-}
-
-GPJ_HD uint32_t class_bytes(uint32_t x) {
-    const uint32_t hi = nibble_selector((x >> 4) & 0x0F0F0F0Fu);
-    const uint32_t lo = nibble_selector((x ^ 0x08080808u) & 0x0F0F0F0Fu);
-    const uint32_t c = byte_perm_sign(kHiTab0, kHiTab1, hi) & byte_perm_sign(kLoTab0, kLoTab1, lo);
-    return c | eq_bytes(x, 0x22222222u);  // '"' at bit 7
-}
-
 // One step of the bit-matrix transpose: swaps bit rows of a and b at
 // distance s (bits of mask m of b with the bits s higher of a).
 GPJ_HD void swap_bits(uint32_t& a, uint32_t& b, int s, uint32_t m) {
@@ -156,19 +102,20 @@ GPJ_HD void swap_bits(uint32_t& a, uint32_t& b, int s, uint32_t m) {
 }
 
 // Classifies 32 bytes given as 8 little-endian u32 (v[j] = bytes 4j..4j+3).
-// The bytes are first transposed so that t[w] holds bytes {w, w+8, w+16,
-// w+24}; their class bytes form, in each byte lane k, an 8x8 bit matrix
-// (row w = t[w]'s class byte, column = class bit), transposed in three
-// rounds of swaps so that row c afterwards holds class c with byte 8k+w at
-// bit 8k+w: the class masks in byte order.
+// The bytes are first transposed so that r[w] holds bytes {w, w+8, w+16,
+// w+24}; in each byte lane k they form an 8x8 bit matrix (row w = byte
+// 8k+w, column = bit of the byte), transposed in three rounds of swaps so
+// that row b afterwards holds bit b of byte 8k+w at bit 8k+w: the eight bit
+// planes of the 32 bytes, in byte order.  Each class is then the AND of its
+// characters' bit pattern over the planes:
+//   '"' 0x22 = 0010 0010   ':' 0x3A = 0011 1010   '\n' 0x0A = 0000 1010
+//   ',' 0x2C = 0010 1100   '\\' 0x5C = 0101 1100
+//   '[' 0x5B, '{' 0x7B = 01x1 1011 (open)   ']' 0x5D, '}' 0x7D = 01x1 1101 (close)
 GPJ_HD void classify32(const uint32_t v[8], uint32_t& bs, uint32_t& qt, uint32_t& nl, uint32_t& op,
                        uint32_t& cl, uint32_t& st, uint32_t& cn) {
-    uint32_t t[8];
-    transpose4(v[0], v[2], v[4], v[6], t[0], t[1], t[2], t[3]);
-    transpose4(v[1], v[3], v[5], v[7], t[4], t[5], t[6], t[7]);
     uint32_t r[8];
-#pragma unroll
-    for (int w = 0; w < 8; w++) r[w] = class_bytes(t[w]);
+    transpose4(v[0], v[2], v[4], v[6], r[0], r[1], r[2], r[3]);
+    transpose4(v[1], v[3], v[5], v[7], r[4], r[5], r[6], r[7]);
 #pragma unroll
     for (int w = 0; w < 4; w++) swap_bits(r[w], r[w + 4], 4, 0x0F0F0F0Fu);
 #pragma unroll
@@ -178,13 +125,20 @@ GPJ_HD void classify32(const uint32_t v[8], uint32_t& bs, uint32_t& qt, uint32_t
     }
 #pragma unroll
     for (int w = 0; w < 8; w += 2) swap_bits(r[w], r[w + 1], 1, 0x55555555u);
-    nl = r[0];
-    cn = r[2];
-    bs = r[3];
-    op = r[4];
-    cl = r[5];
-    qt = r[7];
-    st = r[1] | r[2] | op | cl;  // ',' ':' and the brackets
+    const uint32_t p0 = r[0], p1 = r[1], p2 = r[2], p3 = r[3], p4 = r[4], p5 = r[5], p6 = r[6], p7 = r[7];
+    const uint32_t row0 = ~(p7 | p6);            // 0x00-0x3F
+    const uint32_t row1 = ~p7 & p6;              // 0x40-0x7F
+    const uint32_t low010 = ~p2 & p1 & ~p0;      // bits 2-0 = 010
+    const uint32_t low100 = p2 & ~(p1 | p0);     // bits 2-0 = 100
+    qt = row0 & p5 & ~(p4 | p3) & low010;
+    cn = row0 & p5 & p4 & p3 & low010;
+    nl = row0 & ~(p5 | p4) & p3 & low010;
+    const uint32_t cm = row0 & p5 & ~p4 & p3 & low100;
+    bs = row1 & ~p5 & p4 & p3 & low100;
+    const uint32_t br = row1 & p4 & p3 & p0;     // bits 1-2 tell open from close
+    op = br & ~p2 & p1;
+    cl = br & p2 & ~p1;
+    st = cm | cn | op | cl;  // ',' ':' and the brackets
 }
 
 GPJ_HD ClassMasks classify64(const uint32_t v[16]) {
