@@ -977,8 +977,8 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
 // cross-warp scan and the tile's bookkeeping are paid once per four words.
 // What a word's classification leaves for the second pass (its masks and
 // level changes) is kept in shared memory where the word's bytes were, so
-// the slot holds bytes, then masks, then the level split's inputs, and four
-// CTAs fit per SM.  The level split deals the warp's words that hold
+// the slot holds bytes, then masks, then the level split's inputs and (up
+// to four levels) the level masks, and six CTAs fit per SM.  The level split deals the warp's words that hold
 // bracket cuts over its lanes (deal_levels).  Writes the string index, the ':'
 // bitmap, the leveled bitmaps and the '\n' bitmap with one 32-byte store per
 // thread and bitmap where all four words are its own, and every tile's
@@ -996,13 +996,20 @@ constexpr int kWSlotWords = static_cast<int>(kWSlot / 64);           // 512
 constexpr int64_t kWRound = kWThreads * 64;                // extension rounds: one word per thread
 static_assert(kWTile % kWLaneBytes == 0 && kWSlot - kWTile == kExtBytes, "tile + 2 KiB look-ahead per slot");
 
+// With at most four levels a word's level masks go into cells 0-3 of the
+// word itself (word_cell) once the level split has read them; with more
+// they need an array of their own, which lowers the CTAs per SM.
+template <int LV>
+constexpr bool kCellLevels = LV <= 4;
+
 template <int LV>
 struct WShared {
     // the tile's bytes (TMA destination); after a word is classified, its
     // 64 bytes hold eight 8-byte cells of its state (word_cell)
     uint8_t bytes[kWSlot];
     union {
-        uint64_t acc[LV][kWSlotWords];    // level masks, at i * kWThreads + thread (deal_levels)
+        // level masks, at i * kWThreads + thread (deal_levels); unused with kCellLevels
+        uint64_t acc[kCellLevels<LV> ? 1 : LV][kCellLevels<LV> ? 1 : kWSlotWords];
         uint64_t lvacc[kWWarps][LV][32];  // split_levels_warp in the extension rounds
     };
     TileFile desc[2];  // the file of tile k in desc[k & 1]
@@ -1021,7 +1028,9 @@ struct WShared {
 // state after a reset.  Second pass: 0 opening brackets, 1 closing
 // brackets, 2 structural bytes, 3 level at the word's first byte, all of
 // the word's own and outside strings; 4 string mask, 5 '\n' as before,
-// 6 ':' outside strings.
+// 6 ':' outside strings.  With kCellLevels, cells 0-3 then hold the masks
+// of levels 0-3: written in the second pass for a word without bracket
+// cuts, by deal_levels for a word with some.
 __device__ __forceinline__ uint64_t* word_cell(uint8_t* slot, int g, int i, int c) {
     return reinterpret_cast<uint64_t*>(slot + kWLaneBytes * g + 64 * i + 8 * ((c + g) & 7));
 }
@@ -1051,8 +1060,8 @@ __device__ __forceinline__ void start_wide_tile(const IndexParams& p, WShared<LV
 }
 
 // The level split of the warp's words that hold bracket cuts (inputs in
-// cells 0-3 of each word; sh.acc already holds every word's masks as if it
-// had none): such words are dealt out over the 32 lanes, one per lane per
+// cells 0-3 of each word; the other words' level masks are already in
+// place, sh.acc or their cells 0-3): such words are dealt out over the 32 lanes, one per lane per
 // pass, and each is split by split_levels, which walks its cuts.  A
 // quarter of the words have cuts and their counts differ a lot (tweets: 0.87
 // per word on average, many with eight or more), so dealing them over the
@@ -1095,7 +1104,12 @@ __device__ __forceinline__ void deal_levels(WShared<LV>& sh, unsigned cmask) {
             uint64_t lv[LV];
             split_levels<LV>(op, cl, st, dd, lv);
 #pragma unroll
-            for (int l = 0; l < LV; l++) sh.acc[l][wi * kWThreads + og] = lv[l];
+            for (int l = 0; l < LV; l++) {
+                if constexpr (kCellLevels<LV>)
+                    *word_cell(sh.bytes, og, wi, l) = lv[l];
+                else
+                    sh.acc[l][wi * kWThreads + og] = lv[l];
+            }
         }
     }
     __syncwarp();
@@ -1172,8 +1186,10 @@ __device__ void extend_long_line(const IndexParams& p, const TileFile& F, WShare
     }
 }
 
+// Up to four levels: 6 CTAs per SM (about 37 KiB of shared memory each,
+// at most 85 registers a thread); more levels add the level-mask array.
 template <int LV>
-__global__ void __launch_bounds__(kWThreads, LV <= 4 ? 4 : (LV <= 8 ? 3 : 2)) tile_index_kernel(IndexParams p) {
+__global__ void __launch_bounds__(kWThreads, LV <= 4 ? 6 : (LV <= 8 ? 3 : 2)) tile_index_kernel(IndexParams p) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
     WShared<LV>& sh = *reinterpret_cast<WShared<LV>*>(smem_raw);
     const int tid = threadIdx.x;
@@ -1209,7 +1225,9 @@ __global__ void __launch_bounds__(kWThreads, LV <= 4 ? 4 : (LV <= 8 ? 3 : 2)) ti
         for (int i = 0; i < kWK; i++) {
             const int64_t ws = lane_start + 64 * i;
             const uint64_t valid = bits_between(0, vend - ws);
-            ClassMasks m = load_classify(slot, kWK * tid + i);
+            // the thread's words are 256 bytes apart from the next thread's,
+            // so a rotation by word would be the same for every thread
+            ClassMasks m = load_classify<false>(slot, kWK * tid + i);
             if (valid != ~0ull) restrict_masks(m, valid);
             uint32_t cout = 0;
             const uint64_t esc = (m.backslash | cin) ? escaped_mask(m.backslash, cin, &cout) : 0ull;
@@ -1313,17 +1331,25 @@ __global__ void __launch_bounds__(kWThreads, LV <= 4 ? 4 : (LV <= 8 ? 3 : 2)) ti
             const uint64_t sk = split ? ~0ull : 0ull;
             const uint64_t op = open & sk, cl = close & sk, st = wst & keep & ~in_str & sk;
             const int dd = d_in > 128 ? 128 : (d_in < -128 ? -128 : d_in);
-            *word_cell(slot, tid, i, 0) = op;
-            *word_cell(slot, tid, i, 1) = cl;
-            *word_cell(slot, tid, i, 2) = st;
-            *word_cell(slot, tid, i, 3) = static_cast<uint64_t>(static_cast<int64_t>(dd));
-            *word_cell(slot, tid, i, 4) = in_str;
-            *word_cell(slot, tid, i, 6) = wcolon & keep & ~in_str;
+            const bool cut = (op | (cl << 1)) != 0;
             // a word without bracket cuts is all at its first level (words
             // with cuts are split by deal_levels)
+            if (kCellLevels<LV> && !cut) {
 #pragma unroll
-            for (int l = 0; l < LV; l++) sh.acc[l][i * kWThreads + tid] = dd == l ? st : 0ull;
-            cmask |= (op | (cl << 1)) ? (1u << i) : 0u;
+                for (int l = 0; l < LV; l++) *word_cell(slot, tid, i, l) = dd == l ? st : 0ull;
+            } else {
+                *word_cell(slot, tid, i, 0) = op;
+                *word_cell(slot, tid, i, 1) = cl;
+                *word_cell(slot, tid, i, 2) = st;
+                *word_cell(slot, tid, i, 3) = static_cast<uint64_t>(static_cast<int64_t>(dd));
+                if constexpr (!kCellLevels<LV>) {
+#pragma unroll
+                    for (int l = 0; l < LV; l++) sh.acc[l][i * kWThreads + tid] = dd == l ? st : 0ull;
+                }
+            }
+            *word_cell(slot, tid, i, 4) = in_str;
+            *word_cell(slot, tid, i, 6) = wcolon & keep & ~in_str;
+            cmask |= cut ? (1u << i) : 0u;
             wmask |= split ? (1u << i) : 0u;
             // the state at the next word's first byte
             if (has_nl && !ahead) {
@@ -1365,7 +1391,12 @@ __global__ void __launch_bounds__(kWThreads, LV <= 4 ? 4 : (LV <= 8 ? 3 : 2)) ti
             for (int l = 0; l < LV; l++) {
                 if (l < p.num_levels) {
 #pragma unroll
-                    for (int i = 0; i < kWK; i++) v[i] = sh.acc[l][i * kWThreads + tid];
+                    for (int i = 0; i < kWK; i++) {
+                        if constexpr (kCellLevels<LV>)
+                            v[i] = *word_cell(slot, tid, i, l);
+                        else
+                            v[i] = sh.acc[l][i * kWThreads + tid];
+                    }
                     store_words4(F.leveled + F.level_size * l + w0, v, wmask);
                 }
             }

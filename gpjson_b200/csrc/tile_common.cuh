@@ -21,11 +21,13 @@ __device__ __forceinline__ uint64_t bits_between(int64_t lo, int64_t hi) {
     return upper & ~lower;
 }
 
-// Loads word `w` (64 bytes at buf + 64w) and classifies it.  The two
-// 32-byte halves are read in a thread-dependent order so a quarter-warp of
-// 16-byte loads spreads over more banks; the halves are put back in place.
+// Loads word `w` (64 bytes at buf + 64w) and classifies it.  With kRotate
+// (consecutive threads on consecutive words) the two 32-byte halves are read
+// in a thread-dependent order so a quarter-warp of 16-byte loads spreads
+// over more banks; the halves are put back in place.
+template <bool kRotate = true>
 __device__ __forceinline__ ClassMasks load_classify(const uint8_t* buf, int w) {
-    const int rot = (w >> 1) & 1;
+    const int rot = kRotate ? (w >> 1) & 1 : 0;
     const uint4* src = reinterpret_cast<const uint4*>(buf + 64 * w);
     uint32_t v[16];
     const uint4 q0 = src[2 * rot], q1 = src[2 * rot + 1];
