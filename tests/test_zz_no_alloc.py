@@ -81,7 +81,13 @@ def test_noalloc_matches_context_entry(gpjson, kind, levels):
     data = datagen.tweets(8 << 20).tobytes() if kind == "ndjson" else pretty_json(7, 3000)
     n = len(data)
     d_file = torch.frombuffer(bytearray(data), dtype=torch.uint8).cuda()
+    before = gpjson.timings()["exact_index_fallbacks"]
     want = build(gpjson, torch, d_file, n, levels, noalloc=False)
+    # the pretty input is one the line-parallel kernel flags: the context
+    # entry needed the exact kernel, so the no-alloc entry's equal result
+    # shows that its own fallback ran
+    fallbacks = gpjson.timings()["exact_index_fallbacks"] - before
+    assert (fallbacks >= 1) if kind == "pretty" else (fallbacks == 0)
     first = build(gpjson, torch, d_file, n, levels, noalloc=True)
     second = build(gpjson, torch, d_file, n, levels, noalloc=True)
     assert_same(first, want)
@@ -106,6 +112,40 @@ def test_noalloc_alternates_inputs(gpjson):
     for _ in range(2):
         assert_same(build(gpjson, torch, da, len(a), 8, noalloc=True), want_a)
         assert_same(build(gpjson, torch, db, len(b), 8, noalloc=True), want_b)
+
+
+@pytest.mark.gpu
+def test_noalloc_epoch_wrap(gpjson):
+    """The tile states in the static scratch carry the launch's 16-bit epoch
+    and are cleared when it wraps.  2 x 65,536 + 16 builds alternate two
+    multi-tile inputs, so every epoch value is used again after the wrap by
+    the other input (the cycle of 65,535 values is odd): a tile state left
+    from before the wrap would be taken for the current launch's and shift
+    the other input's newline offsets.  Every build must equal its input's
+    build through the context entry."""
+    import torch
+
+    lib = gpjson._native.lib
+    inputs = []
+    for seed, size in ((41, 192 << 10), (42, 160 << 10)):
+        data = datagen.tweets(size, seed=datagen.SEED_BASE + seed).tobytes()
+        d_file = torch.frombuffer(bytearray(data), dtype=torch.uint8).cuda()
+        want = build(gpjson, torch, d_file, len(data), 4, noalloc=False)
+        d_str, d_lvl, d_nl = device_buffers(torch, len(data), 4)
+        inputs.append((d_file, len(data), want[0], torch.from_numpy(want[1]).cuda(), d_str, d_lvl, d_nl))
+    assert inputs[0][2] != inputs[1][2]
+    stream = torch.cuda.current_stream().cuda_stream
+    torch.cuda.synchronize()
+    lines = ctypes.c_int64(-1)
+    for k in range(2 * 65536 + 16):
+        d_file, n, want_lines, want_nl, d_str, d_lvl, d_nl = inputs[k & 1]
+        rc = lib.gpj_build_index_device_noalloc(
+            ctypes.c_void_p(stream), d_file.data_ptr(), n, 4, d_str.data_ptr(), d_lvl.data_ptr(), d_nl.data_ptr(),
+            d_nl.numel(), ctypes.byref(lines),
+        )
+        assert rc == 0, (k, rc)
+        assert lines.value == want_lines, k
+        assert torch.equal(d_nl[:want_lines], want_nl), k
 
 
 @pytest.mark.gpu
