@@ -610,7 +610,8 @@ int launch_query(gpj_ctx* ctx, gpj_file* f, int nq, int slots, int64_t* d_out, i
     p.long_lines = long_lines(ctx);
     if (p.long_lines.items)
         GPJ_CUDA(ctx, cudaMemsetAsync(ctx->d_long_count, 0, sizeof(unsigned long long), stream));
-    const int64_t want = d_range ? INT64_MAX : (gpj::query_items(f->num_lines, nq) + 255) / 256;
+    const int64_t want =
+        d_range ? INT64_MAX : (gpj::query_items(f->num_lines, nq) + gpj::kQueryThreads - 1) / gpj::kQueryThreads;
     const int64_t grid = std::max<int64_t>(
         1, std::min<int64_t>(want, static_cast<int64_t>(ctx->sms) * query_occupancy(ctx, f->ir_depth)));
     GPJ_CUDA(ctx, gpj::launch_find_value(p, static_cast<int>(grid), ctx->sms * 2, stream));
@@ -2089,7 +2090,7 @@ int gpj_batch_run(gpj_batch* b) {
         // the query phase: captured as a graph (kept for the next run) when
         // the stream allows it, else launched directly
         const int64_t grid = std::max<int64_t>(
-            1, std::min<int64_t>((total_items + 255) / 256,
+            1, std::min<int64_t>((total_items + gpj::kQueryThreads - 1) / gpj::kQueryThreads,
                                  static_cast<int64_t>(ctx->sms) * query_occupancy(ctx, depth)));
         const gpj::LongLines ll = long_lines(ctx);
         auto query_phase = [&]() -> cudaError_t {

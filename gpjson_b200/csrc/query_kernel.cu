@@ -131,7 +131,7 @@ __device__ __forceinline__ void run_long_line(const LineView& view, int64_t star
 // D: level slots of the interpreter's register state (level_slots_for_depth
 // of the deepest query of the launch).
 template <int D>
-__global__ void __launch_bounds__(256) find_value_kernel(QueryParams p) {
+__global__ void __launch_bounds__(kQueryThreads, kQueryMinCtas<D>) find_value_kernel(QueryParams p) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     LineView view{p.file, p.n, p.string_index, p.leveled, p.level_size, p.n, p.colon};
     const int64_t per_line = 2 * static_cast<int64_t>(p.slots);
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(256) find_value_long_kernel(QueryParams p) {
 }
 
 template <int D>
-__global__ void __launch_bounds__(256) find_value_batch_kernel(const QueryFile* files, int nfiles,
+__global__ void __launch_bounds__(kQueryThreads, kQueryMinCtas<D>) find_value_batch_kernel(const QueryFile* files, int nfiles,
                                                                 int64_t total_items, LongLines long_lines) {
     const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
     for (int64_t g = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; g < total_items; g += stride) {
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256) find_value_batch_long_kernel(const QueryF
 template <int D>
 cudaError_t launch_batch_d(const QueryFile* files, int nfiles, int64_t total_items, const LongLines& L, int grid,
                            int long_grid, cudaStream_t stream) {
-    find_value_batch_kernel<D><<<grid, 256, 0, stream>>>(files, nfiles, total_items, L);
+    find_value_batch_kernel<D><<<grid, kQueryThreads, 0, stream>>>(files, nfiles, total_items, L);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && L.items) {
         find_value_batch_long_kernel<D><<<long_grid, 256, 0, stream>>>(files, L);
@@ -248,7 +248,7 @@ cudaError_t launch_batch_d(const QueryFile* files, int nfiles, int64_t total_ite
 
 template <int D>
 cudaError_t launch_d(const QueryParams& p, int grid, int long_grid, cudaStream_t stream) {
-    find_value_kernel<D><<<grid, 256, 0, stream>>>(p);
+    find_value_kernel<D><<<grid, kQueryThreads, 0, stream>>>(p);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess && p.long_lines.items) {
         find_value_long_kernel<D><<<long_grid, 256, 0, stream>>>(p);
@@ -287,13 +287,13 @@ int find_value_max_ctas_per_sm(int depth) {
     cudaError_t e;
     switch (level_slots_for_depth(depth)) {
         case 5:
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel<5>, 256, 0);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel<5>, kQueryThreads, 0);
             break;
         case 9:
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel<9>, 256, 0);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel<9>, kQueryThreads, 0);
             break;
         default:
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel<kLevelSlots>, 256, 0);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, find_value_kernel<kLevelSlots>, kQueryThreads, 0);
     }
     return e == cudaSuccess ? blocks : -1;
 }

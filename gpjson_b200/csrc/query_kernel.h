@@ -28,6 +28,15 @@ struct LongLines {
     int64_t bytes;
 };
 
+// Threads per CTA of find_value_kernel and find_value_batch_kernel (a
+// multiple of 32; grids are sized in these CTAs), and the CTAs per SM their
+// register budget is set for, by register-state size D: 7 (at most 72
+// registers) for D = 5, 6 for D = 9, 4 for D = 17.  128-thread CTAs at 72
+// registers keep 28 warps per SM resident where 256-thread CTAs at 80 kept 24.
+constexpr int kQueryThreads = 128;
+template <int D>
+constexpr int kQueryMinCtas = D <= 5 ? 7 : (D <= 9 ? 6 : 4);
+
 struct QueryParams {
     const uint8_t* file;
     int64_t n;

@@ -31,8 +31,8 @@ ENV = {"long_line_bytes": "GPJSON_LONG_LINE_BYTES", "query_ctas_per_sm": "GPJSON
 # candidates per knob (0 = the library's default: the occupancy maximum, 64 KiB,
 # or whole-file passes)
 CANDIDATES = {
-    "index_ctas_per_sm": [0, 1, 2, 3],
-    "query_ctas_per_sm": [0, 1, 2, 3],
+    "index_ctas_per_sm": [0, 2, 3, 4],
+    "query_ctas_per_sm": [0, 2, 4, 6],
     "long_line_bytes": [0, 16384, 262144, -1],
     "chunk_tiles": [0, 2048],
 }
