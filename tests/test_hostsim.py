@@ -135,12 +135,16 @@ def test_interpreter_matches_oracle(hostsim):
         b'{"a": \n' + b" " * 90 + b'1}',  # a value's whitespace runs on into the next line
         # deep enough for every size of the interpreter's register state
         b'{"p":{"q":[[{"r":{"s":[0,{"t":{"u":[1,2,{"v":{"w":"deep"}}]}}]}}]]}}',
+        # a key check that starts before the key's own string (at the
+        # previous string's closing quote) and one at an escaped quote
+        b'{"cd","ab":1, "e\\"lang":2, "lang":3}',
     ]
     paths = [
         "$.user.lang", "$.user.values[2]", "$.user.values[0:3]", "$.a.a", "$.a[1][0]", "$.a[2].b",
         "$.c.d[0]", "$.c.d[0:2]", "$.user.lang[?(@ == 'nl')]", "$[0]", "$.b.a", "$.a[0].b[2].c",
         "$.key[0]", "$.x.y[1][0]", "$.x.y[0:2]", "$['k\\\"ey']", "$.d", "$.a", "$.b[0]",
         "$.p.q[0][0].r.s[1].t.u[2].v.w", "$.p.q[0][0].r.s[0:2]", "$.p.q[0][0].r.s[1].t.u[0:3]",
+        "$[',\"ab']", "$.lang", "$['\"lang']",
     ]
     for trial in range(40):
         lines = [rng.choice(base) for _ in range(rng.randint(1, 20))]
