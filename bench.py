@@ -34,7 +34,7 @@ sys.path.insert(0, str(ROOT))
 QUERIES = ["$.user.lang", "$.id", "$.user.followers_count", "$.entities.hashtags[0].text"]
 FILE_BYTES = 1 << 31
 LEVELS = 4
-PROFILE_TRAFFIC = ROOT / "profiles" / "dram_traffic_tweets_256MiB.json"
+PROFILE_TRAFFIC = ROOT / "profiles" / "dram_traffic_index_kernels_256MiB.json"
 
 
 class Workload:
@@ -194,8 +194,10 @@ def measured_peak_gbs() -> tuple[float, str]:
 
 
 def ncu_traffic(key: str):
-    """DRAM bytes per launch of the index kernel from the committed ncu
-    summary (profiles/dram_traffic_tweets_256MiB.json), scaled to this input size."""
+    """DRAM bytes of one launch of an index kernel (`key`) and the input
+    bytes it processed, from the committed ncu summary
+    (profiles/dram_traffic_index_kernels_256MiB.json); the caller scales them
+    to its input size."""
     if not PROFILE_TRAFFIC.exists():
         return None
     try:
@@ -389,6 +391,7 @@ def measure_file(args, w: Workload, rank: int, world: int, local: int, device) -
 
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
     launches0 = g.kernel_launches()
+    exact0 = g.timings()["exact_index_fallbacks"]
     lib.gpj_reset_timings(ctx)
     clocks = ClockSampler(local)
     clocks.start()
@@ -404,6 +407,7 @@ def measure_file(args, w: Workload, rank: int, world: int, local: int, device) -
     barrier(world, device)
     clock_info = clocks.stop()
     launches = g.kernel_launches() - launches0
+    exact_builds = g.timings()["exact_index_fallbacks"] - exact0
     # per-kernel device times: the library brackets each kernel phase with
     # CUDA events on this same stream (gpj_get_timings)
     phase_ms: dict[str, list[float]] = {}
@@ -493,9 +497,22 @@ def measure_file(args, w: Workload, rank: int, world: int, local: int, device) -
     dom = "index_and_query" if "index_and_query" in kernel_ms else "build_index"
     dom_ms = kernel_ms[dom]
     achieved = n / (dom_ms / 1000) / 1e9
+    # which kernel the timed builds ran: the exact kernel for input the line
+    # kernels refuse, else the standalone tile kernel (or the line kernel with
+    # the queries, or the chunked pass's kernels)
+    if exact_builds > 0:
+        dom_kernel = "index_kernel (exact, decoupled look-back; the line kernels refuse this input)"
+    elif dom == "build_index":
+        dom_kernel = "tile_index_kernel (+ the two newline index kernels)"
+    elif args.mode == "fused":
+        dom_kernel = "line_index_kernel (with the queries)"
+    else:
+        dom_kernel = "chunked pass: tile_index_kernel, newline index and find_value per chunk"
     traffic = None
-    t = ncu_traffic("index_kernel")
-    if t and t.get("bytes") and t.get("input_bytes"):
+    # the committed captures: the standalone tile kernel's build of tweets,
+    # the exact kernel's build of the adversarial file
+    t = ncu_traffic("exact_index_kernel" if exact_builds > 0 else "index_kernel")
+    if dom == "build_index" and t and t.get("bytes") and t.get("input_bytes"):
         traffic = round(t["bytes"] * n / t["input_bytes"])
 
     result = {
@@ -525,8 +542,7 @@ def measure_file(args, w: Workload, rank: int, world: int, local: int, device) -
         "kernels_ms": {k: round(v, 4) for k, v in kernel_ms.items()},
         "roofline": {
             "bound": "hbm",
-            "kernel": ("line_index_kernel (with the queries)" if dom == "index_and_query"
-                       else "tile_index_kernel (+ the two newline index kernels)"),
+            "kernel": dom_kernel,
             "achieved": round(achieved, 1),
             "peak": peak,
             "unit": "GB/s",

@@ -245,8 +245,12 @@ __device__ int64_t claim_and_load(const IndexParams& p, Shared& sh, int b) {
     return t;
 }
 
+// Bound by the latency of the tile's copy and its look-back, so resident
+// CTAs matter more than registers: 6 per SM (shared memory's limit with two
+// 16 KiB buffers) for up to eight levels, though ptxas then spills a few
+// bytes; 4 with 16 levels, whose level array would spill much more.
 template <int LV>
-__global__ void __launch_bounds__(kThreads) index_kernel(IndexParams p) {
+__global__ void __launch_bounds__(kThreads, LV <= 8 ? 6 : 4) index_kernel(IndexParams p) {
     __shared__ Shared sh;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
