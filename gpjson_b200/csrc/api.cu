@@ -681,10 +681,9 @@ int index_pass(gpj_ctx* ctx, gpj_file* f, int num_levels, const FusedQueries* fq
     return GPJ_OK;
 }
 
-// Bytes copied per step of load_and_index: 2048 standalone-kernel tiles
+// Tiles copied per step of load_and_index: 2048 standalone-kernel tiles
 // (60 MiB), a whole number of the newline scan's 1024-tile blocks.
 constexpr int64_t kLoadTiles = 2048;
-constexpr int64_t kLoadChunk = gpj::kStandaloneTileBytes * kLoadTiles;
 
 // Queries load_and_index evaluates on each chunk's lines as soon as their
 // index is complete (bytecode uploaded; results strided by out_lines).

@@ -621,31 +621,26 @@ __device__ __forceinline__ void start_tile(const IndexParams& p, Sh& sh, int64_t
 }
 
 // ---- index warps -------------------------------------------------------------
-// kLines: line warps run beside these warps (FShared: newline index by
-// look-back, in-kernel queries); otherwise the kernel is these warps alone
-// (TShared) and writes the newline bitmap and per-tile newline counts, from
-// which newline_index.cu builds the newline index.
-template <int LV, bool kLines, class Sh>
-__device__ void index_warps(const IndexParams& p, Sh& sh) {
+// The line kernel's warps 0-7: the tile's masks into a mask slot for the
+// line warps that run beside them (newline index by look-back, in-kernel
+// queries), and the index to device memory.
+template <int LV>
+__device__ void index_warps(const IndexParams& p, FShared<LV>& sh) {
     const int tid = threadIdx.x;  // 0..255
     unsigned long long* nl_agg = p.tile_state;
     const int64_t first_tile = p.tile_begin + blockIdx.x, stride = gridDim.x;
     if (tid == 0 && first_tile < p.tile_end) start_tile(p, sh, first_tile, 0, 0);
     int64_t k = 0;
     for (int64_t t = first_tile; t < p.tile_end; t += stride, ++k) {
-        constexpr int kSlots = Sh::kByteSlots;
+        constexpr int kSlots = FShared<LV>::kByteSlots;
         const int bs = static_cast<int>(k % kSlots), ds = static_cast<int>(k % kRing), ms = static_cast<int>(k & 1);
         const uint32_t buse = static_cast<uint32_t>(k / kSlots), muse = static_cast<uint32_t>(k >> 1);
         // start the copy of the next tile: its byte slot was last used kSlots
-        // tiles ago (two in the standalone kernel: tile k-1, whose bytes no
-        // thread reads after that tile's last barrier)
+        // tiles ago, once the line warps are done with its bytes
         if (tid == 0 && t + stride < p.tile_end) {
             const int nb = static_cast<int>((k + 1) % kSlots);
             const uint32_t nuse = static_cast<uint32_t>((k + 1) / kSlots);
-            if constexpr (kLines) {
-                if (nuse > 0 && !mbar_wait_idle(&sh.bfree[nb], (nuse - 1) & 1))
-                    atomicOr(p.status + 1, kErrCopyTimeout);
-            }
+            if (nuse > 0 && !mbar_wait_idle(&sh.bfree[nb], (nuse - 1) & 1)) atomicOr(p.status + 1, kErrCopyTimeout);
             start_tile(p, sh, t + stride, nb, static_cast<int>((k + 1) % kRing));
         }
         if (!mbar_wait_bounded(&sh.full[bs], buse & 1) && tid == 0) atomicOr(p.status + 1, kErrCopyTimeout);
@@ -662,7 +657,7 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
         // One scan gives the tile's line starts, newline counts and every
         // word's state; the look-ahead words finish the tile's last line.
         const bool ahead = tid >= kTileWords;  // a word past the tile end
-        const int slot = kLines ? tid : -1;    // masks kept in shared memory for the line warps
+        const int slot = tid;                  // masks kept in shared memory for the line warps
         const uint64_t valid = bits_between(0, (ahead ? loaded_end : tile_end) - ws);
         ClassMasks m = load_classify(buf, tid);
         if (valid != ~0ull) restrict_masks(m, valid);
@@ -706,14 +701,10 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
         const int tile_nl = sc.nl_total & 0xFFFF;
         const int ahead_nl = sc.nl_total >> 16;
         const bool lines_here = sc.lines_here != 0;  // a line starts in this tile
-        if constexpr (kLines) {
-            if (tid == 0) st_release(nl_agg + t, tag48(p.epoch, static_cast<unsigned long long>(tile_nl)));
-            // the mask slot was last used two tiles ago
-            if (muse > 0 && !mbar_wait_idle(&sh.mfree[ms], (muse - 1) & 1) && tid == 0)
-                atomicOr(p.status + 1, kErrCopyTimeout);
-        } else {
-            if (tid == 0) p.tile_newlines[t] = tile_nl;
-        }
+        if (tid == 0) st_release(nl_agg + t, tag48(p.epoch, static_cast<unsigned long long>(tile_nl)));
+        // the mask slot was last used two tiles ago
+        if (muse > 0 && !mbar_wait_idle(&sh.mfree[ms], (muse - 1) & 1) && tid == 0)
+            atomicOr(p.status + 1, kErrCopyTimeout);
         // What this CTA finishes of the word, from which state; the branches
         // only choose it, so that finish_word runs converged below.
         bool act = false, own = true;
@@ -722,18 +713,14 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
         int ws_in = sc.s;
         int64_t wd_in = sc.d;
         if (!ahead) {
-            if constexpr (kLines) {
-                const int excl = sc.nl_before & 0xFFFF;
-                sh.nlmask[ms][tid] = m.newline;
-                sh.nlexcl[ms][tid] = excl;
-                uint64_t nm = m.newline;
-                int q = excl;
-                while (nm && q < kMaxTileLines) {
-                    sh.nlpos[ms][q++] = 64 * tid + ctz64(nm);
-                    nm &= nm - 1;
-                }
-            } else {
-                if (ws < tile_end) F.newline_bits[ws >> 6] = m.newline;
+            const int excl = sc.nl_before & 0xFFFF;
+            sh.nlmask[ms][tid] = m.newline;
+            sh.nlexcl[ms][tid] = excl;
+            uint64_t nm = m.newline;
+            int q = excl;
+            while (nm && q < kMaxTileLines) {
+                sh.nlpos[ms][q++] = 64 * tid + ctz64(nm);
+                nm &= nm - 1;
             }
             if (sc.reset) {
                 // every byte of the word belongs to lines that start in this tile
@@ -758,7 +745,7 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
             act = !(has_nl && f == 0);
             check = has_nl ? (1ull << f) : 0ull;
         }
-        finish_word<LV, kLines>(p, F, sh, ms, wm, wp0, ws_in, wd_in, ws >> 6, own, slot, valid, check, act);
+        finish_word<LV, true>(p, F, sh, ms, wm, wp0, ws_in, wd_in, ws >> 6, own, slot, valid, check, act);
         group_sync(kBarIndex, kIndexThreads);  // the tile's masks are complete in the slot
 
         const int64_t a_t = lt == 0 ? 0 : (lines_here ? sh.first_line : kNone);
@@ -824,8 +811,8 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                     const Span cex = index_scan_span(csp, sh.span_scratch, &ctotal);
                     const uint64_t ccheck =
                         (b_t >= cw && b_t < cw + 64) ? (c.newline & (1ull << (b_t - cw))) : 0ull;
-                    finish_word<LV, kLines>(p, F, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
-                                            cw >> 6, true, -1, cvalid, ccheck, cvalid != 0);
+                    finish_word<LV, true>(p, F, sh, ms, c, cp0, s ^ cex.q, d + (s ? (cex.ddt - cex.dd0) : cex.dd0),
+                                          cw >> 6, true, -1, cvalid, ccheck, cvalid != 0);
                     if (tid == kIndexThreads - 1) sh.carry_esc = static_cast<int>(ccout);
                     group_sync(kBarIndex, kIndexThreads);
                     esc = sh.carry_esc;
@@ -835,19 +822,14 @@ __device__ void index_warps(const IndexParams& p, Sh& sh) {
                 }
             }
         }
-        if constexpr (kLines) {
-            if (tid == 0) {
-                SlotInfo& in = sh.info[ms];
-                in.a = a_t;
-                in.b = b_t;
-                in.hi = hi;
-                in.tile_nl = tile_nl;
-                in.byte_slot = bs;
-                mbar_arrive(&sh.mready[ms]);  // the masks were complete at the barrier above
-            }
-        } else {
-            (void)a_t;
-            (void)hi;
+        if (tid == 0) {
+            SlotInfo& in = sh.info[ms];
+            in.a = a_t;
+            in.b = b_t;
+            in.hi = hi;
+            in.tile_nl = tile_nl;
+            in.byte_slot = bs;
+            mbar_arrive(&sh.mready[ms]);  // the masks were complete at the barrier above
         }
     }
 }
@@ -963,7 +945,7 @@ __global__ void __launch_bounds__(kThreads, 2) line_index_kernel(IndexParams p) 
     }
     __syncthreads();
     if (threadIdx.x < kIndexThreads)
-        index_warps<LV, true>(p, sh);
+        index_warps<LV>(p, sh);
     else
         line_warps<LV>(p, sh);
 }
