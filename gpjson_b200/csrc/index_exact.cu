@@ -20,7 +20,10 @@
 //    look-back, which supplies the string state, level counter and newline
 //    count before the tile (the carries the reference scans on the host).
 //  * Each thread then writes its string-index word, its words of the
-//    leveled bitmaps and its newline offsets.
+//    leveled bitmaps and its newline offsets: one tile later, from the
+//    word's state kept in its own bytes of the tile buffer, while warp 0
+//    looks back for the next tile (the look-back's wait overlaps the
+//    stores of the tile before).
 //
 // Output layouts are the reference's: string_index u64[ceil(n/64)],
 // leveled u64[num_levels][ceil(n/64)], newline index i64[lines] with [0]=0.
@@ -216,14 +219,91 @@ __device__ Carry look_back(unsigned long long* states, int64_t t, const Span& ag
 }
 
 struct __align__(128) Shared {
+    // a tile's bytes (TMA destination); once classified, each thread's 64
+    // bytes hold its word's state until the word's stores (stash_word)
     uint8_t buf[2][kTile];
     uint64_t bar[2];
     Span warp_total[kWarps];
     int64_t next_tile;
     int esc_parity[2];  // escape state of each buffered tile's first byte
-    int carry_s;
-    int64_t carry_d, carry_nl;
+    // state before the tile in each buffer (its look-back's result)
+    int carry_s[2];
+    int64_t carry_d[2], carry_nl[2];
 };
+
+// What a word's stores need once the state before its tile is known, kept
+// in the word's own 64 bytes of the tile buffer: eight 8-byte cells, rotated
+// by the thread so that a half-warp's accesses to one cell spread over the
+// banks.
+struct WordState {
+    uint64_t open, close, structural, newline, p0;
+    Span excl;  // composed effect of the tile's words before this one
+};
+
+__device__ __forceinline__ uint64_t* state_cell(uint8_t* buf, int tid, int c) {
+    return reinterpret_cast<uint64_t*>(buf + 64 * tid + 8 * ((c + tid) & 7));
+}
+
+__device__ __forceinline__ void stash_word(uint8_t* buf, int tid, const WordState& w) {
+    *state_cell(buf, tid, 0) = w.open;
+    *state_cell(buf, tid, 1) = w.close;
+    *state_cell(buf, tid, 2) = w.structural;
+    *state_cell(buf, tid, 3) = w.newline;
+    *state_cell(buf, tid, 4) = w.p0;
+    *state_cell(buf, tid, 5) = static_cast<uint32_t>(w.excl.dd0) | (static_cast<uint64_t>(static_cast<uint32_t>(w.excl.ddt)) << 32);
+    *state_cell(buf, tid, 6) = static_cast<uint32_t>(w.excl.nl) | (static_cast<uint64_t>(static_cast<uint32_t>(w.excl.q)) << 32);
+}
+
+__device__ __forceinline__ WordState unstash_word(uint8_t* buf, int tid) {
+    WordState w;
+    w.open = *state_cell(buf, tid, 0);
+    w.close = *state_cell(buf, tid, 1);
+    w.structural = *state_cell(buf, tid, 2);
+    w.newline = *state_cell(buf, tid, 3);
+    w.p0 = *state_cell(buf, tid, 4);
+    const uint64_t a = *state_cell(buf, tid, 5), b = *state_cell(buf, tid, 6);
+    w.excl.dd0 = static_cast<int32_t>(static_cast<uint32_t>(a));
+    w.excl.ddt = static_cast<int32_t>(static_cast<uint32_t>(a >> 32));
+    w.excl.nl = static_cast<int32_t>(static_cast<uint32_t>(b));
+    w.excl.q = static_cast<int32_t>(static_cast<uint32_t>(b >> 32));
+    return w;
+}
+
+// The stores of this thread's word of tile t (state stashed in buffer bb):
+// its string-index word, its words of the leveled bitmaps, its newline
+// offsets.
+template <int LV>
+__device__ __forceinline__ void store_word(const IndexParams& p, Shared& sh, int bb, int64_t t, int tid) {
+    const int64_t ws = t * kTile + 64 * tid;
+    const int64_t left = p.n - ws;
+    const int valid = left <= 0 ? 0 : (left >= 64 ? 64 : static_cast<int>(left));
+    if (valid > 0) {
+        const WordState w = unstash_word(sh.buf[bb], tid);
+        const int s0 = sh.carry_s[bb];
+        const int s_w = s0 ^ w.excl.q;
+        const int64_t d_w = sh.carry_d[bb] + (s0 ? (w.excl.ddt - w.excl.dd0) : w.excl.dd0);
+        uint64_t in_str = w.p0 ^ (s_w ? ~0ull : 0ull);
+        if (valid < 64) in_str &= (1ull << valid) - 1;
+        const int64_t word = ws >> 6;
+        p.string_index[word] = in_str;
+
+        uint64_t lv[LV];
+        split_levels<LV>(w.open & ~in_str, w.close & ~in_str, w.structural & ~in_str, d_w, lv);
+#pragma unroll
+        for (int l = 0; l < LV; l++)
+            if (l < p.num_levels) p.leveled[p.level_size * l + word] = lv[l];
+
+        uint64_t nm = w.newline;
+        int64_t idx = 1 + sh.carry_nl[bb] + w.excl.nl;
+        while (nm) {
+            const int bit = ctz64(nm);
+            if (idx < p.newline_cap) p.newlines[idx] = ws + bit;
+            ++idx;
+            nm &= nm - 1;
+        }
+    }
+    if (t == 0 && tid == 0 && p.newline_cap > 0) p.newlines[0] = 0;
+}
 
 // Thread 0: claim a tile and start loading it into buffer `b`.
 __device__ int64_t claim_and_load(const IndexParams& p, Shared& sh, int b) {
@@ -261,6 +341,7 @@ __global__ void __launch_bounds__(kThreads, LV <= 8 ? 6 : 4) index_kernel(IndexP
     }
     __syncthreads();
     int64_t t = sh.next_tile;
+    int64_t t_prev = -1;  // the tile in buffer b ^ 1 whose words are still to be written
     uint32_t phase[2] = {0, 0};
     int b = 0;
     while (t < p.ntiles) {
@@ -365,55 +446,37 @@ __global__ void __launch_bounds__(kThreads, LV <= 8 ? 6 : 4) index_kernel(IndexP
         for (int w = 0; w < warp; w++) warp_prefix = span_compose(warp_prefix, sh.warp_total[w]);
         excl = span_compose(warp_prefix, excl);
 
+        // every byte of buffer b is read: each word's state goes into its bytes
+        stash_word(sh.buf[b], tid, WordState{m.open, m.close, m.structural, m.newline, p0, excl});
+
+        // Warp 0 looks back for this tile while the other warps write the
+        // previous tile's words (its state before was found one round ago);
+        // warp 0 writes its own words of it after the look-back.
         if (warp == 0) {
             Span tile_total = span_identity();
 #pragma unroll
             for (int w = 0; w < kWarps; w++) tile_total = span_compose(tile_total, sh.warp_total[w]);
             const Carry before = look_back(p.tile_state, t, tile_total, p.epoch, p.status);
             if (lane == 0) {
-                sh.carry_s = before.s;
-                sh.carry_d = before.d;
-                sh.carry_nl = before.nl;
+                sh.carry_s[b] = before.s;
+                sh.carry_d[b] = before.d;
+                sh.carry_nl[b] = before.nl;
                 if (t == p.ntiles - 1) p.status[0] = static_cast<unsigned long long>(before.nl + tile_total.nl + 1);
             }
         }
-        __syncthreads();
+        if (t_prev >= 0) store_word<LV>(p, sh, b ^ 1, t_prev, tid);
+        __syncthreads();  // buffer b ^ 1 is free; this tile's carries are set
         // Claim the next tile only now and start its copy into the other
-        // buffer (last read in the previous iteration): a claimed tile is
-        // processed right away, so successors never wait on a tile whose
-        // owner is still busy with an earlier one.
+        // buffer: a claimed tile is processed right away, so successors never
+        // wait on a tile whose owner is still busy with an earlier one.
         if (tid == 0) sh.next_tile = claim_and_load(p, sh, b ^ 1);
-
-        // ---- final masks and stores ------------------------------------------
-        if (valid > 0) {
-            const int s0 = sh.carry_s;
-            const int s_w = s0 ^ excl.q;
-            const int64_t d_w = sh.carry_d + (s0 ? (excl.ddt - excl.dd0) : excl.dd0);
-            uint64_t in_str = p0 ^ (s_w ? ~0ull : 0ull);
-            if (valid < 64) in_str &= (1ull << valid) - 1;
-            const int64_t word = ws >> 6;
-            p.string_index[word] = in_str;
-
-            uint64_t lv[LV];
-            split_levels<LV>(m.open & ~in_str, m.close & ~in_str, m.structural & ~in_str, d_w, lv);
-#pragma unroll
-            for (int l = 0; l < LV; l++)
-                if (l < p.num_levels) p.leveled[p.level_size * l + word] = lv[l];
-
-            uint64_t nm = m.newline;
-            int64_t idx = 1 + sh.carry_nl + excl.nl;
-            while (nm) {
-                const int bit = ctz64(nm);
-                if (idx < p.newline_cap) p.newlines[idx] = ws + bit;
-                ++idx;
-                nm &= nm - 1;
-            }
-        }
-        if (t == 0 && tid == 0 && p.newline_cap > 0) p.newlines[0] = 0;
-        __syncthreads();  // buffer b and the shared carries are free again
+        __syncthreads();  // the next tile's number is visible
+        t_prev = t;
         t = sh.next_tile;
         b ^= 1;
     }
+    // the last tile's words
+    if (t_prev >= 0) store_word<LV>(p, sh, b ^ 1, t_prev, tid);
 }
 
 }  // namespace
