@@ -554,28 +554,42 @@ __device__ __forceinline__ void finish_word(const IndexParams& p, const TileFile
 // (warp 0 of the index group); flags lines beyond max_ext past the tile.
 __device__ int64_t find_line_end(const TileFile& p, int64_t from, int64_t tile_end, int64_t max_ext) {
     const int lane = threadIdx.x & 31;
+    // four independent 16-byte loads per lane per step: 2 KiB per round
+    // trip (a line of a megabyte is 512 steps; eight loads measured no
+    // faster and cost the tile kernel registers); only bytes below `limit`
+    // are read, those past it may still be on their way from the host
+    constexpr int kChunks = 4;
     int64_t found = kNone;
     int64_t limit = p.n - tile_end > max_ext ? tile_end + max_ext : p.n;
     if (limit > p.avail) limit = p.avail;
-    for (int64_t base = from; base < limit && found == kNone; base += 512) {
-        const int64_t q = base + 16 * lane;
-        uint64_t nlbits = 0;
-        if (q + 16 <= p.n) {
-            const uint4 v = __ldg(reinterpret_cast<const uint4*>(p.file + q));
-            const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+    for (int64_t base = from; base < limit && found == kNone; base += 512 * kChunks) {
+        uint4 v[kChunks];
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                uint32_t f = eq_bytes(w4[i], 0x0A0A0A0Au);
-                while (f) {
-                    nlbits |= 1ull << (4 * i + ((__ffs(f) - 1) >> 3));
-                    f &= f - 1;
-                }
-            }
-        } else {
-            for (int64_t j = q; j < p.n; j++)
-                if (p.file[j] == '\n') nlbits |= 1ull << (j - q);
+        for (int c = 0; c < kChunks; c++) {
+            const int64_t q = base + 512 * c + 16 * lane;
+            v[c] = q + 16 <= limit ? __ldg(reinterpret_cast<const uint4*>(p.file + q)) : make_uint4(0, 0, 0, 0);
         }
-        int64_t best = nlbits ? q + ctz64(nlbits) : kNone;
+        int64_t best = kNone;
+#pragma unroll
+        for (int c = kChunks - 1; c >= 0; c--) {  // the lowest chunk with a '\n' wins
+            const int64_t q = base + 512 * c + 16 * lane;
+            uint64_t nlbits = 0;
+            if (q + 16 <= limit) {
+                const uint32_t w4[4] = {v[c].x, v[c].y, v[c].z, v[c].w};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    uint32_t f = eq_bytes(w4[i], 0x0A0A0A0Au);
+                    while (f) {
+                        nlbits |= 1ull << (4 * i + ((__ffs(f) - 1) >> 3));
+                        f &= f - 1;
+                    }
+                }
+            } else {
+                for (int64_t j = q; j < limit; j++)
+                    if (p.file[j] == '\n') nlbits |= 1ull << (j - q);
+            }
+            if (nlbits) best = q + ctz64(nlbits);
+        }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) {
             const int64_t o = __shfl_xor_sync(~0u, best, off);
