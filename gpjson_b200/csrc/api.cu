@@ -303,6 +303,10 @@ int ensure_tile_state(gpj_ctx* ctx, int64_t ntiles) {
 
 int occupancy_slot(int num_levels) { return num_levels <= 4 ? 0 : (num_levels <= 8 ? 1 : 2); }
 
+// The standalone index kernel's tile counter (the second word of d_counter;
+// the exact kernel uses the first).
+unsigned int* tile_claims(gpj_ctx* ctx) { return ctx->d_counter + 1; }
+
 // One launch of an index kernel; on return h_status holds its status words.
 int launch_index(gpj_ctx* ctx, bool exact, const gpj::IndexParams& base) {
     const int64_t ntiles = base.ntiles;
@@ -387,9 +391,12 @@ int tile_ctas_per_sm(const gpj_ctx* ctx, int num_levels) {
     return want > 0 && want < occ ? want : occ;
 }
 
-int launch_tiles(gpj_ctx* ctx, const gpj::IndexParams& p) {
-    const int occ = tile_ctas_per_sm(ctx, p.num_levels);
-    const int64_t grid = std::min<int64_t>(p.tile_end - p.tile_begin, static_cast<int64_t>(ctx->sms) * occ);
+int launch_tiles(gpj_ctx* ctx, const gpj::IndexParams& base) {
+    const int occ = tile_ctas_per_sm(ctx, base.num_levels);
+    const int64_t grid = std::min<int64_t>(base.tile_end - base.tile_begin, static_cast<int64_t>(ctx->sms) * occ);
+    gpj::IndexParams p = base;
+    p.tile_counter = tile_claims(ctx);
+    GPJ_CUDA(ctx, cudaMemsetAsync(p.tile_counter, 0, sizeof(unsigned int), ctx->stream));
     GPJ_CUDA(ctx, gpj::launch_tile_index_kernel(p, static_cast<int>(grid), ctx->stream));
     ctx->launches++;
     return GPJ_OK;
@@ -1854,7 +1861,9 @@ int batch_index(gpj_ctx* ctx, std::vector<gpj_batch::FileRun>& files) {
                 p.tile_newlines = counts;
                 const int occ = tile_ctas_per_sm(ctx, levels);
                 const int64_t grid = std::min<int64_t>(total_tiles, static_cast<int64_t>(ctx->sms) * occ);
-                e = gpj::launch_tile_index_kernel(p, static_cast<int>(grid), ctx->stream);
+                p.tile_counter = tile_claims(ctx);
+                e = cudaMemsetAsync(p.tile_counter, 0, sizeof(unsigned int), ctx->stream);
+                if (e == cudaSuccess) e = gpj::launch_tile_index_kernel(p, static_cast<int>(grid), ctx->stream);
                 ctx->launches++;
             }
             if (e == cudaSuccess) {

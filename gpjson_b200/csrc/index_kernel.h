@@ -43,7 +43,7 @@ struct IndexParams {
     int64_t* newlines;  // newline_cap entries
     int64_t newline_cap;
     unsigned long long* tile_state;  // 3 * ntiles words, tagged with `epoch`
-    unsigned int* tile_counter;      // zeroed before the launch
+    unsigned int* tile_counter;      // zeroed before the launch; the exact and standalone kernels claim tiles from it
     unsigned long long* status;      // [0] line count, [1] error bits (zeroed before)
     uint32_t epoch;                  // 1..65535
     int materialize;                 // write string_index / leveled / newlines

@@ -1014,6 +1014,7 @@ struct WShared {
     WarpSum rscan[2][kWWarps];
     int carry_esc;
     int64_t long_b;
+    int64_t next_tile;  // the tile claimed for the next round
 };
 
 // Cell c (0..7) of word i of thread g, in the bytes the word was loaded
@@ -1193,11 +1194,17 @@ __global__ void __launch_bounds__(kWThreads, LV <= 4 ? 6 : (LV <= 8 ? 3 : 2)) ti
         mbar_init(&sh.full, 1);
         fence_mbar_init();
     }
+    // Tiles are pulled one at a time from p.tile_counter (zeroed before the
+    // launch), so a CTA that follows a long line past its tile takes fewer
+    // of them; a tile never waits for another, so any claim order is safe.
+    if (tid == 0) {
+        const int64_t t0 = p.tile_begin + static_cast<int64_t>(atomicAdd(p.tile_counter, 1u));
+        sh.next_tile = t0;
+        if (t0 < p.tile_end) start_wide_tile(p, sh, t0, 0);
+    }
     __syncthreads();
-    const int64_t first_tile = p.tile_begin + blockIdx.x, stride = gridDim.x;
-    if (tid == 0 && first_tile < p.tile_end) start_wide_tile(p, sh, first_tile, 0);
     int64_t k = 0;
-    for (int64_t t = first_tile; t < p.tile_end; t += stride, ++k) {
+    for (int64_t t = sh.next_tile; t < p.tile_end; ++k) {
         if (!mbar_wait_bounded(&sh.full, static_cast<uint32_t>(k & 1)) && tid == 0)
             atomicOr(p.status + 1, kErrCopyTimeout);
         uint8_t* slot = sh.bytes;
@@ -1398,9 +1405,17 @@ __global__ void __launch_bounds__(kWThreads, LV <= 4 ? 6 : (LV <= 8 ? 3 : 2)) ti
             }
         }
         group_sync(kBarIndex, kWThreads);  // the slot and sh.acc are read: the next tile's copy may start
-        if (tid == 0 && t + stride < p.tile_end) start_wide_tile(p, sh, t + stride, static_cast<int>((k + 1) & 1));
+        // a line past the slot is finished before the next claim, so that
+        // the tiles go to CTAs that are free
         if (lines_here && tile_end < F.n && ahead_nl == 0 && loaded_end < F.n)
             extend_long_line<LV>(p, F, sh, loaded_end, tile_end, sc.s_end, sc.d_end);
+        if (tid == 0) {
+            const int64_t nt = p.tile_begin + static_cast<int64_t>(atomicAdd(p.tile_counter, 1u));
+            sh.next_tile = nt;
+            if (nt < p.tile_end) start_wide_tile(p, sh, nt, static_cast<int>((k + 1) & 1));
+        }
+        group_sync(kBarIndex, kWThreads);  // the next tile's number is visible
+        t = sh.next_tile;
     }
 }
 
